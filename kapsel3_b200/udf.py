@@ -1,0 +1,230 @@
+"""UDF-driven run description for the SPM step.
+
+KAPSEL reads every run parameter from a UDF file through OCTA's `UDFManager`
+(input.cxx:677-2556).  That library is not available here, so a run is
+described by a flat *key file*: one ``<udf.path> = <value>`` line per UDF
+field the reference reads, keyed by exactly the paths `Gourmet_file_io` asks
+for (e.g. ``mesh.NPX``, ``constitutive_eq.Navier_Stokes.ETA``,
+``switch.INIT_distribution.user_specify.Particles[3].R.x``).  The same file
+drives both the reference program (through its UDF stand-in) and this
+package's C++ loader (`spm_config_from_udf_keys`), so both consume identical
+inputs.
+
+`SPMConfig` carries the physical parameters the step needs; `derived()`
+reproduces the derived globals of `Set_global_parameters`
+(input.cxx:425-604).  `make_particles` is the seeded initial-condition
+generator used for every parity and benchmark case.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Dict, Optional
+
+import numpy as np
+
+EQ_NS = "Navier_Stokes"
+EQ_LE = "Shear_Navier_Stokes_Lees_Edwards"
+
+
+@dataclasses.dataclass
+class SPMConfig:
+    """Parameters of one SPM run (the UDF fields the step reads)."""
+
+    npx: int = 5                 # mesh.NPX: NX = 1 << NPX (input.cxx:1752)
+    npy: int = 5
+    npz: int = 5
+    dx: float = 1.0              # constitutive_eq.<type>.DX
+    rho: float = 1.0
+    eta: float = 1.0
+    kbt: float = 0.0
+    alpha_v: float = 1.0
+    alpha_o: float = 1.0
+    equation: str = EQ_NS        # constitutive_eq.type
+    shear_rate: float = 0.0      # ...Lees_Edwards.External_field.DC.Shear_rate
+    n_particles: int = 2         # Particle_spec[0].Particle_number
+    mass_ratio: float = 1.0
+    a: float = 4.0               # A (radius in units of DX)
+    a_xi: float = 2.0            # A_XI (interface thickness in units of DX)
+    epsilon: float = 1.0         # EPSILON
+    lj_powers: str = "12:6"
+    lj_truncate: str = "ON"
+    rotation: bool = True
+    fix_cell: tuple = (True, True, True)
+    dt: float = 0.05             # time_increment.manual.delta_t
+    gts: int = 1                 # output.GTS
+    num_snap: int = 1            # output.Num_snap (MSTEP = GTS*Num_snap)
+    body_force: tuple = (0.0, 0.0, 0.0)  # constant force on every particle
+
+    # ------------------------------------------------------------------
+    @property
+    def shape(self):
+        return (1 << self.npx, 1 << self.npy, 1 << self.npz)
+
+    def derived(self) -> Dict[str, float]:
+        """Derived globals, as `Set_global_parameters` (input.cxx:425-604)
+        and the particle section of `Gourmet_file_io` (input.cxx:1701-1707,
+        1807-1827) compute them."""
+        nx, ny, nz = self.shape
+        radius = self.a * self.dx
+        xi = self.a_xi * self.dx
+        sigma = 2.0 * radius
+        mass = self.mass_ratio * self.rho * 4.0 / 3.0 * math.pi * radius ** 3
+        moi = 2.0 / 5.0 * mass * radius ** 2
+        pw = {"12:6": 6.0, "24:12": 12.0, "36:18": 18.0}[self.lj_powers]
+        if self.lj_truncate == "ON":
+            a_r_cutoff = 2.0 ** (1.0 / pw)
+        elif self.lj_truncate == "OFF":
+            a_r_cutoff = min(min(nx, ny, nz) * self.dx * 0.5 / sigma, 2.5)
+        else:
+            a_r_cutoff = 0.0
+        if self.equation == EQ_LE:
+            lj_dia = min((sigma + xi) / 2.0 ** (1.0 / pw), sigma)
+        else:
+            lj_dia = sigma
+        return dict(
+            NX=nx, NY=ny, NZ=nz, HNZ_=nz // 2 + 1, NZ_=2 * (nz // 2 + 1),
+            TRN_X=(nx + 2) // 3, TRN_Y=(ny + 2) // 3, TRN_Z=(nz + 2) // 3,
+            RADIUS=radius, XI=xi, HXI=0.5 * xi, SIGMA=sigma,
+            MASS=mass, IMASS=1.0 / mass, MOI=moi, IMOI=1.0 / moi,
+            NU=self.eta / self.rho, DX3=self.dx ** 3,
+            LX=nx * self.dx, LY=ny * self.dx, LZ=nz * self.dx,
+            WAVE_X=2 * math.pi / (nx * self.dx), WAVE_Y=2 * math.pi / (ny * self.dx),
+            WAVE_Z=2 * math.pi / (nz * self.dx),
+            A_R_cutoff=a_r_cutoff, LJ_dia=lj_dia,
+            Ivolume=1.0 / (nx * ny * nz * self.dx ** 3),
+        )
+
+    @property
+    def mstep(self) -> int:
+        return self.gts * self.num_snap
+
+
+def make_particles(cfg: SPMConfig, seed: int, v_sd: float = 0.0,
+                   random_orientation: bool = False,
+                   min_dist_factor: float = 1.05,
+                   max_tries: int = 200000) -> Dict[str, np.ndarray]:
+    """Seeded, non-overlapping uniform positions (random sequential addition
+    with the reference's overlap length 1.05*SIGMA, init_particle.cxx:65-82),
+    optional random unit quaternions and Gaussian velocities.  Deterministic
+    for a given seed (numpy PCG64)."""
+    rng = np.random.default_rng(seed)
+    d = cfg.derived()
+    L = np.array([d["LX"], d["LY"], d["LZ"]])
+    rmin = min_dist_factor * d["SIGMA"]
+    n = cfg.n_particles
+    x = np.zeros((n, 3))
+    tries = 0
+    for i in range(n):
+        while True:
+            tries += 1
+            if tries > max_tries:
+                raise ValueError(f"cannot place {n} particles of radius {cfg.a} in {cfg.shape}")
+            c = rng.random(3) * L
+            if i == 0:
+                break
+            dd = x[:i] - c
+            dd -= np.rint(dd / L) * L
+            if np.min(np.sqrt((dd ** 2).sum(1))) > rmin:
+                break
+        x[i] = c
+    v = rng.normal(0.0, v_sd, size=(n, 3)) if v_sd > 0 else np.zeros((n, 3))
+    if random_orientation:
+        q = rng.normal(size=(n, 4))
+        q /= np.linalg.norm(q, axis=1, keepdims=True)
+    else:
+        q = np.tile(np.array([1.0, 0.0, 0.0, 0.0]), (n, 1))
+    omega = np.zeros((n, 3))
+    return dict(x=x, v=v, q=q, omega=omega)
+
+
+def _fmt(v) -> str:
+    if isinstance(v, bool):
+        return "ON" if v else "OFF"
+    if isinstance(v, float):
+        return repr(v)
+    return str(v)
+
+
+def udf_keys(cfg: SPMConfig, particles: Dict[str, np.ndarray],
+             out_dir: str = "/tmp/kapsel_avs") -> Dict[str, str]:
+    """All UDF paths the reference reads for a spherical-particle spectral
+    run, with this run's values."""
+    eq = cfg.equation
+    k: Dict[str, str] = {}
+    k["resume.Calculation"] = "NEW"
+    k["resume.CONTINUE.Saved_Data.jikan.ts"] = "0"
+    k["constitutive_eq.type"] = eq
+    base = f"constitutive_eq.{eq}"
+    for name, val in (("DX", cfg.dx), ("RHO", cfg.rho), ("ETA", cfg.eta), ("kBT", cfg.kbt),
+                      ("alpha_v", cfg.alpha_v), ("alpha_o", cfg.alpha_o)):
+        k[f"{base}.{name}"] = _fmt(float(val))
+    if eq == EQ_LE:
+        k[f"{base}.External_field.type"] = "DC"
+        k[f"{base}.External_field.DC.Shear_rate"] = _fmt(float(cfg.shear_rate))
+    k["object_type.type"] = "spherical_particle"
+    ps = "object_type.spherical_particle.Particle_spec[0]"
+    k[f"{ps}.Particle_number"] = str(cfg.n_particles)
+    k[f"{ps}.MASS_RATIO"] = _fmt(float(cfg.mass_ratio))
+    k[f"{ps}.Surface_charge"] = "0.0"
+    k[f"{ps}.janus_axis"] = "NONE"
+    k[f"{ps}.janus_propulsion"] = "OFF"
+    k["A_XI"] = _fmt(float(cfg.a_xi))
+    k["A"] = _fmt(float(cfg.a))
+    # Gravity is never used as such (MASS_RATIO=1); a nonzero G only makes the
+    # reference call Add_f_gravity, where the oracle build injects body_force.
+    has_bf = any(f != 0.0 for f in cfg.body_force)
+    k["gravity.G"] = "1.0" if has_bf else "0.0"
+    k["gravity.G_direction"] = "-X"
+    k["EPSILON"] = _fmt(float(cfg.epsilon))
+    k["LJ_powers"] = cfg.lj_powers
+    k["mesh.NPX"], k["mesh.NPY"], k["mesh.NPZ"] = str(cfg.npx), str(cfg.npy), str(cfg.npz)
+    k["time_increment.type"] = "manual"
+    k["time_increment.manual.delta_t"] = _fmt(float(cfg.dt))
+    k["switch.ROTATION"] = _fmt(bool(cfg.rotation))
+    k["switch.LJ_truncate"] = cfg.lj_truncate
+    k["switch.INIT_distribution.type"] = "user_specify"
+    k["switch.INIT_orientation"] = "user_specify"
+    k["switch.SLIP_tol"] = "1e-5"
+    k["switch.SLIP_iter"] = "100"
+    for d, on in zip("xyz", cfg.fix_cell):
+        k[f"switch.FIX_CELL.{d}"] = _fmt(bool(on))
+    k["switch.pin.type"] = "NO"
+    k["output.GTS"] = str(cfg.gts)
+    k["output.Num_snap"] = str(cfg.num_snap)
+    k["output.AVS"] = "ON"
+    k["output.ON.Out_dir"] = out_dir
+    k["output.ON.Out_name"] = "frame"
+    k["output.ON.FileType"] = "BINARY"
+    k["output.UDF"] = "OFF"
+    up = "switch.INIT_distribution.user_specify.Particles"
+    x, v, q, w = particles["x"], particles["v"], particles["q"], particles["omega"]
+    for i in range(cfg.n_particles):
+        t = f"{up}[{i}]"
+        for j, c in enumerate("xyz"):
+            k[f"{t}.R.{c}"] = repr(float(x[i, j]))
+            k[f"{t}.v.{c}"] = repr(float(v[i, j]))
+            k[f"{t}.omega.{c}"] = repr(float(w[i, j]))
+        for j in range(4):
+            k[f"{t}.q.q{j}"] = repr(float(q[i, j]))
+    return k
+
+
+def write_udf_keys(path: str, cfg: SPMConfig, particles: Dict[str, np.ndarray],
+                   out_dir: Optional[str] = None) -> None:
+    keys = udf_keys(cfg, particles, out_dir or "/tmp/kapsel_avs")
+    with open(path, "w") as f:
+        for kk, vv in keys.items():
+            f.write(f"{kk} = {vv}\n")
+
+
+def read_udf_keys(path: str) -> Dict[str, str]:
+    out: Dict[str, str] = {}
+    with open(path) as f:
+        for line in f:
+            line = line.split("#", 1)[0]
+            if "=" not in line:
+                continue
+            kk, vv = line.split("=", 1)
+            out[kk.strip()] = vv.strip()
+    return out

@@ -1,0 +1,155 @@
+// Link-time hooks (`-Wl,--wrap=<mangled name>`; the wrapper functions carry
+// the Itanium-mangled names of the reference functions they replace) that turn the unmodified reference
+// program into a parity oracle.  Nothing here changes the reference's
+// arithmetic; the hooks only observe its state and inject the one input the
+// reference has no UDF knob for.
+//
+//  * Output_* (output.cxx:15-262, called from sp_3d_ns.cxx:863-869 at every
+//    `ts % GTS == 0`): instead of writing AVS/HDF5 frames, append an FP64 record
+//    of the state to the file named by KAPSEL_REF_DUMP.  With GTS=1 the record
+//    at `ts` is the state after `ts` completed steps.  Every
+//    KAPSEL_REF_FIELDS_EVERY frames the record also carries zeta (full
+//    k-space arrays incl. padding), phi, and the real-space velocity rebuilt
+//    from zeta with the reference's own Zeta_k2u_k + U_k2u
+//    (fft_wrapper.cxx:591-688, operate_omega.h:124-128).  Writing the frame
+//    is excluded from the per-step wall-clock samples.
+//  * Add_f_gravity (md_force.cxx:306-324, called from the inline Force() in
+//    particle_solver.h:88-111): when KAPSEL_REF_BODY_FORCE="fx,fy,fz" is set,
+//    add that constant force to every particle's `fr` instead of gravity.  The
+//    reference has no knob for a body force on neutrally buoyant particles
+//    (gravity is scaled by MASS_RATIO-1 = 0 at density 1).
+//  * KAPSEL_REF_STEP_TIMES: file that receives one wall-clock stamp (s) per
+//    frame, i.e. per step, measured with CLOCK_MONOTONIC.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <vector>
+
+#include "fft_wrapper.h"
+#include "input.h"
+#include "operate_omega.h"
+#include "variable.h"
+
+extern double *phi;
+
+extern "C" {
+void __real__Z11Init_outputP8Particle(Particle *p);
+void __real__Z13Add_f_gravityP8Particle(Particle *p);
+}
+
+namespace {
+FILE *             g_dump        = nullptr;
+FILE *             g_times       = nullptr;
+int                g_fields_every = 1;
+int                g_frame       = 0;
+double             g_fx[3]       = {0, 0, 0};
+bool               g_body_force  = false;
+std::vector<double> g_tmp;
+
+double now_s() {
+    timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
+void write_particles(const Particle *p) {
+    std::vector<double> rec;
+    rec.reserve((size_t)Particle_Number * 44);
+    for (int n = 0; n < Particle_Number; n++) {
+        const Particle &q = p[n];
+        const double *  v3[] = {q.x,       q.x_nopbc,        q.v,         q.v_old, q.omega, q.omega_old};
+        for (const double *a : v3) rec.insert(rec.end(), a, a + 3);
+        rec.push_back(q.q.s);
+        rec.insert(rec.end(), q.q.v, q.q.v + 3);
+        rec.push_back(q.q_old.s);
+        rec.insert(rec.end(), q.q_old.v, q.q_old.v + 3);
+        const double *f3[] = {q.f_hydro, q.f_hydro_previous, q.torque_hydro, q.torque_hydro_previous, q.fr,
+                              q.fr_previous};
+        for (const double *a : f3) rec.insert(rec.end(), a, a + 3);
+    }
+    fwrite(rec.data(), sizeof(double), rec.size(), g_dump);
+}
+}  // namespace
+
+extern "C" {
+
+void __wrap__Z11Init_outputP8Particle(Particle *p) {
+    (void)p;
+    const char *path = getenv("KAPSEL_REF_DUMP");
+    if (path && *path) {
+        g_dump = fopen(path, "wb");
+        if (!g_dump) {
+            perror("KAPSEL_REF_DUMP");
+            exit(1);
+        }
+        const char *fe = getenv("KAPSEL_REF_FIELDS_EVERY");
+        if (fe && *fe) g_fields_every = atoi(fe);
+        int hdr[8] = {0x4b53504d, 1, NX, NY, NZ, NZ_, Particle_Number, g_fields_every};
+        fwrite(hdr, sizeof(int), 8, g_dump);
+    }
+    const char *tp = getenv("KAPSEL_REF_STEP_TIMES");
+    if (tp && *tp) g_times = fopen(tp, "w");
+    const char *bf = getenv("KAPSEL_REF_BODY_FORCE");
+    if (bf && *bf) {
+        g_body_force = (sscanf(bf, "%lf,%lf,%lf", &g_fx[0], &g_fx[1], &g_fx[2]) == 3);
+    }
+}
+
+void __wrap__Z11Free_outputv() {
+    if (g_dump) fclose(g_dump);
+    if (g_times) fclose(g_times);
+    g_dump = g_times = nullptr;
+}
+
+void __wrap__Z17Output_open_framev() {
+    if (g_times) fprintf(g_times, "%.9f\n", now_s());
+}
+
+void __wrap__Z18Output_close_framev() {}
+
+// The AVS writer is never initialised (Init_output is replaced above), so its
+// parameter report (output.cxx:89-106) is replaced by one line.
+void __wrap__Z21Show_output_parameterv() { fprintf(stderr, "# oracle build: frames go to KAPSEL_REF_DUMP\n"); }
+
+void __wrap__Z20Output_particle_dataP8ParticleRK5CTime(Particle *p, const CTime &jikan) {
+    (void)jikan;
+    if (g_dump) write_particles(p);
+}
+
+void __wrap__Z17Output_field_dataPPdS_P8ParticleRK5CTime(double **zeta, double *uk_dc, Particle *p, const CTime &jikan) {
+    (void)p;
+    if (!g_dump) return;
+    const size_t n_field = (size_t)NX * NY * NZ_;
+    // 0: no fields; 1: zeta and phi; 2: zeta, phi and the real-space velocity
+    int has_fields = (g_fields_every > 0 && (g_frame % g_fields_every) == 0) ? 1 : 0;
+    if (has_fields && SW_EQ == Navier_Stokes) has_fields = 2;
+    int          ihdr[2]    = {jikan.ts, has_fields};
+    fwrite(ihdr, sizeof(int), 2, g_dump);
+    double dhdr[5] = {jikan.time, degree_oblique, uk_dc[0], uk_dc[1], uk_dc[2]};
+    fwrite(dhdr, sizeof(double), 5, g_dump);
+    if (has_fields) {
+        fwrite(zeta[0], sizeof(double), n_field, g_dump);
+        fwrite(zeta[1], sizeof(double), n_field, g_dump);
+        fwrite(phi, sizeof(double), n_field, g_dump);
+        if (has_fields == 2) {
+            g_tmp.assign(3 * n_field, 0.0);
+            double *uu[3] = {g_tmp.data(), g_tmp.data() + n_field, g_tmp.data() + 2 * n_field};
+            double  dc[3] = {uk_dc[0], uk_dc[1], uk_dc[2]};
+            Zeta_k2u_k(zeta, dc, uu);
+            U_k2u(uu);
+            fwrite(g_tmp.data(), sizeof(double), 3 * n_field, g_dump);
+        }
+    }
+    g_frame++;
+}
+
+void __wrap__Z13Add_f_gravityP8Particle(Particle *p) {
+    if (!g_body_force) {
+        __real__Z13Add_f_gravityP8Particle(p);
+        return;
+    }
+    for (int n = 0; n < Particle_Number; n++)
+        for (int d = 0; d < DIM; d++) p[n].fr[d] += g_fx[d];
+}
+}

@@ -1,0 +1,107 @@
+"""Runs the reference program built from its own sources (oracle/_ref) and
+reads back its FP64 state dumps.
+
+TEST INFRASTRUCTURE ONLY.  Only tests, fixture generation, `smoke()` and the
+CPU-baseline legs of bench.py may use this module; the product never does.
+
+The binaries are produced by oracle/ref_build/Makefile from the unmodified
+reference sources.  A run is described by a UDF key file
+(kapsel3_b200.udf.write_udf_keys); the dump format is written by
+oracle/ref_build/ref_dump.cxx:
+  header  int32[8]: magic 0x4b53504d, version 1, NX, NY, NZ, NZ_, Np, fields_every
+  frame   int32[2]: ts, has_fields
+          f64[5]:   time, degree_oblique, uk_dc[3]
+          has_fields>=1: zeta0, zeta1, phi (each NX*NY*NZ_ f64, reference layout)
+          has_fields==2: u (3 real fields, padded rows; Navier_Stokes runs)
+          f64[Np*44]: per particle x, x_nopbc, v, v_old, omega, omega_old,
+                      q(s,v), q_old(s,v), f_hydro, f_hydro_previous,
+                      torque_hydro, torque_hydro_previous, fr, fr_previous
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+from typing import Dict, List, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+PARTICLE_FIELDS = [("x", 3), ("x_nopbc", 3), ("v", 3), ("v_old", 3), ("omega", 3), ("omega_old", 3),
+                   ("q", 4), ("q_old", 4), ("f_hydro", 3), ("f_hydro_previous", 3),
+                   ("torque_hydro", 3), ("torque_hydro_previous", 3), ("fr", 3), ("fr_previous", 3)]
+PARTICLE_WORDS = sum(n for _, n in PARTICLE_FIELDS)
+
+
+def ref_binary(omp: bool = False) -> Optional[str]:
+    p = os.path.join(REF_DIR, "kapsel_ref_omp" if omp else "kapsel_ref")
+    return p if os.access(p, os.X_OK) else None
+
+
+def available(omp: bool = False) -> bool:
+    return ref_binary(omp) is not None
+
+
+def run_reference(keys_path: str, dump_path: Optional[str] = None, fields_every: int = 1,
+                  body_force=(0.0, 0.0, 0.0), omp: bool = False, threads: Optional[int] = None,
+                  step_times_path: Optional[str] = None, timeout: float = 3600.0) -> str:
+    exe = ref_binary(omp)
+    if exe is None:
+        raise FileNotFoundError("oracle/_ref is not built (make -C oracle/ref_build)")
+    env = dict(os.environ)
+    if dump_path:
+        env["KAPSEL_REF_DUMP"] = dump_path
+        env["KAPSEL_REF_FIELDS_EVERY"] = str(fields_every)
+    if any(f != 0.0 for f in body_force):
+        env["KAPSEL_REF_BODY_FORCE"] = ",".join(repr(float(f)) for f in body_force)
+    if step_times_path:
+        env["KAPSEL_REF_STEP_TIMES"] = step_times_path
+    if threads is not None:
+        env["OMP_NUM_THREADS"] = str(threads)
+    wd = tempfile.mkdtemp(prefix="kapsel_ref_")
+    cmd = [exe, f"-I{keys_path}", f"-O{wd}/out.udf", f"-D{wd}/def.udf", f"-R{wd}/res.udf"]
+    open(f"{wd}/def.udf", "w").close()
+    r = subprocess.run(cmd, env=env, cwd=wd, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference run failed ({r.returncode}):\n{r.stderr[-3000:]}")
+    return r.stderr
+
+
+def read_dump(path: str) -> Dict:
+    raw = open(path, "rb").read()
+    hdr = np.frombuffer(raw, dtype=np.int32, count=8)
+    if hdr[0] != 0x4B53504D:
+        raise ValueError("not a reference dump")
+    nx, ny, nz, nz_, npart, _ = (int(v) for v in hdr[2:8])
+    nfield = nx * ny * nz_
+    off = 32
+    frames: List[Dict] = []
+    while off < len(raw):
+        ts, has_fields = np.frombuffer(raw, dtype=np.int32, count=2, offset=off)
+        off += 8
+        t, deg, u0, u1, u2 = np.frombuffer(raw, dtype=np.float64, count=5, offset=off)
+        off += 40
+        fr: Dict = dict(ts=int(ts), time=float(t), degree_oblique=float(deg),
+                        uk_dc=np.array([u0, u1, u2]))
+        if has_fields:
+            def take(n):
+                nonlocal off
+                a = np.frombuffer(raw, dtype=np.float64, count=n, offset=off).copy()
+                off += 8 * n
+                return a
+            z0 = take(nfield).reshape(nx, ny, nz_)
+            z1 = take(nfield).reshape(nx, ny, nz_)
+            fr["zeta"] = np.stack([z0, z1]).view(np.complex128)  # [2, NX, NY, NZ/2+1]
+            fr["phi"] = take(nfield).reshape(nx, ny, nz_)[:, :, :nz].copy()
+            if has_fields == 2:
+                fr["u"] = take(3 * nfield).reshape(3, nx, ny, nz_)[..., :nz].copy()
+        prec = np.frombuffer(raw, dtype=np.float64, count=npart * PARTICLE_WORDS, offset=off)
+        off += 8 * npart * PARTICLE_WORDS
+        prec = prec.reshape(npart, PARTICLE_WORDS)
+        c = 0
+        for name, n in PARTICLE_FIELDS:
+            fr[name] = prec[:, c:c + n].copy()
+            c += n
+        frames.append(fr)
+    return dict(shape=(nx, ny, nz), n_particles=npart, frames=frames)
