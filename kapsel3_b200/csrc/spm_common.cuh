@@ -1,0 +1,81 @@
+// Common device/host definitions for the B200 SPM step.
+//
+// Field layout in HBM (both precisions):
+//   k-space field  : complex<T> [NX][NY][HNZP]        (HNZP >= NZ/2+1)
+//   real field     : T          [NX][NY][2*HNZP]      (rows padded, in place)
+// For T = double HNZP = NZ/2+1, which is exactly the reference's in-place r2c
+// array [NX][NY][NZ_] (input.cxx:444-445, fft_wrapper.cxx:104-112), so FP64
+// fields cross the C ABI without any reshuffle.  For T = float one extra
+// complex is appended when NZ/2+1 is odd so every row starts on a 16-byte
+// boundary.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstdio>
+
+namespace spm {
+
+template <typename T>
+struct cplx {
+    T re, im;
+};
+
+template <typename T>
+struct vec2_of;
+template <>
+struct vec2_of<double> {
+    using type = double2;
+};
+template <>
+struct vec2_of<float> {
+    using type = float2;
+};
+
+template <typename T>
+__host__ __device__ __forceinline__ cplx<T> cmul(cplx<T> a, cplx<T> b) {
+    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <typename T>
+__host__ __device__ __forceinline__ cplx<T> cadd(cplx<T> a, cplx<T> b) {
+    return {a.re + b.re, a.im + b.im};
+}
+template <typename T>
+__host__ __device__ __forceinline__ cplx<T> csub(cplx<T> a, cplx<T> b) {
+    return {a.re - b.re, a.im - b.im};
+}
+
+// Grid geometry shared by every kernel.
+struct Grid {
+    int nx, ny, nz;
+    int hnz;     // NZ/2+1 complex values per row that carry data
+    int hnzp;    // allocated complex values per row (>= hnz)
+    int trn[3];  // 2/3-rule limits TRN = (N+2)/3 (input.cxx:448)
+    double wave[3];
+    double dx;
+    __host__ __device__ size_t field_elems_c() const { return (size_t)nx * ny * hnzp; }  // complex elements
+};
+
+// Device-side error word: kernels that detect a violated precondition (a
+// particle outside the box, a bounded wait that ran out) set a bit here and
+// skip the offending work; the host checks it after the step.
+enum SpmDeviceError : unsigned int {
+    SPM_DEVERR_PARTICLE_OUT_OF_BOX = 1u << 0,
+    SPM_DEVERR_LJ_CELL_OVERFLOW    = 1u << 1,
+    SPM_DEVERR_NAN                 = 1u << 2,
+    SPM_DEVERR_SCRATCH_TOO_SMALL   = 1u << 3,
+};
+
+}  // namespace spm
+
+#define SPM_CUDA_CHECK(expr)                                                                         \
+    do {                                                                                             \
+        cudaError_t _e = (expr);                                                                     \
+        if (_e != cudaSuccess) {                                                                     \
+            std::fprintf(stderr, "kapsel_spm: CUDA error %s at %s:%d: %s\n", cudaGetErrorName(_e), \
+                         __FILE__, __LINE__, cudaGetErrorString(_e));                                \
+            return SPM_ERR_CUDA;                                                                     \
+        }                                                                                            \
+    } while (0)

@@ -1,0 +1,244 @@
+// Hand-written 3D real FFT for sm_100a (FP64 and FP32), replacing Ooura's
+// rdft3d / rdft3dsort + conjugation behind A2a_k / A_k2a
+// (fft_wrapper.h:641-681, fftsg3d.c:554-709).
+//
+// Convention (FFTW r2c, as the reference produces after its conjugation):
+//   forward  X[kx][ky][kz] = sum_xyz a(x,y,z) e^{-2 pi i (kx x/NX + ky y/NY + kz z/NZ)}
+//            kz = 0..NZ/2, unnormalised
+//   inverse  a = (1/(NX NY NZ)) sum_k X e^{+...}, imaginary parts of the kz=0
+//            and kz=NZ/2 planes are discarded (c2r semantics)
+//
+// Three in-place passes over HBM, each a single kernel:
+//   Z pass: real rows (contiguous) <-> complex rows; length-NZ real transform
+//           done as an NZ/2-point complex four-step FFT in registers + shared
+//           memory, with the even/odd split post-/pre-processing.
+//   Y pass, X pass: length-N complex transforms along a strided axis; a CTA
+//           owns W adjacent kz columns of N lines (W*16 B contiguous per
+//           line) and runs a four-step N = N1*N2 FFT: step 1 loads straight
+//           from HBM into registers (N2-point DFT per thread), twiddles,
+//           transposes through shared memory, step 2 (N1-point DFTs) writes
+//           straight back to HBM.
+// Each pass reads and writes every element exactly once.
+#pragma once
+
+#include "spm_dft.cuh"
+
+namespace spm {
+
+// ---------------------------------------------------------------------------
+// Strided complex pass (Y or X axis).
+// Element n of column c of tile b lives at
+//   base + (b / col_tiles) * outer_stride + (b % col_tiles) * W + c + n * axis_stride
+// ---------------------------------------------------------------------------
+template <typename T, int N, int W, int DIR>
+__global__ void __launch_bounds__(W *Split<N>::N1)
+    fft_strided_kernel(cplx<T> *__restrict__ data, size_t field_stride, int ncols, int col_tiles,
+                       size_t outer_stride, size_t axis_stride, const cplx<T> *__restrict__ twN) {
+    constexpr int N1 = Split<N>::N1;
+    constexpr int N2 = Split<N>::N2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *s = reinterpret_cast<cplx<T> *>(smem_raw);
+
+    const int c   = threadIdx.x % W;
+    const int g   = threadIdx.x / W;  // n1 in step 1, k1 base in step 2
+    const int b   = blockIdx.x;
+    const int col = (b % col_tiles) * W + c;
+    const bool ok = col < ncols;
+    cplx<T> *base = data + (size_t)blockIdx.y * field_stride + (size_t)(b / col_tiles) * outer_stride + col;
+
+    // Step 1: N2-point DFTs over n2 for fixed n1 = g, input index n1 + N1*n2.
+    cplx<T> v[N2];
+#pragma unroll
+    for (int m = 0; m < N2; m++) {
+        if (ok) {
+            v[m] = base[(size_t)(g + N1 * m) * axis_stride];
+        } else {
+            v[m] = cplx<T>{0, 0};
+        }
+    }
+    dft_reg<T, N2, DIR>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < N2; k1++) {
+        cplx<T> w = twN[(g * k1) & (N - 1)];
+        if (DIR > 0) w.im = -w.im;
+        v[k1] = cmul(v[k1], w);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < N2; k1++) s[(g + N1 * k1) * W + c] = v[k1];
+    __syncthreads();
+
+    // Step 2: N1-point DFTs over n1 for each k1 owned by this thread.
+#pragma unroll
+    for (int i = 0; i < N2 / N1; i++) {
+        const int k1 = g + N1 * i;
+        cplx<T>   u[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; n1++) u[n1] = s[(n1 + N1 * k1) * W + c];
+        dft_reg<T, N1, DIR>(u);
+        if (ok) {
+#pragma unroll
+            for (int k2 = 0; k2 < N1; k2++) base[(size_t)(k1 + N2 * k2) * axis_stride] = u[k2];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Z pass, forward: real rows -> complex rows.
+// in:  real row r at in + r*2*hnzp (2M reals used),   M = NZ/2
+// out: complex row r at out + r*hnzp (M+1 values, padding zeroed)
+// in and out may alias (same row footprint).
+// ---------------------------------------------------------------------------
+template <typename T, int M, int R>
+__global__ void __launch_bounds__(R *Split<M>::N1)
+    fft_z_r2c_kernel(const T *in, cplx<T> *out, size_t field_stride_real, size_t field_stride_c, int nrows,
+                     int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN) {
+    constexpr int M1 = Split<M>::N1;
+    constexpr int M2 = Split<M>::N2;
+    constexpr int P  = M1;
+    __shared__ __align__(16) cplx<T> s[R][M];
+    using V2 = typename vec2_of<T>::type;
+
+    const int r   = threadIdx.x / P;
+    const int t   = threadIdx.x % P;
+    const int row = blockIdx.x * R + r;
+    const bool ok = row < nrows;
+    const T *rin  = in + (size_t)blockIdx.y * field_stride_real + (size_t)row * 2 * hnzp;
+    cplx<T> *rout = out + (size_t)blockIdx.y * field_stride_c + (size_t)row * hnzp;
+
+    cplx<T> v[M2];
+#pragma unroll
+    for (int m = 0; m < M2; m++) {
+        if (ok) {
+            V2 p = reinterpret_cast<const V2 *>(rin)[t + M1 * m];
+            v[m] = cplx<T>{p.x, p.y};
+        } else {
+            v[m] = cplx<T>{0, 0};
+        }
+    }
+    dft_reg<T, M2, -1>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < M2; k1++) v[k1] = cmul(v[k1], twM[(t * k1) & (M - 1)]);
+#pragma unroll
+    for (int k1 = 0; k1 < M2; k1++) s[r][t + M1 * k1] = v[k1];
+    __syncthreads();
+
+    cplx<T> z[M2 / M1][M1];
+#pragma unroll
+    for (int i = 0; i < M2 / M1; i++) {
+        const int k1 = t + M1 * i;
+#pragma unroll
+        for (int n1 = 0; n1 < M1; n1++) z[i][n1] = s[r][n1 + M1 * k1];
+        dft_reg<T, M1, -1>(z[i]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < M2 / M1; i++) {
+        const int k1 = t + M1 * i;
+#pragma unroll
+        for (int k2 = 0; k2 < M1; k2++) s[r][k1 + M2 * k2] = z[i][k2];
+    }
+    __syncthreads();
+
+    if (ok) {
+        // X[k] = E[k] + W_N^k O[k],  E = (Z[k] + conj Z[M-k]) / 2,
+        // O = -i (Z[k] - conj Z[M-k]) / 2,  k = 0..M.
+        for (int k = t; k <= M; k += P) {
+            const cplx<T> zk  = s[r][k & (M - 1)];
+            const cplx<T> zmk = s[r][(M - k) & (M - 1)];
+            const T er = (T)0.5 * (zk.re + zmk.re);
+            const T ei = (T)0.5 * (zk.im - zmk.im);
+            const T orr = (T)0.5 * (zk.im + zmk.im);
+            const T oi  = (T)-0.5 * (zk.re - zmk.re);
+            const cplx<T> w = twN[k];  // e^{-2 pi i k / (2M)}, k = 0..M
+            rout[k] = cplx<T>{er + (w.re * orr - w.im * oi), ei + (w.re * oi + w.im * orr)};
+        }
+        for (int k = M + 1 + t; k < hnzp; k += P) rout[k] = cplx<T>{0, 0};
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Z pass, inverse: complex rows -> real rows, output scaled by `scale`.
+// ---------------------------------------------------------------------------
+template <typename T, int M, int R>
+__global__ void __launch_bounds__(R *Split<M>::N1)
+    fft_z_c2r_kernel(const cplx<T> *in, T *out, size_t field_stride_c, size_t field_stride_real, int nrows,
+                     int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale) {
+    constexpr int M1 = Split<M>::N1;
+    constexpr int M2 = Split<M>::N2;
+    constexpr int P  = M1;
+    __shared__ __align__(16) cplx<T> s[R][M + 1];
+    using V2 = typename vec2_of<T>::type;
+
+    const int r   = threadIdx.x / P;
+    const int t   = threadIdx.x % P;
+    const int row = blockIdx.x * R + r;
+    const bool ok = row < nrows;
+    const cplx<T> *rin = in + (size_t)blockIdx.y * field_stride_c + (size_t)row * hnzp;
+    T *rout            = out + (size_t)blockIdx.y * field_stride_real + (size_t)row * 2 * hnzp;
+
+    for (int k = t; k <= M; k += P) {
+        cplx<T> x = ok ? rin[k] : cplx<T>{0, 0};
+        if (k == 0 || k == M) x.im = 0;
+        s[r][k] = x;
+    }
+    __syncthreads();
+    // Z'[k] = E' + i O',  E' = c (X[k] + conj X[M-k]),
+    // O' = c (X[k] - conj X[M-k]) W_N^{-k},  k = 0..M-1.
+    constexpr int KPT = M / P;
+    cplx<T>       zz[KPT];
+#pragma unroll
+    for (int i = 0; i < KPT; i++) {
+        const int k = t + P * i;
+        const cplx<T> xk  = s[r][k];
+        const cplx<T> xmk = s[r][M - k];
+        const T er = scale * (xk.re + xmk.re);
+        const T ei = scale * (xk.im - xmk.im);
+        const T dr = scale * (xk.re - xmk.re);
+        const T di = scale * (xk.im + xmk.im);
+        const cplx<T> w = twN[k];  // e^{-2 pi i k/N}; use its conjugate
+        const T orr = dr * w.re + di * w.im;
+        const T oi  = di * w.re - dr * w.im;
+        zz[i] = cplx<T>{er - oi, ei + orr};
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < KPT; i++) s[r][t + P * i] = zz[i];
+    __syncthreads();
+
+    cplx<T> v[M2];
+#pragma unroll
+    for (int m = 0; m < M2; m++) v[m] = s[r][t + M1 * m];
+    dft_reg<T, M2, +1>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < M2; k1++) {
+        cplx<T> w = twM[(t * k1) & (M - 1)];
+        w.im      = -w.im;
+        v[k1]     = cmul(v[k1], w);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k1 = 0; k1 < M2; k1++) s[r][t + M1 * k1] = v[k1];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < M2 / M1; i++) {
+        const int k1 = t + M1 * i;
+        cplx<T>   u[M1];
+#pragma unroll
+        for (int n1 = 0; n1 < M1; n1++) u[n1] = s[r][n1 + M1 * k1];
+        dft_reg<T, M1, +1>(u);
+        if (ok) {
+#pragma unroll
+            for (int k2 = 0; k2 < M1; k2++) {
+                V2 p;
+                p.x = u[k2].re;
+                p.y = u[k2].im;
+                reinterpret_cast<V2 *>(rout)[k1 + M2 * k2] = p;
+            }
+        }
+    }
+    if (ok && t == 0) {
+        for (int k = 2 * M; k < 2 * hnzp; k++) rout[k] = (T)0;
+    }
+}
+
+}  // namespace spm

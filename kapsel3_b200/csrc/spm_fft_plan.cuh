@@ -1,0 +1,143 @@
+// Host-side plan for the hand-written 3D real FFT: twiddle tables and the
+// dispatch from runtime sizes to the compile-time kernels of spm_fft.cuh.
+#pragma once
+
+#include <vector>
+
+#include "spm_fft.cuh"
+
+namespace spm {
+
+template <typename T>
+struct FFTPlan {
+    Grid     g{};
+    cplx<T> *tw_x  = nullptr;  // e^{-2 pi i j/NX}, j < NX
+    cplx<T> *tw_y  = nullptr;  // e^{-2 pi i j/NY}
+    cplx<T> *tw_zm = nullptr;  // e^{-2 pi i j/(NZ/2)}, j < NZ/2
+    cplx<T> *tw_zn = nullptr;  // e^{-2 pi i k/NZ}, k <= NZ/2
+
+    static constexpr int W = sizeof(T) == 8 ? 16 : 32;  // kz columns per strided tile
+    // rows per Z-pass CTA: 16, fewer for long rows so a CTA's row buffer
+    // stays within 33 KB of static shared memory
+    static constexpr int zrows(int m) {
+        return (int)(32768 / (m * sizeof(cplx<T>))) >= 16 ? 16 : (int)(32768 / (m * sizeof(cplx<T>)));
+    }
+
+    static bool size_ok(int n) { return n >= 8 && n <= 512 && (n & (n - 1)) == 0; }
+
+    cudaError_t create(const Grid &grid) {
+        g = grid;
+        cudaError_t e;
+        if ((e = make_table(&tw_x, g.nx, g.nx)) != cudaSuccess) return e;
+        if ((e = make_table(&tw_y, g.ny, g.ny)) != cudaSuccess) return e;
+        if ((e = make_table(&tw_zm, g.nz / 2, g.nz / 2)) != cudaSuccess) return e;
+        if ((e = make_table(&tw_zn, g.nz, g.nz / 2 + 1)) != cudaSuccess) return e;
+        return set_smem_attrs();
+    }
+    void destroy() {
+        cudaFree(tw_x);
+        cudaFree(tw_y);
+        cudaFree(tw_zm);
+        cudaFree(tw_zn);
+        tw_x = tw_y = tw_zm = tw_zn = nullptr;
+    }
+
+    // In-place forward transform of nfields real fields (padded rows).
+    cudaError_t forward(T *data, int nfields, size_t fstride_c, cudaStream_t st) const {
+        cudaError_t e = z_r2c(data, reinterpret_cast<cplx<T> *>(data), nfields, 2 * fstride_c, fstride_c, st);
+        if (e != cudaSuccess) return e;
+        if ((e = strided<-1>(reinterpret_cast<cplx<T> *>(data), nfields, fstride_c, 1, st)) != cudaSuccess) return e;
+        return strided<-1>(reinterpret_cast<cplx<T> *>(data), nfields, fstride_c, 0, st);
+    }
+    // In-place normalised inverse transform.
+    cudaError_t inverse(cplx<T> *data, int nfields, size_t fstride_c, cudaStream_t st) const {
+        cudaError_t e = strided<+1>(data, nfields, fstride_c, 0, st);
+        if (e != cudaSuccess) return e;
+        if ((e = strided<+1>(data, nfields, fstride_c, 1, st)) != cudaSuccess) return e;
+        return z_c2r(data, reinterpret_cast<T *>(data), nfields, fstride_c, 2 * fstride_c,
+                     (T)(1.0 / ((double)g.nx * g.ny * g.nz)), st);
+    }
+
+    // Individual passes (exposed for the fused step).
+    cudaError_t z_r2c(const T *in, cplx<T> *out, int nfields, size_t fs_real, size_t fs_c, cudaStream_t st) const {
+        const int nrows = g.nx * g.ny;
+        switch (g.nz / 2) {
+#define SPM_ZR2C(MM)                                                                                   \
+    case MM: {                                                                                         \
+        constexpr int RR = zrows(MM);                                                                  \
+        fft_z_r2c_kernel<T, MM, RR><<<dim3((nrows + RR - 1) / RR, nfields), RR * Split<MM>::N1, 0, st>>>( \
+            in, out, fs_real, fs_c, nrows, g.hnzp, tw_zm, tw_zn);                                      \
+    } break;
+            SPM_ZR2C(4) SPM_ZR2C(8) SPM_ZR2C(16) SPM_ZR2C(32) SPM_ZR2C(64) SPM_ZR2C(128) SPM_ZR2C(256)
+#undef SPM_ZR2C
+            default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
+    cudaError_t z_c2r(const cplx<T> *in, T *out, int nfields, size_t fs_c, size_t fs_real, T scale,
+                      cudaStream_t st) const {
+        const int nrows = g.nx * g.ny;
+        switch (g.nz / 2) {
+#define SPM_ZC2R(MM)                                                                                   \
+    case MM: {                                                                                         \
+        constexpr int RR = zrows(MM);                                                                  \
+        fft_z_c2r_kernel<T, MM, RR><<<dim3((nrows + RR - 1) / RR, nfields), RR * Split<MM>::N1, 0, st>>>( \
+            in, out, fs_c, fs_real, nrows, g.hnzp, tw_zm, tw_zn, scale);                               \
+    } break;
+            SPM_ZC2R(4) SPM_ZC2R(8) SPM_ZC2R(16) SPM_ZC2R(32) SPM_ZC2R(64) SPM_ZC2R(128) SPM_ZC2R(256)
+#undef SPM_ZC2R
+            default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
+    // axis 1 = Y, axis 0 = X
+    template <int DIR>
+    cudaError_t strided(cplx<T> *data, int nfields, size_t fs_c, int axis, cudaStream_t st) const {
+        const int    n            = axis == 1 ? g.ny : g.nx;
+        const int    outer        = axis == 1 ? g.nx : g.ny;
+        const size_t outer_stride = axis == 1 ? (size_t)g.ny * g.hnzp : (size_t)g.hnzp;
+        const size_t axis_stride  = axis == 1 ? (size_t)g.hnzp : (size_t)g.ny * g.hnzp;
+        const cplx<T> *tw         = axis == 1 ? tw_y : tw_x;
+        const int    col_tiles    = (g.hnz + W - 1) / W;
+        const dim3   grid(outer * col_tiles, nfields);
+        switch (n) {
+#define SPM_STR(NN)                                                                                              \
+    case NN:                                                                                                     \
+        fft_strided_kernel<T, NN, W, DIR><<<grid, W * Split<NN>::N1, (size_t)NN * W * sizeof(cplx<T>), st>>>( \
+            data, fs_c, g.hnz, col_tiles, outer_stride, axis_stride, tw);                                       \
+        break;
+            SPM_STR(8) SPM_STR(16) SPM_STR(32) SPM_STR(64) SPM_STR(128) SPM_STR(256) SPM_STR(512)
+#undef SPM_STR
+            default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
+
+  private:
+    static cudaError_t make_table(cplx<T> **dst, int n, int count) {
+        std::vector<cplx<T>> h(count);
+        for (int j = 0; j < count; j++) {
+            const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)j / (long double)n;
+            h[j] = cplx<T>{(T)std::cos(a), (T)std::sin(a)};
+        }
+        cudaError_t e = cudaMalloc(dst, sizeof(cplx<T>) * count);
+        if (e != cudaSuccess) return e;
+        return cudaMemcpy(*dst, h.data(), sizeof(cplx<T>) * count, cudaMemcpyHostToDevice);
+    }
+    template <int NN, int DIR>
+    static cudaError_t attr_one() {
+        return cudaFuncSetAttribute(fft_strided_kernel<T, NN, W, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(NN * W * sizeof(cplx<T>)));
+    }
+    static cudaError_t set_smem_attrs() {
+        cudaError_t e = cudaSuccess;
+#define SPM_ATTR(NN)                                               \
+    if ((e = attr_one<NN, -1>()) != cudaSuccess) return e;          \
+    if ((e = attr_one<NN, +1>()) != cudaSuccess) return e;
+        SPM_ATTR(8) SPM_ATTR(16) SPM_ATTR(32) SPM_ATTR(64) SPM_ATTR(128) SPM_ATTR(256) SPM_ATTR(512)
+#undef SPM_ATTR
+        return e;
+    }
+};
+
+}  // namespace spm

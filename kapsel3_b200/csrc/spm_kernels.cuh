@@ -1,0 +1,752 @@
+// Pointwise k-space / real-space kernels, smoothed-profile stencils and the
+// particle integrators of the SPM step.  Field element type T is double (FP64
+// path) or float (FP32-mixed path); particle state, stencil reductions and
+// integrators are always double.
+#pragma once
+
+#include "spm_common.cuh"
+
+namespace spm {
+
+// ---------------------------------------------------------------------------
+// Physical constants of one run, passed by value to every kernel.
+// ---------------------------------------------------------------------------
+struct Phys {
+    double dt, hdt;
+    double nu;          // ETA / RHO
+    double rho;
+    double dx3;
+    double radius, hxi;  // RADIUS, XI/2
+    double L[3];
+    double imass, imoi;
+    double lj_sigma, lj_cutoff, lj_eps;
+    int    lj_powers;   // 0: 12:6, 1: 24:12, 2: 36:18
+    int    lj_on;       // LJ_truncate >= 0
+    int    rotation;
+    int    fix_cell[3];
+    double body_force[3];
+    double noise_v, noise_o;  // thermostat intensities (fluct.cxx:14-18)
+    int    np;
+    int    lc[3];       // reference cell-list cells per axis (md_force.cxx:56-58)
+    double cell_len;    // Cell_length * DX (md_force.cxx:14, 59-61)
+};
+
+// k index decomposition: element (i, j, kz) of a k-space field.
+struct KPoint {
+    int    KX, KY, KZ;
+    double kx, ky, kz;
+    bool   keep;  // inside the 2/3-rule retained box
+};
+
+__device__ __forceinline__ bool k_point(const Grid &g, size_t idx, KPoint &p, size_t &row) {
+    const int kz = (int)(idx % (size_t)g.hnzp);
+    row          = idx / (size_t)g.hnzp;
+    const int j  = (int)(row % (size_t)g.ny);
+    const int i  = (int)(row / (size_t)g.ny);
+    if (kz >= g.hnz) return false;
+    p.KX   = i > g.nx / 2 ? i - g.nx : i;  // Calc_KX_Ooura (fft_wrapper.h:719)
+    p.KY   = j > g.ny / 2 ? j - g.ny : j;
+    p.KZ   = kz;
+    p.kx   = g.wave[0] * (double)p.KX;
+    p.ky   = g.wave[1] * (double)p.KY;
+    p.kz   = g.wave[2] * (double)p.KZ;
+    p.keep = (abs(p.KX) < g.trn[0]) && (abs(p.KY) < g.trn[1]) && (p.KZ < g.trn[2]);
+    return true;
+}
+
+template <typename T>
+__device__ __forceinline__ T ik2_of(const KPoint &p) {
+    const double k2 = p.kx * p.kx + p.ky * p.ky + p.kz * p.kz;
+    return k2 > 0.0 ? (T)(1.0 / k2) : (T)0;
+}
+
+// reduced vorticity -> full vorticity (Zeta_k2u_k case analysis,
+// fft_wrapper.cxx:617-655)
+template <typename T>
+__device__ __forceinline__ void zeta_to_omega(const KPoint &p, cplx<T> z0, cplx<T> z1, cplx<T> om[3]) {
+    if (p.KX != 0) {
+        const T a = -(T)(1.0 / p.kx);
+        const T ky = (T)p.ky, kz = (T)p.kz;
+        om[0] = cplx<T>{a * (ky * z0.re + kz * z1.re), a * (ky * z0.im + kz * z1.im)};
+        om[1] = z0;
+        om[2] = z1;
+    } else if (p.KY != 0) {
+        const T dmy = (T)(-(p.kz / p.ky));
+        om[0] = z1;
+        om[1] = cplx<T>{dmy * z0.re, dmy * z0.im};
+        om[2] = z0;
+    } else {
+        om[0] = z0;
+        om[1] = z1;
+        om[2] = cplx<T>{0, 0};
+    }
+}
+
+// full vorticity -> reduced pair (Omega_k2zeta_k, fft_wrapper.cxx:227-263)
+template <typename T>
+__device__ __forceinline__ void omega_to_zeta(const KPoint &p, const cplx<T> om[3], cplx<T> &z0, cplx<T> &z1) {
+    if (p.KX != 0) {
+        z0 = om[1];
+        z1 = om[2];
+    } else if (p.KY != 0) {
+        z0 = om[2];
+        z1 = om[0];
+    } else {
+        z0 = om[0];
+        z1 = om[1];
+    }
+}
+
+// i (k x a)
+template <typename T>
+__device__ __forceinline__ void i_cross(T kx, T ky, T kz, const cplx<T> a[3], cplx<T> out[3]) {
+    out[0] = cplx<T>{-(ky * a[2].im - kz * a[1].im), ky * a[2].re - kz * a[1].re};
+    out[1] = cplx<T>{-(kz * a[0].im - kx * a[2].im), kz * a[0].re - kx * a[2].re};
+    out[2] = cplx<T>{-(kx * a[1].im - ky * a[0].im), kx * a[1].re - ky * a[0].re};
+}
+
+// ---------------------------------------------------------------------------
+// zeta (2/3-truncated on the fly) -> u_hat (3 fields).  Zeta_k2u_k with the
+// preceding Truncate_two_third_rule (fft_wrapper.cxx:591-688,
+// fft_wrapper.h:754-796).  uk_dc is inserted into the real part of k = 0.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_zeta_to_u(Grid g, const cplx<T> *__restrict__ z0p, const cplx<T> *__restrict__ z1p,
+                            const double *__restrict__ uk_dc, cplx<T> *__restrict__ u0, cplx<T> *__restrict__ u1,
+                            cplx<T> *__restrict__ u2, int truncate) {
+    const size_t n = g.field_elems_c();
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        KPoint p;
+        size_t row;
+        if (!k_point(g, idx, p, row)) {
+            u0[idx] = u1[idx] = u2[idx] = cplx<T>{0, 0};
+            continue;
+        }
+        cplx<T> u[3] = {{0, 0}, {0, 0}, {0, 0}};
+        if (p.keep || !truncate) {
+            cplx<T> om[3];
+            zeta_to_omega<T>(p, z0p[idx], z1p[idx], om);
+            const T ik2 = ik2_of<T>(p);
+            i_cross<T>((T)p.kx * ik2, (T)p.ky * ik2, (T)p.kz * ik2, om, u);
+        }
+        if (idx == 0) {
+            u[0].re = (T)uk_dc[0];
+            u[1].re = (T)uk_dc[1];
+            u[2].re = (T)uk_dc[2];
+        }
+        u0[idx] = u[0];
+        u1[idx] = u[1];
+        u2[idx] = u[2];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Real-space quadratic products of U2advection_k (operate_omega.cxx:31-47):
+//   u0 <- u2 u3, u1 <- u3 u1, u2 <- u1 u2, a0 <- (u2-u3)(u2+u3), a1 <- (u3-u1)(u3+u1)
+// (u1,u2,u3 = x,y,z components).  Rows of 2*hnzp reals, NZ used.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void r_advection_products(Grid g, T *__restrict__ u0, T *__restrict__ u1, T *__restrict__ u2,
+                                     T *__restrict__ a0, T *__restrict__ a1) {
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if ((int)(idx % rowlen) >= g.nz) continue;
+        const T x = u0[idx], y = u1[idx], z = u2[idx];
+        u0[idx] = y * z;
+        u1[idx] = z * x;
+        u2[idx] = x * y;
+        a0[idx] = (y - z) * (y + z);
+        a1[idx] = (z - x) * (z + x);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Curl of the advection term from the FFT'd products, reduction to two
+// components and the slaved-Euler update of zeta on the retained modes
+// (U2advection_k k-part operate_omega.cxx:57-83, Omega_k2zeta_k,
+// NS_solver_slavedEuler fluid_solver.cxx:357-373).  Modes outside the
+// retained box are written as zero (the reference truncates zeta in place at
+// the start of Zeta_k2advection_k and never updates those modes).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_ns_update(Grid g, cplx<T> *__restrict__ z0p, cplx<T> *__restrict__ z1p,
+                            const cplx<T> *__restrict__ p_u2u3, const cplx<T> *__restrict__ p_u3u1,
+                            const cplx<T> *__restrict__ p_u1u2, const cplx<T> *__restrict__ p_a0,
+                            const cplx<T> *__restrict__ p_a1, double nu, double dt) {
+    const size_t n = g.field_elems_c();
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        KPoint p;
+        size_t row;
+        if (!k_point(g, idx, p, row)) continue;
+        if (!p.keep) {
+            z0p[idx] = z1p[idx] = cplx<T>{0, 0};
+            continue;
+        }
+        const T k1 = (T)p.kx, k2 = (T)p.ky, k3 = (T)p.kz;
+        const T k1k2 = k1 * k2, k2k3 = k2 * k3, k3k1 = k3 * k1;
+        const T c0 = (k3 - k2) * (k3 + k2), c1 = (k1 - k3) * (k1 + k3), c2 = (k2 - k1) * (k2 + k1);
+        const cplx<T> u2u3 = p_u2u3[idx], u3u1 = p_u3u1[idx], u1u2 = p_u1u2[idx];
+        const cplx<T> a0 = p_a0[idx], a1 = p_a1[idx];
+        const cplx<T> a2 = {-a1.re - a0.re, -a1.im - a0.im};
+        cplx<T> om[3];
+        om[0] = {-(k2k3 * a0.re + c0 * u2u3.re + k3k1 * u1u2.re - k1k2 * u3u1.re),
+                 -(k2k3 * a0.im + c0 * u2u3.im + k3k1 * u1u2.im - k1k2 * u3u1.im)};
+        om[1] = {-(k3k1 * a1.re + c1 * u3u1.re + k1k2 * u2u3.re - k2k3 * u1u2.re),
+                 -(k3k1 * a1.im + c1 * u3u1.im + k1k2 * u2u3.im - k2k3 * u1u2.im)};
+        om[2] = {-(k1k2 * a2.re + c2 * u1u2.re + k2k3 * u3u1.re - k3k1 * u2u3.re),
+                 -(k1k2 * a2.im + c2 * u1u2.im + k2k3 * u3u1.im - k3k1 * u2u3.im)};
+        cplx<T> f0, f1;
+        omega_to_zeta<T>(p, om, f0, f1);
+        const double k2sum = p.kx * p.kx + p.ky * p.ky + p.kz * p.kz;
+        T            dmy, c;
+        if (sizeof(T) == 8) {
+            dmy = (T)(exp(-nu * dt * k2sum) - 1.0);
+        } else {
+            dmy = (T)expm1(-nu * dt * k2sum);
+        }
+        c = (T)((1.0 / nu) * (k2sum > 0.0 ? 1.0 / k2sum : 0.0));
+        cplx<T> z0 = z0p[idx], z1 = z1p[idx];
+        z0.re += dmy * (z0.re - c * f0.re);
+        z0.im += dmy * (z0.im - c * f0.im);
+        z1.re += dmy * (z1.re - c * f1.re);
+        z1.im += dmy * (z1.im - c * f1.im);
+        z0p[idx] = z0;
+        z1p[idx] = z1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 2/3 truncation + solenoidal projection of three k-space fields
+// (Solenoidal_u's k-space part: Truncate_two_third_rule + Solenoidal_uk,
+// operate_omega.h:105-112, operate_omega.cxx:171-195).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_truncate_project(Grid g, cplx<T> *__restrict__ f0, cplx<T> *__restrict__ f1,
+                                   cplx<T> *__restrict__ f2, int truncate) {
+    const size_t n = g.field_elems_c();
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        KPoint p;
+        size_t row;
+        if (!k_point(g, idx, p, row)) continue;
+        if (truncate && !p.keep) {
+            f0[idx] = f1[idx] = f2[idx] = cplx<T>{0, 0};
+            continue;
+        }
+        const T kx = (T)p.kx, ky = (T)p.ky, kz = (T)p.kz, ik2 = ik2_of<T>(p);
+        cplx<T> a = f0[idx], b = f1[idx], c = f2[idx];
+        const T dr = ik2 * (a.re * kx + b.re * ky + c.re * kz);
+        const T di = ik2 * (a.im * kx + b.im * ky + c.im * kz);
+        a.re -= dr * kx;
+        a.im -= di * kx;
+        b.re -= dr * ky;
+        b.im -= di * ky;
+        c.re -= dr * kz;
+        c.im -= di * kz;
+        f0[idx] = a;
+        f1[idx] = b;
+        f2[idx] = c;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// u_hat -> zeta and uk_dc (U_k2zeta_k, fft_wrapper.cxx:407-476).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_u_to_zeta(Grid g, const cplx<T> *__restrict__ u0, const cplx<T> *__restrict__ u1,
+                            const cplx<T> *__restrict__ u2, cplx<T> *__restrict__ z0p, cplx<T> *__restrict__ z1p,
+                            double *__restrict__ uk_dc) {
+    const size_t n = g.field_elems_c();
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        KPoint p;
+        size_t row;
+        if (!k_point(g, idx, p, row)) {
+            z0p[idx] = z1p[idx] = cplx<T>{0, 0};
+            continue;
+        }
+        const cplx<T> u[3] = {u0[idx], u1[idx], u2[idx]};
+        if (idx == 0) {
+            uk_dc[0] = (double)u[0].re;
+            uk_dc[1] = (double)u[1].re;
+            uk_dc[2] = (double)u[2].re;
+        }
+        cplx<T> om[3];
+        i_cross<T>((T)p.kx, (T)p.ky, (T)p.kz, u, om);
+        cplx<T> a, b;
+        omega_to_zeta<T>(p, om, a, b);
+        z0p[idx] = a;
+        z1p[idx] = b;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Real-space field updates.
+// f = up - min(phi_sum, 1) u   (Make_f_particle_dt_nonsole, f_particle.h:35-54)
+// written in place over up.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void r_make_f(Grid g, T *__restrict__ up0, T *__restrict__ up1, T *__restrict__ up2,
+                         const T *__restrict__ u0, const T *__restrict__ u1, const T *__restrict__ u2,
+                         const T *__restrict__ phi_sum) {
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if ((int)(idx % rowlen) >= g.nz) continue;
+        const T ph = phi_sum[idx] < (T)1 ? phi_sum[idx] : (T)1;
+        up0[idx]   = up0[idx] - ph * u0[idx];
+        up1[idx]   = up1[idx] - ph * u1[idx];
+        up2[idx]   = up2[idx] - ph * u2[idx];
+    }
+}
+
+// u += f  (Add_f_particle, f_particle.h:68-84)
+template <typename T>
+__global__ void r_add3(Grid g, T *__restrict__ u0, T *__restrict__ u1, T *__restrict__ u2, const T *__restrict__ f0,
+                       const T *__restrict__ f1, const T *__restrict__ f2) {
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if ((int)(idx % rowlen) >= g.nz) continue;
+        u0[idx] += f0[idx];
+        u1[idx] += f1[idx];
+        u2[idx] += f2[idx];
+    }
+}
+
+// phi = min(phi_sum, 1) over the whole field (Make_phi_particle_sum tail,
+// make_phi.cxx:248-259) -- only materialised for the per-function API.
+template <typename T>
+__global__ void r_phi_clamp(Grid g, const T *__restrict__ phi_sum, T *__restrict__ phi) {
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if ((int)(idx % rowlen) >= g.nz) continue;
+        phi[idx] = phi_sum[idx] < (T)1 ? phi_sum[idx] : (T)1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Smoothed profile (profile.h:30-50) and stencil geometry (make_phi.h:114-170,
+// interaction.h:113-132).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double H_prof(double x, double dx) {
+    if (!(x > 0.0)) return 0.0;
+    const double r = dx / x;
+    return exp(-(r * r));
+}
+__device__ __forceinline__ double phi_prof(double x, double radius, double hxi, double dx) {
+    const double h1 = H_prof(radius + hxi - x, dx);
+    return h1 / (h1 + H_prof(x - radius + hxi, dx));
+}
+__device__ __forceinline__ int nint_d(double a) { return a >= 0.0 ? (int)(a + 0.5) : (int)(a - 0.5); }
+
+struct StencilPoint {
+    size_t idx;   // real-field element index (padded rows)
+    double r[3];  // cell * dx - residue
+    double dist;  // minimum-image distance grid point <-> particle centre
+};
+
+__device__ __forceinline__ void stencil_point(const Grid &g, const Phys &ph, const double xp[3], int cell_packed,
+                                              StencilPoint &s) {
+    const int    c[3] = {(int)(int8_t)(cell_packed & 0xff), (int)(int8_t)((cell_packed >> 8) & 0xff),
+                         (int)(int8_t)((cell_packed >> 16) & 0xff)};
+    const int    n[3] = {g.nx, g.ny, g.nz};
+    const double idx  = 1.0 / g.dx;
+    int          rm[3];
+    double       d2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double dmy     = xp[d] * idx;
+        const int    x_int   = (int)dmy;
+        const double residue = (dmy - (double)x_int) * g.dx;
+        rm[d]                = (x_int + c[d] + n[d]) % n[d];
+        s.r[d]               = (double)c[d] * g.dx - residue;
+        double x12           = xp[d] - (double)rm[d] * g.dx;
+        x12 -= (double)nint_d(x12 / ph.L[d]) * ph.L[d];
+        d2 += x12 * x12;
+    }
+    s.dist = sqrt(d2);
+    s.idx  = ((size_t)rm[0] * g.ny + rm[1]) * (2 * (size_t)g.hnzp) + rm[2];
+}
+
+__device__ __forceinline__ bool particle_in_box(const Phys &ph, const double xp[3]) {
+    return xp[0] >= 0.0 && xp[0] < ph.L[0] && xp[1] >= 0.0 && xp[1] < ph.L[1] && xp[2] >= 0.0 && xp[2] < ph.L[2];
+}
+
+// phi_sum += Phi over every (particle, Sekibun cell)  (make_phi.cxx:214-247)
+template <typename T>
+__global__ void s_phi_scatter(Grid g, Phys ph, const double *__restrict__ x, const int *__restrict__ cells,
+                              int ncells, T *__restrict__ phi_sum, unsigned int *err) {
+    const int p = blockIdx.y;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ph.np || m >= ncells) return;
+    const double xp[3] = {x[3 * p], x[3 * p + 1], x[3 * p + 2]};
+    if (!particle_in_box(ph, xp)) {
+        if (m == 0) atomicOr(err, (unsigned)SPM_DEVERR_PARTICLE_OUT_OF_BOX);
+        return;
+    }
+    StencilPoint s;
+    stencil_point(g, ph, xp, cells[m], s);
+    const double v = phi_prof(s.dist, ph.radius, ph.hxi, g.dx);
+    if (v != 0.0) atomicAdd(&phi_sum[s.idx], (T)v);
+}
+
+// up += (v + w x r) Phi / max(phi_sum, 1)   (make_phi.cxx:313-354)
+template <typename T>
+__global__ void s_up_scatter(Grid g, Phys ph, const double *__restrict__ x, const double *__restrict__ v,
+                             const double *__restrict__ w, const int *__restrict__ cells, int ncells,
+                             const T *__restrict__ phi_sum, T *__restrict__ up0, T *__restrict__ up1,
+                             T *__restrict__ up2) {
+    const int p = blockIdx.y;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ph.np || m >= ncells) return;
+    const double xp[3] = {x[3 * p], x[3 * p + 1], x[3 * p + 2]};
+    if (!particle_in_box(ph, xp)) return;
+    StencilPoint s;
+    stencil_point(g, ph, xp, cells[m], s);
+    double wgt = phi_prof(s.dist, ph.radius, ph.hxi, g.dx);
+    if (wgt == 0.0) return;
+    const double ps = (double)phi_sum[s.idx];
+    wgt /= (ps > 1.0 ? ps : 1.0);
+    double vs[3] = {v[3 * p], v[3 * p + 1], v[3 * p + 2]};
+    if (ph.rotation) {
+        const double *o = w + 3 * p;
+        vs[0] += o[1] * s.r[2] - o[2] * s.r[1];
+        vs[1] += o[2] * s.r[0] - o[0] * s.r[2];
+        vs[2] += o[0] * s.r[1] - o[1] * s.r[0];
+    }
+    atomicAdd(&up0[s.idx], (T)(vs[0] * wgt));
+    atomicAdd(&up1[s.idx], (T)(vs[1] * wgt));
+    atomicAdd(&up2[s.idx], (T)(vs[2] * wgt));
+}
+
+// Block-wide sum of 6 doubles (blockDim.x a multiple of 32, <= 1024).
+__device__ __forceinline__ void block_sum6(double v[6]) {
+    __shared__ double red[32][6];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) red[wid][k] = v[k];
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            double a = lane < nw ? red[lane][k] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+            v[k] = a;
+        }
+    }
+}
+
+// Hydrodynamic force and torque (Calc_f_hydro_correct_precision,
+// md_force.cxx:383-506): one CTA per particle, FP64 accumulation.
+template <typename T>
+__global__ void s_hydro_force(Grid g, Phys ph, const double *__restrict__ x, const double *__restrict__ v,
+                              const double *__restrict__ w, const int *__restrict__ cells, int ncells,
+                              const T *__restrict__ phi_sum, const T *__restrict__ u0, const T *__restrict__ u1,
+                              const T *__restrict__ u2, double *__restrict__ f_hydro,
+                              double *__restrict__ torque_hydro) {
+    const int p = blockIdx.x;
+    if (p >= ph.np) return;
+    const double xp[3] = {x[3 * p], x[3 * p + 1], x[3 * p + 2]};
+    const double vp[3] = {v[3 * p], v[3 * p + 1], v[3 * p + 2]};
+    const double op[3] = {w[3 * p], w[3 * p + 1], w[3 * p + 2]};
+    const bool   inbox = particle_in_box(ph, xp);
+    double       acc[6] = {0, 0, 0, 0, 0, 0};
+    if (inbox) {
+        for (int m = threadIdx.x; m < ncells; m += blockDim.x) {
+            StencilPoint s;
+            stencil_point(g, ph, xp, cells[m], s);
+            double wgt = phi_prof(s.dist, ph.radius, ph.hxi, g.dx);
+            if (wgt == 0.0) continue;
+            const double ps = (double)phi_sum[s.idx];
+            wgt /= (ps > 1.0 ? ps : 1.0);
+            double vs[3] = {vp[0], vp[1], vp[2]};
+            if (ph.rotation) {
+                vs[0] += op[1] * s.r[2] - op[2] * s.r[1];
+                vs[1] += op[2] * s.r[0] - op[0] * s.r[2];
+                vs[2] += op[0] * s.r[1] - op[1] * s.r[0];
+            }
+            const double fp0 = (vs[0] - (double)u0[s.idx]) * wgt;
+            const double fp1 = (vs[1] - (double)u1[s.idx]) * wgt;
+            const double fp2 = (vs[2] - (double)u2[s.idx]) * wgt;
+            acc[0] += fp0;
+            acc[1] += fp1;
+            acc[2] += fp2;
+            acc[3] += s.r[1] * fp2 - s.r[2] * fp1;
+            acc[4] += s.r[2] * fp0 - s.r[0] * fp2;
+            acc[5] += s.r[0] * fp1 - s.r[1] * fp0;
+        }
+    }
+    block_sum6(acc);
+    if (threadIdx.x == 0) {
+        const double dmy = -ph.dx3 * ph.rho / ph.dt;
+        for (int d = 0; d < 3; d++) f_hydro[3 * p + d] = dmy * acc[d];
+        if (ph.rotation)
+            for (int d = 0; d < 3; d++) torque_hydro[3 * p + d] = dmy * acc[3 + d];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Particle state (FP64, [Np][3] / [Np][4] arrays).
+// ---------------------------------------------------------------------------
+struct PState {
+    double *x, *x_nopbc, *x_previous, *v, *v_old, *omega, *omega_old;
+    double *q, *q_old;  // [Np][4]: s, v0, v1, v2
+    double *f_hydro, *f_hydro_previous, *torque_hydro, *torque_hydro_previous;
+    double *fr, *fr_previous, *torque_r, *torque_r_previous;
+    double *lj_stress;  // [Np] per-particle share of sum f_x r_y (LE stress)
+};
+
+__device__ __forceinline__ void qtn_prod_d(const double *qa, const double *qb, double alpha, double *q) {
+    q[0] = alpha * (qa[0] * qb[0] - (qa[1] * qb[1] + qa[2] * qb[2] + qa[3] * qb[3]));
+    q[1] = alpha * (qa[0] * qb[1] + qb[0] * qa[1] + qa[2] * qb[3] - qa[3] * qb[2]);
+    q[2] = alpha * (qa[0] * qb[2] + qb[0] * qa[2] + qa[3] * qb[1] - qa[1] * qb[3]);
+    q[3] = alpha * (qa[0] * qb[3] + qb[0] * qa[3] + qa[1] * qb[2] - qa[2] * qb[1]);
+}
+// dq/dt = 0.5 (0, w) o q  (qdot SPACE_FRAME, rigid_body.cxx:157-168)
+__device__ __forceinline__ void qdot_space_d(const double *q, const double *w, double *dq) {
+    const double qw[4] = {0.0, w[0], w[1], w[2]};
+    qtn_prod_d(qw, q, 0.5, dq);
+}
+__device__ __forceinline__ void qtn_normalize_d(double *q) {
+    const double n = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    const double s = 1.0 / n;
+    for (int k = 0; k < 4; k++) q[k] *= s;
+}
+
+// MD_solver_position_Euler / _AB2 (particle_solver.cxx:39-85) with the
+// orientation updates (particle_rotation_solver.h:23-29, 72-81) and PBC
+// (periodic_boundary.h:9-16).
+__global__ void p_position(Phys ph, PState s, int euler) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ph.np) return;
+    for (int d = 0; d < 3; d++) {
+        const int i       = 3 * n + d;
+        s.x_previous[i]   = s.x[i];
+        const double dlt  = euler ? ph.dt * s.v[i] : ph.hdt * (3.0 * s.v[i] - s.v_old[i]);
+        s.x_nopbc[i] += dlt;
+        s.x[i] = fmod(s.x[i] + dlt + ph.L[d], ph.L[d]);
+    }
+    if (ph.rotation) {
+        double *q = s.q + 4 * n, *qo = s.q_old + 4 * n;
+        double  dq[4];
+        if (euler) {
+            for (int k = 0; k < 4; k++) qo[k] = q[k];
+            qdot_space_d(q, s.omega + 3 * n, dq);
+            for (int k = 0; k < 4; k++) q[k] += dq[k] * ph.dt;
+        } else {
+            double dqo[4];
+            qdot_space_d(q, s.omega + 3 * n, dq);
+            qdot_space_d(qo, s.omega_old + 3 * n, dqo);
+            for (int k = 0; k < 4; k++) qo[k] = q[k];
+            for (int k = 0; k < 4; k++) q[k] += dq[k] * (3.0 * ph.hdt);
+            for (int k = 0; k < 4; k++) q[k] += dqo[k] * (-ph.hdt);
+        }
+        qtn_normalize_d(q);
+    }
+}
+
+// Lennard-Jones magnitude / r (Lennard_Jones_f, interaction.h:160-199).
+__device__ __forceinline__ double lj_f(double r, const Phys &ph) {
+    double s = ph.lj_sigma / r;
+    double p = (s * s) * (s * s) * (s * s);
+    double coeff = 24.0 * ph.lj_eps;
+    if (ph.lj_powers == 1) {
+        p = p * p;
+        coeff = 48.0 * ph.lj_eps;
+    } else if (ph.lj_powers == 2) {
+        p = p * p * p;
+        coeff = 72.0 * ph.lj_eps;
+    }
+    return coeff / (r * r) * (2.0 * p * p - p);
+}
+
+// Number of times the reference cell list visits a pair (md_force.cxx:56-101):
+// cells of Cell_length*DX = 16*DX, per axis the neighbour scan ic-1, ic, ic+1
+// wraps -1 -> lc-1 and lc -> 0, so with lc < 3 cells per axis a neighbour
+// cell is visited more than once (and with lc = 1 three times).
+__device__ __forceinline__ int lj_multiplicity(const Phys &ph, const double *xa, const double *xb) {
+    int mult = 1;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const int ma = (int)(xa[d] / ph.cell_len);
+        const int mb = (int)(xb[d] / ph.cell_len);
+        int       cnt = 0;
+#pragma unroll
+        for (int o = -1; o <= 1; o++) {
+            int c = ma + o;
+            if (c < 0) c = ph.lc[d] - 1;
+            if (c > ph.lc[d] - 1) c = 0;
+            cnt += (c == mb);
+        }
+        mult *= cnt;
+    }
+    return mult;
+}
+
+// Minimum-image x_b - x_a (Distance0, interaction.h:113-122).
+__device__ __forceinline__ double min_image(const Phys &ph, const double *xa, const double *xb, double r[3]) {
+    double d2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        double x12 = xb[d] - xa[d];
+        x12 -= (double)nint_d(x12 / ph.L[d]) * ph.L[d];
+        r[d] = x12;
+        d2 += x12 * x12;
+    }
+    return sqrt(d2);
+}
+
+// LJ pair forces plus the constant body force (Force, particle_solver.h:88-111;
+// Calc_f_Lennard_Jones_shear_cap_primitive_lnk, md_force.cxx:34-196).  Thread
+// n gathers every pair term acting on particle n with the reference's pair
+// multiplicity, so no atomics are needed.  lj_stress[n] receives particle n's
+// share of sum f_x r_y over the pairs where it is the higher index, as the
+// reference accumulates dev_shear_stress_lj.
+__global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ph.np) return;
+    double f[3]   = {0.0, 0.0, 0.0};
+    double stress = 0.0;
+    if (ph.lj_on) {
+        for (int m = 0; m < ph.np; m++) {
+            if (m == n) continue;
+            const int     hi = n > m ? n : m, lo = n > m ? m : n;
+            double        r[3], rr;  // r = x_other - x_n (with the periodic image rule)
+            int           mult = 1;
+            if (all_pairs_le) {
+                // O(N^2) loop with Distance0_OBL(x_lo, x_hi) (md_force.cxx:198-304,
+                // interaction.h:50-72): y image first, then the x shift of the
+                // Lees-Edwards image.
+                const double *x1 = s.x + 3 * lo, *x2 = s.x + 3 * hi;
+                double        y12 = x2[1] - x1[1];
+                double        sy  = y12;
+                y12 -= (double)nint_d(y12 / ph.L[1]) * ph.L[1];
+                sy -= y12;
+                int sign = (int)sy;
+                if (sign != 0) sign = sign / abs(sign);
+                double x12 = x2[0] - (x1[0] + (double)sign * le_shift);
+                x12 -= (double)nint_d(x12 / ph.L[0]) * ph.L[0];
+                double z12 = x2[2] - x1[2];
+                z12 -= (double)nint_d(z12 / ph.L[2]) * ph.L[2];
+                rr = sqrt(y12 * y12 + x12 * x12 + z12 * z12);
+                const double sg = (n == lo) ? 1.0 : -1.0;
+                r[0]            = sg * x12;
+                r[1]            = sg * y12;
+                r[2]            = sg * z12;
+            } else {
+                // cell-list pairs (i > j) with Distance0(x_i, x_j)
+                mult = lj_multiplicity(ph, s.x + 3 * hi, s.x + 3 * lo);
+                if (mult == 0) continue;
+                double rij[3];
+                rr              = min_image(ph, s.x + 3 * hi, s.x + 3 * lo, rij);
+                const double sg = (n == hi) ? 1.0 : -1.0;
+                r[0]            = sg * rij[0];
+                r[1]            = sg * rij[1];
+                r[2]            = sg * rij[2];
+            }
+            if (!(rr < ph.lj_cutoff)) continue;
+            const double dmy_r = lj_f(rr, ph);
+            for (int d = 0; d < 3; d++) f[d] += (double)mult * (-dmy_r * r[d]);
+            if (n == hi) stress += (double)mult * (-dmy_r * r[0]) * r[1];
+        }
+    }
+    for (int d = 0; d < 3; d++) s.fr[3 * n + d] += f[d] + ph.body_force[d];
+    s.lj_stress[n] = stress;
+}
+
+// MD_solver_velocity_Euler / _AB2_hydro (particle_solver.cxx:103-142,
+// 239-281) followed by reset_Forces (particle_solver.cxx:11-37).
+__global__ void p_velocity(Phys ph, PState s, int euler) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ph.np) return;
+    const double dmy = (euler ? ph.dt : ph.hdt) * ph.imass;
+    const double dmr = (euler ? ph.dt : ph.hdt) * ph.imoi;
+    for (int d = 0; d < 3; d++) {
+        const int i      = 3 * n + d;
+        s.v_old[i]       = s.v[i];
+        s.omega_old[i]   = s.omega[i];
+        if (euler) {
+            s.v[i] += dmy * (s.f_hydro[i] + s.fr[i]);
+            s.omega[i] += dmr * (s.torque_hydro[i] + s.torque_r[i]);
+        } else {
+            s.v[i] += dmy * (2.0 * s.f_hydro[i] + s.fr[i] + s.fr_previous[i]);
+            s.omega[i] += dmr * (2.0 * s.torque_hydro[i] + s.torque_r[i] + s.torque_r_previous[i]);
+        }
+        s.fr_previous[i]           = s.fr[i];
+        s.fr[i]                    = 0.0;
+        s.f_hydro_previous[i]      = s.f_hydro[i];
+        s.f_hydro[i]               = 0.0;
+        s.torque_r_previous[i]     = s.torque_r[i];
+        s.torque_r[i]              = 0.0;
+        s.torque_hydro_previous[i] = s.torque_hydro[i];
+        s.torque_hydro[i]          = 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Thermostat: MT19937 (Matsumoto & Nishimura 1998; init_genrand/genrand_real3
+// as used by the reference, mt19937ar.c:65-192) and polar Box-Muller
+// (Gauss2, fluct.h:48-60), drawn in the reference's serial order: per
+// particle three pairs, v gets the first three normals, omega the last three
+// (Add_random_force_thermostat, fluct.cxx:10-37).
+// State layout: mt[0..623], mt[624] = mti.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned int mt_next(unsigned int *mt) {
+    unsigned int mti = mt[624];
+    if (mti >= 624u) {
+        for (int i = 0; i < 624; i++) {
+            const unsigned int y = (mt[i] & 0x80000000u) | (mt[(i + 1) % 624] & 0x7fffffffu);
+            unsigned int       v = mt[(i + 397) % 624] ^ (y >> 1);
+            if (y & 1u) v ^= 0x9908b0dfu;
+            mt[i] = v;
+        }
+        mti = 0;
+    }
+    unsigned int y = mt[mti++];
+    mt[624]        = mti;
+    y ^= (y >> 11);
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= (y >> 18);
+    return y;
+}
+__device__ __forceinline__ double mt_real3(unsigned int *mt) {
+    return ((double)mt_next(mt) + 0.5) * (1.0 / 4294967296.0);
+}
+__device__ __forceinline__ void gauss2(unsigned int *mt, double &g0, double &g1) {
+    double x1, x2, rsq;
+    do {
+        x1  = 2.0 * mt_real3(mt) - 1.0;
+        x2  = 2.0 * mt_real3(mt) - 1.0;
+        rsq = x1 * x1 + x2 * x2;
+    } while (rsq >= 1.0 || rsq == 0.0);
+    const double factor = sqrt(-2.0 * log(rsq) / rsq);
+    g0                  = factor * x1;
+    g1                  = factor * x2;
+}
+
+__global__ void p_thermostat_serial(Phys ph, PState s, unsigned int *mt) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int n = 0; n < ph.np; n++) {
+        double g[6];
+        gauss2(mt, g[0], g[1]);
+        gauss2(mt, g[2], g[3]);
+        gauss2(mt, g[4], g[5]);
+        for (int d = 0; d < 3; d++) {
+            s.v[3 * n + d] += g[d] * ph.noise_v * ph.imass;
+            if (ph.rotation) s.omega[3 * n + d] += g[d + 3] * ph.noise_o * ph.imoi;
+        }
+    }
+}
+
+}  // namespace spm

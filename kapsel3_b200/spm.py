@@ -1,0 +1,296 @@
+"""Python host mirror of the reference's SPM-step interface, over the C ABI.
+
+`SPMRun` owns one device context.  Its methods carry the reference's names
+and argument meaning (Time_evolution_hydro, NS_solver_slavedEuler,
+Solenoidal_uk, Make_phi_particle_sum, Make_u_particle_sum, Make_phi_u_particle,
+Make_f_particle_dt_sole, Calc_f_hydro_correct_precision, Calc_f_Lennard_Jones);
+arrays are numpy float64 in the reference layout:
+  * k-space field: complex128 [NX, NY, NZ//2+1] (== double[NX*NY*NZ_])
+  * real field:    float64   [NX, NY, NZ]   (padded to NZ_ at the boundary)
+  * particles:     dict of [Np, 3] / [Np, 4] arrays, or the packed
+                   [Np, SPM_PARTICLE_WORDS] record array of the C ABI.
+Errors raise `SpmError` with the library's message (the reference exits).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import _native as N
+from .udf import EQ_LE, SPMConfig
+
+RECORD = [("x", 3), ("x_nopbc", 3), ("v", 3), ("v_old", 3), ("omega", 3), ("omega_old", 3),
+          ("q", 4), ("q_old", 4), ("f_hydro", 3), ("f_hydro_previous", 3),
+          ("torque_hydro", 3), ("torque_hydro_previous", 3), ("fr", 3), ("fr_previous", 3)]
+
+
+def pack_particles(p: Dict[str, np.ndarray], n: int) -> np.ndarray:
+    rec = np.zeros((n, N.SPM_PARTICLE_WORDS))
+    c = 0
+    for name, w in RECORD:
+        if name in p:
+            rec[:, c:c + w] = np.asarray(p[name], dtype=float).reshape(n, w)
+        elif name == "x_nopbc" and "x" in p:
+            rec[:, c:c + w] = np.asarray(p["x"], dtype=float)
+        elif name == "q_old" and "q" in p:
+            rec[:, c:c + w] = np.asarray(p["q"], dtype=float)
+        elif name in ("q", "q_old"):
+            rec[:, c] = 1.0
+        c += w
+    return rec
+
+
+def unpack_particles(rec: np.ndarray) -> Dict[str, np.ndarray]:
+    out, c = {}, 0
+    for name, w in RECORD:
+        out[name] = rec[:, c:c + w].copy()
+        c += w
+    return out
+
+
+def params_from_config(cfg: SPMConfig, precision: int = N.SPM_PREC_FP64,
+                       mt_seed: int = 0) -> N.SpmParams:
+    L = N.lib()
+    p = N.SpmParams()
+    N.check(L.spm_params_default(C.byref(p)), "spm_params_default")
+    p.npx, p.npy, p.npz = cfg.npx, cfg.npy, cfg.npz
+    p.dx, p.rho, p.eta, p.kbt = cfg.dx, cfg.rho, cfg.eta, cfg.kbt
+    p.alpha_v, p.alpha_o = cfg.alpha_v, cfg.alpha_o
+    p.equation = N.SPM_EQ_LEES_EDWARDS if cfg.equation == EQ_LE else N.SPM_EQ_NAVIER_STOKES
+    p.shear_rate = cfg.shear_rate
+    p.n_particles = cfg.n_particles
+    p.mass_ratio = cfg.mass_ratio
+    p.a, p.a_xi = cfg.a, cfg.a_xi
+    p.epsilon = cfg.epsilon
+    p.lj_powers = {"12:6": 0, "24:12": 1, "36:18": 2}[cfg.lj_powers]
+    p.lj_truncate = {"ON": 1, "OFF": 0, "NONE": -1}[cfg.lj_truncate]
+    p.rotation = 1 if cfg.rotation else 0
+    for d in range(3):
+        p.fix_cell[d] = 1 if cfg.fix_cell[d] else 0
+        p.body_force[d] = float(cfg.body_force[d])
+    p.dt = cfg.dt
+    p.precision = precision
+    p.mt_seed = mt_seed
+    return p
+
+
+class SPMRun:
+    """One SPM run resident on the GPU."""
+
+    def __init__(self, cfg: SPMConfig, precision: int = N.SPM_PREC_FP64, stream: Optional[int] = None,
+                 mt_seed: int = 0):
+        self.cfg = cfg
+        self.L = N.lib()
+        self.params = params_from_config(cfg, precision, mt_seed)
+        self.precision = precision
+        self.shape = cfg.shape
+        nx, ny, nz = self.shape
+        self.hnz = nz // 2 + 1
+        self.nfield = nx * ny * 2 * self.hnz
+        h = C.c_void_p()
+        N.check(self.L.spm_create(C.byref(self.params), C.c_void_p(stream) if stream else None, C.byref(h)),
+                "spm_create")
+        self.h = h
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if self.h:
+            self.L.spm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- helpers ---------------------------------------------------------
+    def _kfield(self):
+        return np.zeros(self.nfield)
+
+    def _as_k(self, a: np.ndarray) -> np.ndarray:
+        nx, ny, _ = self.shape
+        return a.view(np.complex128).reshape(nx, ny, self.hnz)
+
+    def _real_out(self, a: np.ndarray) -> np.ndarray:
+        nx, ny, nz = self.shape
+        return a.reshape(nx, ny, 2 * self.hnz)[:, :, :nz].copy()
+
+    def _real_in(self, r: np.ndarray) -> np.ndarray:
+        nx, ny, nz = self.shape
+        a = np.zeros((nx, ny, 2 * self.hnz))
+        a[:, :, :nz] = r
+        return a.ravel()
+
+    def _k_in(self, k: np.ndarray) -> np.ndarray:
+        return np.ascontiguousarray(k, dtype=np.complex128).view(np.float64).ravel().copy()
+
+    # -- whole run -------------------------------------------------------
+    def initialize(self, particles):
+        rec = particles if isinstance(particles, np.ndarray) else pack_particles(particles, self.cfg.n_particles)
+        rec = np.ascontiguousarray(rec, dtype=float)
+        N.check(self.L.spm_initialize(self.h, N.dptr(rec)), "spm_initialize")
+
+    def step(self, n: int = 1):
+        """Time_evolution_hydro / Time_evolution_hydro_OBL, n times."""
+        N.check(self.L.spm_step(self.h, n), "spm_step")
+
+    def synchronize(self):
+        N.check(self.L.spm_synchronize(self.h), "spm_synchronize")
+
+    def time_steps(self, n: int) -> float:
+        ms = C.c_float()
+        N.check(self.L.spm_time_steps(self.h, n, C.byref(ms)), "spm_time_steps")
+        return float(ms.value)
+
+    def particles_record(self) -> np.ndarray:
+        rec = np.zeros((self.cfg.n_particles, N.SPM_PARTICLE_WORDS))
+        N.check(self.L.spm_get_particles(self.h, N.dptr(rec)), "spm_get_particles")
+        return rec
+
+    def particles(self) -> Dict[str, np.ndarray]:
+        return unpack_particles(self.particles_record())
+
+    def set_particles(self, particles):
+        rec = particles if isinstance(particles, np.ndarray) else pack_particles(particles, self.cfg.n_particles)
+        rec = np.ascontiguousarray(rec, dtype=float)
+        N.check(self.L.spm_set_particles(self.h, N.dptr(rec)), "spm_set_particles")
+
+    def zeta(self):
+        z0, z1, dc = self._kfield(), self._kfield(), np.zeros(3)
+        N.check(self.L.spm_get_zeta(self.h, N.dptr(z0), N.dptr(z1), N.dptr(dc)), "spm_get_zeta")
+        return np.stack([self._as_k(z0), self._as_k(z1)]), dc
+
+    def set_zeta(self, zeta: np.ndarray, uk_dc):
+        z0, z1 = self._k_in(zeta[0]), self._k_in(zeta[1])
+        dc = np.ascontiguousarray(uk_dc, dtype=float)
+        N.check(self.L.spm_set_zeta(self.h, N.dptr(z0), N.dptr(z1), N.dptr(dc)), "spm_set_zeta")
+
+    def velocity(self) -> np.ndarray:
+        u = [self._kfield() for _ in range(3)]
+        N.check(self.L.spm_get_velocity(self.h, *[N.dptr(a) for a in u]), "spm_get_velocity")
+        return np.stack([self._real_out(a) for a in u])
+
+    def phi(self) -> np.ndarray:
+        a = self._kfield()
+        N.check(self.L.spm_get_phi(self.h, N.dptr(a)), "spm_get_phi")
+        return self._real_out(a)
+
+    def time(self):
+        ts, t = C.c_int(), C.c_double()
+        N.check(self.L.spm_get_time(self.h, C.byref(ts), C.byref(t)), "spm_get_time")
+        return ts.value, t.value
+
+    def shear_state(self):
+        deg, st = C.c_double(), np.zeros(4)
+        N.check(self.L.spm_get_shear_state(self.h, C.byref(deg), N.dptr(st)), "spm_get_shear_state")
+        return deg.value, st
+
+    def kernel_launches(self, reset: bool = False) -> int:
+        n = C.c_longlong()
+        N.check(self.L.spm_kernel_launches(self.h, C.byref(n), 1 if reset else 0), "spm_kernel_launches")
+        return n.value
+
+    # -- reference solver boundaries (host arrays) -----------------------
+    def NS_solver_slavedEuler(self, zeta: np.ndarray, uk_dc: np.ndarray):
+        z0, z1 = self._k_in(zeta[0]), self._k_in(zeta[1])
+        dc = np.ascontiguousarray(uk_dc, dtype=float).copy()
+        N.check(self.L.spm_ns_solver_slaved_euler_host(self.h, N.dptr(z0), N.dptr(z1), N.dptr(dc)),
+                "NS_solver_slavedEuler")
+        return np.stack([self._as_k(z0), self._as_k(z1)])
+
+    def Solenoidal_uk(self, uk: np.ndarray) -> np.ndarray:
+        a = [self._k_in(uk[d]) for d in range(3)]
+        N.check(self.L.spm_solenoidal_uk_host(self.h, *[N.dptr(x) for x in a]), "Solenoidal_uk")
+        return np.stack([self._as_k(x) for x in a])
+
+    def Zeta_k2u_k(self, zeta: np.ndarray, uk_dc) -> np.ndarray:
+        z0, z1 = self._k_in(zeta[0]), self._k_in(zeta[1])
+        dc = np.ascontiguousarray(uk_dc, dtype=float)
+        u = [self._kfield() for _ in range(3)]
+        N.check(self.L.spm_zeta_k2u_k_host(self.h, N.dptr(z0), N.dptr(z1), N.dptr(dc), *[N.dptr(x) for x in u]),
+                "Zeta_k2u_k")
+        return np.stack([self._as_k(x) for x in u])
+
+    def U_k2zeta_k(self, uk: np.ndarray):
+        a = [self._k_in(uk[d]) for d in range(3)]
+        z0, z1, dc = self._kfield(), self._kfield(), np.zeros(3)
+        N.check(self.L.spm_u_k2zeta_k_host(self.h, *[N.dptr(x) for x in a], N.dptr(z0), N.dptr(z1), N.dptr(dc)),
+                "U_k2zeta_k")
+        return np.stack([self._as_k(z0), self._as_k(z1)]), dc
+
+    def A2a_k(self, a_real: np.ndarray) -> np.ndarray:
+        a = self._real_in(a_real)
+        N.check(self.L.spm_a2a_k_host(self.h, N.dptr(a)), "A2a_k")
+        return self._as_k(a)
+
+    def A_k2a(self, ak: np.ndarray) -> np.ndarray:
+        a = self._k_in(ak)
+        N.check(self.L.spm_a_k2a_host(self.h, N.dptr(a)), "A_k2a")
+        return self._real_out(a)
+
+    def Make_phi_particle_sum(self, particles):
+        rec = np.ascontiguousarray(particles if isinstance(particles, np.ndarray)
+                                   else pack_particles(particles, self.cfg.n_particles), dtype=float)
+        phi, phs = self._kfield(), self._kfield()
+        N.check(self.L.spm_make_phi_particle_sum_host(self.h, N.dptr(rec), N.dptr(phi), N.dptr(phs)),
+                "Make_phi_particle_sum")
+        return self._real_out(phi), self._real_out(phs)
+
+    def Make_u_particle_sum(self, particles, phi_sum: np.ndarray) -> np.ndarray:
+        rec = np.ascontiguousarray(particles if isinstance(particles, np.ndarray)
+                                   else pack_particles(particles, self.cfg.n_particles), dtype=float)
+        ps = self._real_in(phi_sum)
+        up = [self._kfield() for _ in range(3)]
+        N.check(self.L.spm_make_u_particle_sum_host(self.h, N.dptr(rec), N.dptr(ps), *[N.dptr(x) for x in up]),
+                "Make_u_particle_sum")
+        return np.stack([self._real_out(x) for x in up])
+
+    def Make_phi_u_particle(self, particles):
+        rec = np.ascontiguousarray(particles if isinstance(particles, np.ndarray)
+                                   else pack_particles(particles, self.cfg.n_particles), dtype=float)
+        phi = self._kfield()
+        up = [self._kfield() for _ in range(3)]
+        N.check(self.L.spm_make_phi_u_particle_host(self.h, N.dptr(rec), N.dptr(phi), *[N.dptr(x) for x in up]),
+                "Make_phi_u_particle")
+        return self._real_out(phi), np.stack([self._real_out(x) for x in up])
+
+    def Make_f_particle_dt_sole(self, u: np.ndarray, up: np.ndarray, phi: np.ndarray) -> np.ndarray:
+        ua = [self._real_in(u[d]) for d in range(3)]
+        upa = [self._real_in(up[d]) for d in range(3)]
+        ph = self._real_in(phi)
+        f = [self._kfield() for _ in range(3)]
+        N.check(self.L.spm_make_f_particle_dt_sole_host(self.h, *[N.dptr(x) for x in ua], *[N.dptr(x) for x in upa],
+                                                        N.dptr(ph), *[N.dptr(x) for x in f]),
+                "Make_f_particle_dt_sole")
+        return np.stack([self._real_out(x) for x in f])
+
+    def Calc_f_hydro_correct_precision(self, particles, phi_sum: np.ndarray, u: np.ndarray) -> np.ndarray:
+        rec = np.ascontiguousarray(particles if isinstance(particles, np.ndarray)
+                                   else pack_particles(particles, self.cfg.n_particles), dtype=float).copy()
+        ps = self._real_in(phi_sum)
+        ua = [self._real_in(u[d]) for d in range(3)]
+        N.check(self.L.spm_calc_f_hydro_correct_precision_host(self.h, N.dptr(rec), N.dptr(ps),
+                                                               *[N.dptr(x) for x in ua]),
+                "Calc_f_hydro_correct_precision")
+        return rec
+
+    def Calc_f_Lennard_Jones(self, particles) -> np.ndarray:
+        rec = np.ascontiguousarray(particles if isinstance(particles, np.ndarray)
+                                   else pack_particles(particles, self.cfg.n_particles), dtype=float).copy()
+        N.check(self.L.spm_calc_f_lennard_jones_host(self.h, N.dptr(rec)), "Calc_f_Lennard_Jones")
+        return rec
+
+
+def device_count() -> int:
+    n = C.c_int()
+    N.check(N.lib().spm_device_count(C.byref(n)), "spm_device_count")
+    return n.value

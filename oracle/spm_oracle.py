@@ -524,6 +524,13 @@ class OracleSPM:
         self.ts += 1
         self.time += self.dt
 
+    def _phi_of_positions(self) -> np.ndarray:
+        """phi_sum of the current particle positions (Make_phi_particle_sum)."""
+        flat, r, dist = self.stencil_geometry(self.x)
+        phi_sum = np.zeros(self.NX * self.NY * self.NZ)
+        np.add.at(phi_sum, flat.ravel(), self.profile(dist).ravel())
+        return phi_sum.reshape(self.NX, self.NY, self.NZ)
+
     def velocity_field(self) -> np.ndarray:
         """Real-space velocity of the current state, as rebuilt from zeta
         (Zeta_k2u_k + U_k2u)."""
