@@ -1,0 +1,386 @@
+"""Benchmark of the B200 SPM step (KAPSEL smoothed-profile method).
+
+Workload (the headline configuration): 256^3 periodic grid, 1000 colloids
+a=5, xi=2, seeded non-overlapping positions, random unit quaternions,
+Gaussian velocities sd=1e-3, LJ repulsion (sigma=2a, eps=1, cutoff
+2^(1/6) sigma), dt=0.05, no thermal noise.  A step is one
+Time_evolution_hydro (sp_3d_ns.cxx:41-194) on device-resident state.
+
+  value      FP32-mixed steps/s, whole job (N replicas, one per GPU)
+  e2e        same metric through the C ABI with host particle records:
+             every step uploads the Np particle records from pinned host
+             memory, runs the step and reads them back
+  fp64       FP64 GPU path steps/s on the same workload
+  accuracy   relative L2 velocity error FP32-mixed vs FP64 after the
+             timed steps from the same initial state
+  roofline   dominant kernel (FFT strided pass) achieved GB/s vs measured peak
+  cpu_baseline  the reference program built from its sources (oracle/_ref),
+             OpenMP, all host cores, on a bounded sample of the same workload
+
+`--impl reference` runs that reference program alone on rank 0 (other ranks
+exit) for the same metric on a bounded number of steps.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(npx=8, npy=8, npz=8, n_particles=1000, a=5.0, a_xi=2.0, dt=0.05)
+METRIC = "SPM steps/s 256³ 1000 colloids, FP32-mixed vs FP64 GPU @≤1e-5; p99 serve lat"
+UNIT = "steps/s"
+
+
+def workload_config():
+    from kapsel3_b200.udf import SPMConfig
+    return SPMConfig(**WORKLOAD)
+
+
+def workload_particles(cfg):
+    from kapsel3_b200.udf import make_particles
+    return make_particles(cfg, seed=2024, v_sd=1e-3, random_orientation=True)
+
+
+def config_block():
+    return {"workload": "SPM step, 256^3 periodic grid, 1000 colloids a=5 xi=2, LJ 12:6 WCA, dt=0.05, no noise",
+            "grid": [256, 256, 256], "colloids": 1000, "radius": 5.0, "xi": 2.0, "dt": 0.05,
+            "l2": "inputs larger than L2 (one field is 135 MB FP64 / 67 MB FP32; 11 fields resident)",
+            "parallelism": "replicas (one independent run per GPU, no collective)"}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    def __init__(self):
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            try:
+                import pynvml
+                pynvml.nvmlInit()
+                idx = int(os.environ.get("LOCAL_RANK", "0"))
+                vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+                h = pynvml.nvmlDeviceGetHandleByIndex(idx if vis is None else 0 if "," not in vis else idx)
+                smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+                while not self._stop.is_set():
+                    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    reasons = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((sm, smax, reasons))
+                    time.sleep(0.05)
+            except Exception as e:  # no NVML: report that
+                self.samples.append(("error", str(e), 0))
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=2)
+        good = [s for s in self.samples if s[0] != "error"]
+        if not good:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        names = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+                 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+                 0x100: "display_clock_setting"}
+        mask = 0
+        for s in good:
+            mask |= int(s[2])
+        return {"sm_mhz": float(np.median([s[0] for s in good])), "sm_max_mhz": float(good[0][1]),
+                "reasons": [v for k, v in names.items() if mask & k], "samples": len(good)}
+
+
+# --------------------------------------------------------------- reference
+def reference_available():
+    from oracle import ref_runner
+    return ref_runner.available(omp=True)
+
+
+def time_reference(cfg, parts, nsteps, threads):
+    """Runs the reference program (oracle/_ref, OpenMP build) for nsteps+1
+    steps and returns steps/s over steps 1..nsteps (step 0 excluded: it
+    includes first-touch of every array)."""
+    from kapsel3_b200.udf import write_udf_keys
+    from oracle import ref_runner
+    import dataclasses
+    c = dataclasses.replace(cfg, gts=1, num_snap=nsteps)
+    d = tempfile.mkdtemp(prefix="kapsel_bench_ref_")
+    keys, stamps = os.path.join(d, "run.keys"), os.path.join(d, "stamps.txt")
+    write_udf_keys(keys, c, parts, out_dir=os.path.join(d, "avs"))
+    ref_runner.run_reference(keys, dump_path=None, omp=True, threads=threads, step_times_path=stamps,
+                             timeout=1800)
+    t = np.loadtxt(stamps)
+    # stamp i is taken at the start of step i (after i completed steps)
+    dts = np.diff(t)[1:]
+    return float(1.0 / np.mean(dts)), len(dts)
+
+
+def port_baseline(cfg, parts, nsteps):
+    """Fallback when the reference program is not built: the numpy oracle."""
+    from oracle.spm_oracle import OracleSPM
+    o = OracleSPM(cfg, parts)
+    o.step()
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        o.step()
+    return nsteps / (time.perf_counter() - t0), nsteps
+
+
+def cpu_baseline(cfg, parts):
+    threads = os.cpu_count() or 1
+    if reference_available():
+        v, n = time_reference(cfg, parts, 3, threads)
+        return {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"{n} steps of the full 256^3/1000-colloid workload (steps 2..{n + 1} of a fresh run), "
+                          f"reference program built from its sources, GCC_OMP flags, OMP_NUM_THREADS={threads}"}
+    v, n = port_baseline(cfg, parts, 1)
+    return {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n} step of the full workload with the numpy restatement (reference program not built)"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cfg = workload_config()
+    parts = workload_particles(cfg)
+    threads = os.cpu_count() or 1
+    nsteps = max(1, min(args.steps, 4))
+    if reference_available():
+        v, n = time_reference(cfg, parts, nsteps + 1, threads)
+        kind = "reference"
+        sample = (f"{n} steps of the full workload after one warm-up step, reference program built from its own "
+                  f"sources (GCC_OMP flags), OMP_NUM_THREADS={threads}")
+    else:
+        v, n = port_baseline(cfg, parts, min(nsteps, 2))
+        kind, threads = "port", 1
+        sample = f"{n} steps with the numpy restatement (reference program not built)"
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus, "steps": n,
+            "warmup": 1, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded initial state)",
+            "config": config_block(),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------- GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", choices=["fp32", "fp64"], default=None,
+                    help="only run warm-up + timed steps of one precision (for ncu captures)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    if args.profile_run:
+        return profile_run(args)
+
+    import torch
+    import torch.distributed as dist
+    from kapsel3_b200 import _native as N
+    from kapsel3_b200.spm import SPMRun, pack_particles
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    W, K = max(3, args.warmup), max(1, args.steps)
+    cfg = workload_config()
+    parts = workload_particles(cfg)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    stream = torch.cuda.current_stream().cuda_stream
+    for prec, name in ((N.SPM_PREC_FP32_MIXED, "fp32"), (N.SPM_PREC_FP64, "fp64")):
+        run = SPMRun(cfg, precision=prec, stream=stream)
+        run.initialize(parts)
+        run.step(W)
+        run.synchronize()
+        run.kernel_launches(reset=True)
+        barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler()
+        clocks.start()
+        ms = run.time_steps(K)
+        cl = clocks.stop()
+        torch.cuda.synchronize()
+        barrier()
+        ms = max_over_ranks(ms)
+        launches = run.kernel_launches(reset=True)
+        results[name] = dict(ms=ms, clocks=cl, launches=launches, u=run.velocity())
+        if name == "fp32":
+            # e2e through the C ABI: particle records from pinned host memory
+            # in, step, records out, every step.
+            L = N.lib()
+            n = cfg.n_particles
+            rec_t = torch.from_numpy(run.particles_record()).pin_memory()
+            rec = rec_t.numpy()
+            ptr = rec.ctypes.data_as(C.POINTER(C.c_double))
+            for _ in range(2):
+                N.check(L.spm_set_particles(run.h, ptr), "spm_set_particles")
+                N.check(L.spm_step(run.h, 1), "spm_step")
+                N.check(L.spm_get_particles(run.h, ptr), "spm_get_particles")
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(K):
+                N.check(L.spm_set_particles(run.h, ptr), "spm_set_particles")
+                N.check(L.spm_step(run.h, 1), "spm_step")
+                N.check(L.spm_get_particles(run.h, ptr), "spm_get_particles")
+            e2e_s = max_over_ranks(time.perf_counter() - t0)
+            results["e2e"] = dict(value=world * K / e2e_s, h2d=n * N.SPM_PARTICLE_WORDS * 8,
+                                  d2h=n * N.SPM_PARTICLE_WORDS * 8)
+            # dominant kernel timing inside real steps (CUDA events on the stream)
+            results["prof"] = profile_dominant(run, K)
+        run.close()
+
+    # accuracy: FP32-mixed vs FP64 after W+K steps from the same state (+ the 2 e2e warm-up + K e2e steps on fp32:
+    # recompute both on an equal footing below)
+    acc = accuracy_check(cfg, parts, steps=W + K)
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+    fp32, fp64 = results["fp32"], results["fp64"]
+    value = world * K / (fp32["ms"] / 1000.0)
+    peaks = read_peaks()
+    prof = results["prof"]
+    roof = {"bound": "hbm", "kernel": prof["kernel"], "achieved": prof["gbs"], "peak": peaks["hbm_gbs"],
+            "unit": "GB/s", "frac": prof["gbs"] / peaks["hbm_gbs"], "traffic": None,
+            "peak_source": peaks["source"], "bytes_per_launch": prof["bytes"], "avg_launch_us": prof["us"],
+            "note": "algorithmic bytes = one read + one write of every complex element the pass transforms"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": fp32["ms"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 fields / f64 particle reductions", "data": "synthetic (seeded initial state)",
+        "config": config_block(),
+        "fp64": {"value": world * K / (fp64["ms"] / 1000.0), "unit": UNIT, "ms_per_step": fp64["ms"] / K,
+                 "clocks": fp64["clocks"]},
+        "fp32_over_fp64": fp64["ms"] / fp32["ms"],
+        "accuracy": acc,
+        "e2e": {"value": results["e2e"]["value"], "unit": UNIT, "h2d_bytes_per_step": results["e2e"]["h2d"],
+                "d2h_bytes_per_step": results["e2e"]["d2h"]},
+        "roofline": roof,
+        "step_hbm": {"algorithmic_gb_per_step_fp32": step_bytes(cfg, 4) / 1e9,
+                     "achieved_gbs": step_bytes(cfg, 4) / (fp32["ms"] / K / 1000.0) / 1e9,
+                     "frac_of_peak": step_bytes(cfg, 4) / (fp32["ms"] / K / 1000.0) / 1e9 / peaks["hbm_gbs"]},
+        "clocks": fp32["clocks"],
+        "gpu_launches": fp32["launches"],
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, parts)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def profile_run(args):
+    """Warm-up + timed steps of one precision, nothing else: the command the
+    ncu launch lists and captures under profiles/ were taken with."""
+    from kapsel3_b200 import _native as N
+    from kapsel3_b200.spm import SPMRun
+    cfg = workload_config()
+    if os.environ.get("SPM_PROFILE_GRID"):
+        import dataclasses
+        k = int(os.environ["SPM_PROFILE_GRID"])
+        cfg = dataclasses.replace(cfg, npx=k, npy=k, npz=k)
+    parts = workload_particles(cfg)
+    prec = N.SPM_PREC_FP32_MIXED if args.profile_run == "fp32" else N.SPM_PREC_FP64
+    with SPMRun(cfg, precision=prec) as run:
+        run.initialize(parts)
+        run.step(args.warmup)
+        run.synchronize()
+        ms = run.time_steps(args.steps)
+        print(json.dumps({"profile_run": args.profile_run, "grid": cfg.shape, "steps": args.steps,
+                          "ms_per_step": ms / args.steps}), flush=True)
+    return 0
+
+
+def step_bytes(cfg, w):
+    """Algorithmic HBM bytes of one step: (2*20 + 12) field passes of
+    S_w = N^2 (N+2) w bytes plus 13 words per stencil cell (FP64 words for
+    the particle side)."""
+    nx, ny, nz = cfg.shape
+    S = nx * ny * (nz + 2) * w
+    return 52 * S + cfg.n_particles * 1935 * 13 * 8
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured (MEASURED_PEAKS.json)"}
+    except Exception:
+        return {"hbm_gbs": 6650.0, "source": "fallback 6.65 TB/s"}
+
+
+def profile_dominant(run, K):
+    from kapsel3_b200 import _native as N
+    L = N.lib()
+    L.spm_profile_pass.restype = C.c_int
+    L.spm_profile_pass.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_longlong)]
+    us, nbytes, cnt = C.c_double(), C.c_double(), C.c_longlong()
+    N.check(L.spm_profile_pass(run.h, K, C.byref(us), C.byref(nbytes), C.byref(cnt)), "spm_profile_pass")
+    gbs = nbytes.value / (us.value * 1e-6) / 1e9 if us.value > 0 else 0.0
+    return {"kernel": "fft_strided_kernel (X/Y passes)", "us": us.value, "bytes": nbytes.value, "gbs": gbs,
+            "launches": cnt.value}
+
+
+def accuracy_check(cfg, parts, steps):
+    from kapsel3_b200 import _native as N
+    from kapsel3_b200.spm import SPMRun
+    out = {}
+    res = {}
+    for prec in (N.SPM_PREC_FP64, N.SPM_PREC_FP32_MIXED):
+        with SPMRun(cfg, precision=prec) as run:
+            run.initialize(parts)
+            run.step(steps)
+            res[prec] = (run.velocity(), run.particles())
+    u64, p64 = res[N.SPM_PREC_FP64]
+    u32, p32 = res[N.SPM_PREC_FP32_MIXED]
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    out["steps"] = steps
+    out["rel_l2_u"] = rel(u32, u64)
+    for k in ("x", "v", "omega"):
+        out[f"rel_l2_{k}"] = rel(p32[k], p64[k])
+    out["meets_1e-5"] = out["rel_l2_u"] <= 1e-5
+    return out
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -168,6 +168,10 @@ int spm_row_complex(spm_ctx *ctx, int *hnzp);
 /* ---- measurement -------------------------------------------------------- */
 /* Times n steps with CUDA events on the context stream (ms total). */
 int spm_time_steps(spm_ctx *ctx, int nsteps, float *ms);
+/* Runs n steps with CUDA events around every strided (Y/X) FFT pass, the
+ * dominant kernel; returns its average duration (us), algorithmic bytes per
+ * launch (one read + one write of every transformed element) and count. */
+int spm_profile_pass(spm_ctx *ctx, int nsteps, double *avg_us, double *bytes_per_launch, long long *count);
 /* Launches of this library's kernels since the last reset. */
 int spm_kernel_launches(spm_ctx *ctx, long long *count, int reset);
 

@@ -87,6 +87,7 @@ _SIGS = {
     "spm_row_complex": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "spm_time_steps": (C.c_int, [_P, C.c_int, C.POINTER(C.c_float)]),
     "spm_kernel_launches": (C.c_int, [_P, C.POINTER(C.c_longlong), C.c_int]),
+    "spm_profile_pass": (C.c_int, [_P, C.c_int, _D, _D, C.POINTER(C.c_longlong)]),
 }
 
 

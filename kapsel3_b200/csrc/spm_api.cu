@@ -62,6 +62,10 @@ struct spm_ctx {
     long long    launches = 0;
     int          sm_count = 148;
     LEState      le{};
+    // optional CUDA-event timing of the strided FFT passes inside real steps
+    bool                     prof_on = false;
+    std::vector<cudaEvent_t> prof_ev;
+    double                   prof_bytes = 0.0;
 
     bool fp64() const { return P.precision == SPM_PREC_FP64; }
     template <typename T>
@@ -210,16 +214,41 @@ FFTPlan<float> &plan_of<float>(spm_ctx *c) {
     return c->plan32;
 }
 
-template <typename T>
-int fft_fwd(spm_ctx *c, int slot, int nf) {
-    SPM_CUDA_CHECK(plan_of<T>(c).forward(c->real<T>(slot), nf, c->fstride_c, c->st));
-    c->launches += 3;
+// Strided (Y/X) FFT pass, bracketed by CUDA events when profiling is on.
+template <typename T, int DIR>
+int fft_strided_pass(spm_ctx *c, int slot, int nf, int axis) {
+    if (c->prof_on) {
+        cudaEvent_t a, b;
+        SPM_CUDA_CHECK(cudaEventCreate(&a));
+        SPM_CUDA_CHECK(cudaEventCreate(&b));
+        SPM_CUDA_CHECK(cudaEventRecord(a, c->st));
+        SPM_CUDA_CHECK(plan_of<T>(c).template strided<DIR>(c->cx<T>(slot), nf, c->fstride_c, axis, c->st));
+        SPM_CUDA_CHECK(cudaEventRecord(b, c->st));
+        c->prof_ev.push_back(a);
+        c->prof_ev.push_back(b);
+        c->prof_bytes += 2.0 * nf * (double)c->g.nx * c->g.ny * c->g.hnz * sizeof(cplx<T>);
+    } else {
+        SPM_CUDA_CHECK(plan_of<T>(c).template strided<DIR>(c->cx<T>(slot), nf, c->fstride_c, axis, c->st));
+    }
+    c->launches++;
     return SPM_OK;
 }
 template <typename T>
+int fft_fwd(spm_ctx *c, int slot, int nf) {
+    SPM_CUDA_CHECK(plan_of<T>(c).z_r2c(c->real<T>(slot), c->cx<T>(slot), nf, 2 * c->fstride_c, c->fstride_c, c->st));
+    c->launches++;
+    int rc;
+    if ((rc = fft_strided_pass<T, -1>(c, slot, nf, 1)) != SPM_OK) return rc;
+    return fft_strided_pass<T, -1>(c, slot, nf, 0);
+}
+template <typename T>
 int fft_inv(spm_ctx *c, int slot, int nf) {
-    SPM_CUDA_CHECK(plan_of<T>(c).inverse(c->cx<T>(slot), nf, c->fstride_c, c->st));
-    c->launches += 3;
+    int rc;
+    if ((rc = fft_strided_pass<T, +1>(c, slot, nf, 0)) != SPM_OK) return rc;
+    if ((rc = fft_strided_pass<T, +1>(c, slot, nf, 1)) != SPM_OK) return rc;
+    SPM_CUDA_CHECK(plan_of<T>(c).z_c2r(c->cx<T>(slot), c->real<T>(slot), nf, c->fstride_c, 2 * c->fstride_c,
+                                       (T)(1.0 / ((double)c->g.nx * c->g.ny * c->g.nz)), c->st));
+    c->launches++;
     return SPM_OK;
 }
 
@@ -248,10 +277,16 @@ int zeta_to_velocity(spm_ctx *c, int truncate) {
 template <typename T>
 int ns_solver(spm_ctx *c) {
     int rc;
-    if ((rc = zeta_to_velocity<T>(c, 1)) != SPM_OK) return rc;
-    LAUNCH(c, r_advection_products<T>, c->grid_blocks(), 256, 0, c->g, c->real<T>(U0), c->real<T>(U1),
-           c->real<T>(U2), c->real<T>(A0), c->real<T>(A1));
-    if ((rc = fft_fwd<T>(c, U0, 5)) != SPM_OK) return rc;
+    // zeta -> u_hat (truncated) -> inverse x, y passes
+    LAUNCH(c, k_zeta_to_u<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(Z0), c->cx<T>(Z1), c->uk_dc, c->cx<T>(U0),
+           c->cx<T>(U1), c->cx<T>(U2), 1);
+    if ((rc = fft_strided_pass<T, +1>(c, U0, 3, 0)) != SPM_OK) return rc;
+    if ((rc = fft_strided_pass<T, +1>(c, U0, 3, 1)) != SPM_OK) return rc;
+    // inverse z + products + forward z in one pass, then forward y, x passes
+    SPM_CUDA_CHECK(plan_of<T>(c).z_products(c->cx<T>(U0), c->fstride_c, c->st));
+    c->launches++;
+    if ((rc = fft_strided_pass<T, -1>(c, U0, 5, 1)) != SPM_OK) return rc;
+    if ((rc = fft_strided_pass<T, -1>(c, U0, 5, 0)) != SPM_OK) return rc;
     LAUNCH(c, k_ns_update<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(Z0), c->cx<T>(Z1), c->cx<T>(U0),
            c->cx<T>(U1), c->cx<T>(U2), c->cx<T>(A0), c->cx<T>(A1), c->ph.nu, c->ph.dt);
     return SPM_OK;
@@ -276,9 +311,25 @@ int up_scatter(spm_ctx *c) {
     return SPM_OK;
 }
 
-// f = P_sole(up - phi u) into UP slots; u += f; zeta, uk_dc = U_k2zeta_k(FFT u)
+// Rigidity projection of the step: f = up - phi u formed inside the forward z
+// pass, forward y, x passes, then the projection and the update of zeta and
+// uk_dc closed in k space (k_project_add_curl).
 template <typename T>
 int rigidity_projection(spm_ctx *c) {
+    int rc;
+    SPM_CUDA_CHECK(plan_of<T>(c).z_makef(c->real<T>(UP0), c->real<T>(U0), c->real<T>(PHIS), c->fstride_c, c->st));
+    c->launches++;
+    if ((rc = fft_strided_pass<T, -1>(c, UP0, 3, 1)) != SPM_OK) return rc;
+    if ((rc = fft_strided_pass<T, -1>(c, UP0, 3, 0)) != SPM_OK) return rc;
+    LAUNCH(c, k_project_add_curl<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(UP0), c->cx<T>(UP1), c->cx<T>(UP2),
+           c->cx<T>(Z0), c->cx<T>(Z1), c->uk_dc);
+    return SPM_OK;
+}
+
+// The same projection in the reference's order (real-space f_sole, u += f,
+// forward transform of u, U_k2zeta_k); kept as the unfused reference path.
+template <typename T>
+int rigidity_projection_unfused(spm_ctx *c) {
     int rc;
     LAUNCH(c, r_make_f<T>, c->grid_blocks(), 256, 0, c->g, c->real<T>(UP0), c->real<T>(UP1), c->real<T>(UP2),
            c->real<T>(U0), c->real<T>(U1), c->real<T>(U2), c->real<T>(PHIS));
@@ -309,7 +360,7 @@ int step_ns(spm_ctx *c) {
         LAUNCH(c, s_hydro_force<T>, c->ph.np, 256, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
                c->ncells, c->real<T>(PHIS), c->real<T>(U0), c->real<T>(U1), c->real<T>(U2), c->ps.f_hydro,
                c->ps.torque_hydro);
-        LAUNCH(c, p_forces, particle_blocks(c), 128, 0, c->ph, c->ps, 0, 0.0);
+        LAUNCH(c, p_forces, (c->ph.np + 3) / 4, 128, 0, c->ph, c->ps, 0, 0.0);
         LAUNCH(c, p_velocity, particle_blocks(c), 128, 0, c->ph, c->ps, euler);
         if (c->P.kbt > 0.0) LAUNCH(c, p_thermostat_serial, 1, 32, 0, c->ph, c->ps, c->mt);
     }
@@ -719,6 +770,29 @@ int spm_time_steps(spm_ctx *c, int nsteps, float *ms) {
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (rc != SPM_OK) return rc;
+    return check_device_error(c);
+}
+
+int spm_profile_pass(spm_ctx *c, int nsteps, double *avg_us, double *bytes_per_launch, long long *count) {
+    if (!c || nsteps < 1 || !avg_us || !bytes_per_launch || !count) return fail(SPM_ERR_ARG, "bad argument");
+    c->prof_on    = true;
+    c->prof_bytes = 0.0;
+    int rc        = spm_step(c, nsteps);
+    c->prof_on    = false;
+    SPM_CUDA_CHECK(cudaStreamSynchronize(c->st));
+    double total = 0.0;
+    const size_t n = c->prof_ev.size() / 2;
+    for (size_t i = 0; i < n; i++) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->prof_ev[2 * i], c->prof_ev[2 * i + 1]);
+        total += ms;
+    }
+    for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
+    c->prof_ev.clear();
+    if (rc != SPM_OK) return rc;
+    *count            = (long long)n;
+    *avg_us           = n ? 1000.0 * total / (double)n : 0.0;
+    *bytes_per_launch = n ? c->prof_bytes / (double)n : 0.0;
     return check_device_error(c);
 }
 

@@ -83,51 +83,37 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
 }
 
 // ---------------------------------------------------------------------------
-// Z pass, forward: real rows -> complex rows.
-// in:  real row r at in + r*2*hnzp (2M reals used),   M = NZ/2
-// out: complex row r at out + r*hnzp (M+1 values, padding zeroed)
-// in and out may alias (same row footprint).
+// Z pass building blocks: one row of NZ = 2M reals <-> M+1 complex, handled
+// by P = Split<M>::N1 threads (t = 0..P-1) with a shared workspace row `s`.
+// Every thread of the CTA must call these together (they synchronise).
+//
+// r2c_row: ld(n) returns the packed pair (x[2n], x[2n+1]) for n < M;
+//          st(k, X) receives X[k] for k = 0..M.
+// c2r_row: ld(k) returns X[k] for k = 0..M (imaginary parts of X[0] and X[M]
+//          are discarded); st(n, z) receives z = (x[2n], x[2n+1]) * scale-
+//          normalised output.
 // ---------------------------------------------------------------------------
-template <typename T, int M, int R>
-__global__ void __launch_bounds__(R *Split<M>::N1)
-    fft_z_r2c_kernel(const T *in, cplx<T> *out, size_t field_stride_real, size_t field_stride_c, int nrows,
-                     int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN) {
+template <typename T, int M, class Ld, class St>
+__device__ __forceinline__ void r2c_row(int t, Ld ld, cplx<T> *s, const cplx<T> *__restrict__ twM,
+                                        const cplx<T> *__restrict__ twN, St st) {
     constexpr int M1 = Split<M>::N1;
     constexpr int M2 = Split<M>::N2;
     constexpr int P  = M1;
-    __shared__ __align__(16) cplx<T> s[R][M];
-    using V2 = typename vec2_of<T>::type;
-
-    const int r   = threadIdx.x / P;
-    const int t   = threadIdx.x % P;
-    const int row = blockIdx.x * R + r;
-    const bool ok = row < nrows;
-    const T *rin  = in + (size_t)blockIdx.y * field_stride_real + (size_t)row * 2 * hnzp;
-    cplx<T> *rout = out + (size_t)blockIdx.y * field_stride_c + (size_t)row * hnzp;
-
-    cplx<T> v[M2];
+    cplx<T>       v[M2];
 #pragma unroll
-    for (int m = 0; m < M2; m++) {
-        if (ok) {
-            V2 p = reinterpret_cast<const V2 *>(rin)[t + M1 * m];
-            v[m] = cplx<T>{p.x, p.y};
-        } else {
-            v[m] = cplx<T>{0, 0};
-        }
-    }
+    for (int m = 0; m < M2; m++) v[m] = ld(t + M1 * m);
     dft_reg<T, M2, -1>(v);
 #pragma unroll
     for (int k1 = 1; k1 < M2; k1++) v[k1] = cmul(v[k1], twM[(t * k1) & (M - 1)]);
 #pragma unroll
-    for (int k1 = 0; k1 < M2; k1++) s[r][t + M1 * k1] = v[k1];
+    for (int k1 = 0; k1 < M2; k1++) s[t + M1 * k1] = v[k1];
     __syncthreads();
-
     cplx<T> z[M2 / M1][M1];
 #pragma unroll
     for (int i = 0; i < M2 / M1; i++) {
         const int k1 = t + M1 * i;
 #pragma unroll
-        for (int n1 = 0; n1 < M1; n1++) z[i][n1] = s[r][n1 + M1 * k1];
+        for (int n1 = 0; n1 < M1; n1++) z[i][n1] = s[n1 + M1 * k1];
         dft_reg<T, M1, -1>(z[i]);
     }
     __syncthreads();
@@ -135,25 +121,123 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
     for (int i = 0; i < M2 / M1; i++) {
         const int k1 = t + M1 * i;
 #pragma unroll
-        for (int k2 = 0; k2 < M1; k2++) s[r][k1 + M2 * k2] = z[i][k2];
+        for (int k2 = 0; k2 < M1; k2++) s[k1 + M2 * k2] = z[i][k2];
     }
     __syncthreads();
-
-    if (ok) {
-        // X[k] = E[k] + W_N^k O[k],  E = (Z[k] + conj Z[M-k]) / 2,
-        // O = -i (Z[k] - conj Z[M-k]) / 2,  k = 0..M.
-        for (int k = t; k <= M; k += P) {
-            const cplx<T> zk  = s[r][k & (M - 1)];
-            const cplx<T> zmk = s[r][(M - k) & (M - 1)];
-            const T er = (T)0.5 * (zk.re + zmk.re);
-            const T ei = (T)0.5 * (zk.im - zmk.im);
-            const T orr = (T)0.5 * (zk.im + zmk.im);
-            const T oi  = (T)-0.5 * (zk.re - zmk.re);
-            const cplx<T> w = twN[k];  // e^{-2 pi i k / (2M)}, k = 0..M
-            rout[k] = cplx<T>{er + (w.re * orr - w.im * oi), ei + (w.re * oi + w.im * orr)};
-        }
-        for (int k = M + 1 + t; k < hnzp; k += P) rout[k] = cplx<T>{0, 0};
+    // X[k] = E[k] + W_N^k O[k],  E = (Z[k] + conj Z[M-k]) / 2,
+    // O = -i (Z[k] - conj Z[M-k]) / 2,  k = 0..M.
+    for (int k = t; k <= M; k += P) {
+        const cplx<T> zk  = s[k & (M - 1)];
+        const cplx<T> zmk = s[(M - k) & (M - 1)];
+        const T       er  = (T)0.5 * (zk.re + zmk.re);
+        const T       ei  = (T)0.5 * (zk.im - zmk.im);
+        const T       orr = (T)0.5 * (zk.im + zmk.im);
+        const T       oi  = (T)-0.5 * (zk.re - zmk.re);
+        const cplx<T> w   = twN[k];  // e^{-2 pi i k / (2M)}, k = 0..M
+        st(k, cplx<T>{er + (w.re * orr - w.im * oi), ei + (w.re * oi + w.im * orr)});
     }
+    __syncthreads();
+}
+
+template <typename T, int M, class Ld, class St>
+__device__ __forceinline__ void c2r_row(int t, Ld ld, cplx<T> *s, const cplx<T> *__restrict__ twM,
+                                        const cplx<T> *__restrict__ twN, T scale, St st) {
+    constexpr int M1 = Split<M>::N1;
+    constexpr int M2 = Split<M>::N2;
+    constexpr int P  = M1;
+    for (int k = t; k <= M; k += P) {
+        cplx<T> x = ld(k);
+        if (k == 0 || k == M) x.im = 0;
+        s[k] = x;
+    }
+    __syncthreads();
+    // Z'[k] = E' + i O',  E' = c (X[k] + conj X[M-k]),
+    // O' = c (X[k] - conj X[M-k]) W_N^{-k},  k = 0..M-1.
+    constexpr int KPT = M / P;
+    cplx<T>       zz[KPT];
+#pragma unroll
+    for (int i = 0; i < KPT; i++) {
+        const int     k   = t + P * i;
+        const cplx<T> xk  = s[k];
+        const cplx<T> xmk = s[M - k];
+        const T       er  = scale * (xk.re + xmk.re);
+        const T       ei  = scale * (xk.im - xmk.im);
+        const T       dr  = scale * (xk.re - xmk.re);
+        const T       di  = scale * (xk.im + xmk.im);
+        const cplx<T> w   = twN[k];
+        const T       orr = dr * w.re + di * w.im;
+        const T       oi  = di * w.re - dr * w.im;
+        zz[i]             = cplx<T>{er - oi, ei + orr};
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < KPT; i++) s[t + P * i] = zz[i];
+    __syncthreads();
+    cplx<T> v[M2];
+#pragma unroll
+    for (int m = 0; m < M2; m++) v[m] = s[t + M1 * m];
+    dft_reg<T, M2, +1>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < M2; k1++) {
+        cplx<T> w = twM[(t * k1) & (M - 1)];
+        w.im      = -w.im;
+        v[k1]     = cmul(v[k1], w);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < M2; k1++) s[t + M1 * k1] = v[k1];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < M2 / M1; i++) {
+        const int k1 = t + M1 * i;
+        cplx<T>   u[M1];
+#pragma unroll
+        for (int n1 = 0; n1 < M1; n1++) u[n1] = s[n1 + M1 * k1];
+        dft_reg<T, M1, +1>(u);
+#pragma unroll
+        for (int k2 = 0; k2 < M1; k2++) st(k1 + M2 * k2, u[k2]);
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__device__ __forceinline__ cplx<T> load_pair(const T *row, int n) {
+    using V2   = typename vec2_of<T>::type;
+    const V2 p = reinterpret_cast<const V2 *>(row)[n];
+    return cplx<T>{p.x, p.y};
+}
+template <typename T>
+__device__ __forceinline__ void store_pair(T *row, int n, cplx<T> z) {
+    using V2 = typename vec2_of<T>::type;
+    V2 p;
+    p.x                             = z.re;
+    p.y                             = z.im;
+    reinterpret_cast<V2 *>(row)[n] = p;
+}
+
+// ---------------------------------------------------------------------------
+// Z pass, forward: real rows -> complex rows (in and out may alias).
+// in:  real row r at in + r*2*hnzp (2M reals used),   M = NZ/2
+// out: complex row r at out + r*hnzp (M+1 values, padding zeroed)
+// ---------------------------------------------------------------------------
+template <typename T, int M, int R>
+__global__ void __launch_bounds__(R *Split<M>::N1)
+    fft_z_r2c_kernel(const T *in, cplx<T> *out, size_t field_stride_real, size_t field_stride_c, int nrows,
+                     int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN) {
+    constexpr int P = Split<M>::N1;
+    __shared__ __align__(16) cplx<T> s[R][M];
+    const int r   = threadIdx.x / P;
+    const int t   = threadIdx.x % P;
+    const int row = blockIdx.x * R + r;
+    const bool ok = row < nrows;
+    const T *rin  = in + (size_t)blockIdx.y * field_stride_real + (size_t)(ok ? row : 0) * 2 * hnzp;
+    cplx<T> *rout = out + (size_t)blockIdx.y * field_stride_c + (size_t)(ok ? row : 0) * hnzp;
+    r2c_row<T, M>(
+        t, [&](int n) { return ok ? load_pair<T>(rin, n) : cplx<T>{0, 0}; }, s[r], twM, twN,
+        [&](int k, cplx<T> X) {
+            if (ok) rout[k] = X;
+        });
+    if (ok)
+        for (int k = M + 1 + t; k < hnzp; k += P) rout[k] = cplx<T>{0, 0};
 }
 
 // ---------------------------------------------------------------------------
@@ -163,81 +247,115 @@ template <typename T, int M, int R>
 __global__ void __launch_bounds__(R *Split<M>::N1)
     fft_z_c2r_kernel(const cplx<T> *in, T *out, size_t field_stride_c, size_t field_stride_real, int nrows,
                      int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale) {
-    constexpr int M1 = Split<M>::N1;
-    constexpr int M2 = Split<M>::N2;
-    constexpr int P  = M1;
+    constexpr int P = Split<M>::N1;
     __shared__ __align__(16) cplx<T> s[R][M + 1];
-    using V2 = typename vec2_of<T>::type;
-
     const int r   = threadIdx.x / P;
     const int t   = threadIdx.x % P;
     const int row = blockIdx.x * R + r;
     const bool ok = row < nrows;
-    const cplx<T> *rin = in + (size_t)blockIdx.y * field_stride_c + (size_t)row * hnzp;
-    T *rout            = out + (size_t)blockIdx.y * field_stride_real + (size_t)row * 2 * hnzp;
-
-    for (int k = t; k <= M; k += P) {
-        cplx<T> x = ok ? rin[k] : cplx<T>{0, 0};
-        if (k == 0 || k == M) x.im = 0;
-        s[r][k] = x;
-    }
-    __syncthreads();
-    // Z'[k] = E' + i O',  E' = c (X[k] + conj X[M-k]),
-    // O' = c (X[k] - conj X[M-k]) W_N^{-k},  k = 0..M-1.
-    constexpr int KPT = M / P;
-    cplx<T>       zz[KPT];
-#pragma unroll
-    for (int i = 0; i < KPT; i++) {
-        const int k = t + P * i;
-        const cplx<T> xk  = s[r][k];
-        const cplx<T> xmk = s[r][M - k];
-        const T er = scale * (xk.re + xmk.re);
-        const T ei = scale * (xk.im - xmk.im);
-        const T dr = scale * (xk.re - xmk.re);
-        const T di = scale * (xk.im + xmk.im);
-        const cplx<T> w = twN[k];  // e^{-2 pi i k/N}; use its conjugate
-        const T orr = dr * w.re + di * w.im;
-        const T oi  = di * w.re - dr * w.im;
-        zz[i] = cplx<T>{er - oi, ei + orr};
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < KPT; i++) s[r][t + P * i] = zz[i];
-    __syncthreads();
-
-    cplx<T> v[M2];
-#pragma unroll
-    for (int m = 0; m < M2; m++) v[m] = s[r][t + M1 * m];
-    dft_reg<T, M2, +1>(v);
-#pragma unroll
-    for (int k1 = 1; k1 < M2; k1++) {
-        cplx<T> w = twM[(t * k1) & (M - 1)];
-        w.im      = -w.im;
-        v[k1]     = cmul(v[k1], w);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k1 = 0; k1 < M2; k1++) s[r][t + M1 * k1] = v[k1];
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < M2 / M1; i++) {
-        const int k1 = t + M1 * i;
-        cplx<T>   u[M1];
-#pragma unroll
-        for (int n1 = 0; n1 < M1; n1++) u[n1] = s[r][n1 + M1 * k1];
-        dft_reg<T, M1, +1>(u);
-        if (ok) {
-#pragma unroll
-            for (int k2 = 0; k2 < M1; k2++) {
-                V2 p;
-                p.x = u[k2].re;
-                p.y = u[k2].im;
-                reinterpret_cast<V2 *>(rout)[k1 + M2 * k2] = p;
-            }
-        }
-    }
-    if (ok && t == 0) {
+    const cplx<T> *rin = in + (size_t)blockIdx.y * field_stride_c + (size_t)(ok ? row : 0) * hnzp;
+    T *rout            = out + (size_t)blockIdx.y * field_stride_real + (size_t)(ok ? row : 0) * 2 * hnzp;
+    c2r_row<T, M>(
+        t, [&](int k) { return ok ? rin[k] : cplx<T>{0, 0}; }, s[r], twM, twN, scale,
+        [&](int n, cplx<T> z) {
+            if (ok) store_pair<T>(rout, n, z);
+        });
+    if (ok && t == 0)
         for (int k = 2 * M; k < 2 * hnzp; k++) rout[k] = (T)0;
+}
+
+// ---------------------------------------------------------------------------
+// Fused Z pass of the advection term (U2advection_k, operate_omega.cxx:12-55):
+// inverse z transform of the three velocity components, the five quadratic
+// products in registers/shared memory, forward z transform of the products.
+// io[0..2] hold u_hat (z-complex rows) on input; io[0..4] receive the
+// z-transformed products u2u3, u3u1, u1u2, (u2-u3)(u2+u3), (u3-u1)(u3+u1).
+// ---------------------------------------------------------------------------
+template <typename T, int M, int R>
+__global__ void __launch_bounds__(R *Split<M>::N1)
+    fft_z_products_kernel(cplx<T> *io, size_t field_stride_c, int nrows, int hnzp,
+                          const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale) {
+    constexpr int P = Split<M>::N1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T       *U  = reinterpret_cast<T *>(smem_raw);                   // [3][R][2M]
+    cplx<T> *ws = reinterpret_cast<cplx<T> *>(U + 3 * R * 2 * M);     // [R][M+1]
+    const int r   = threadIdx.x / P;
+    const int t   = threadIdx.x % P;
+    const int row = blockIdx.x * R + r;
+    const bool ok = row < nrows;
+    const size_t roff = (size_t)(ok ? row : 0) * hnzp;
+    T *Ur[3] = {U + (0 * R + r) * 2 * M, U + (1 * R + r) * 2 * M, U + (2 * R + r) * 2 * M};
+#pragma unroll 1
+    for (int d = 0; d < 3; d++) {
+        const cplx<T> *rin = io + d * field_stride_c + roff;
+        T             *ur  = Ur[d];
+        c2r_row<T, M>(
+            t, [&](int k) { return ok ? rin[k] : cplx<T>{0, 0}; }, ws + r * (M + 1), twM, twN, scale,
+            [&](int n, cplx<T> z) {
+                ur[2 * n]     = z.re;
+                ur[2 * n + 1] = z.im;
+            });
+    }
+#pragma unroll 1
+    for (int p = 0; p < 5; p++) {
+        cplx<T> *rout = io + p * field_stride_c + roff;
+        r2c_row<T, M>(
+            t,
+            [&](int n) {
+                T o[2];
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const T x = Ur[0][2 * n + e], y = Ur[1][2 * n + e], z = Ur[2][2 * n + e];
+                    o[e] = p == 0 ? y * z : p == 1 ? z * x : p == 2 ? x * y : p == 3 ? (y - z) * (y + z)
+                                                                                     : (z - x) * (z + x);
+                }
+                return cplx<T>{o[0], o[1]};
+            },
+            ws + r * (M + 1), twM, twN,
+            [&](int k, cplx<T> X) {
+                if (ok) rout[k] = X;
+            });
+        if (ok)
+            for (int k = M + 1 + t; k < hnzp; k += P) rout[k] = cplx<T>{0, 0};
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused Z pass of the rigidity force (Make_f_particle_dt_nonsole,
+// f_particle.h:35-54): f = up - min(phi_sum, 1) u formed on the fly and
+// transformed forward.  up[0..2] (real rows) are overwritten by f_hat rows.
+// ---------------------------------------------------------------------------
+template <typename T, int M, int R>
+__global__ void __launch_bounds__(R *Split<M>::N1)
+    fft_z_makef_kernel(T *up, const T *__restrict__ u, const T *__restrict__ phi_sum, size_t field_stride_c,
+                       int nrows, int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN) {
+    constexpr int P = Split<M>::N1;
+    __shared__ __align__(16) cplx<T> s[R][M];
+    const int r   = threadIdx.x / P;
+    const int t   = threadIdx.x % P;
+    const int row = blockIdx.x * R + r;
+    const bool ok = row < nrows;
+    const size_t roff = (size_t)(ok ? row : 0) * 2 * hnzp;
+    const T *ph = phi_sum + roff;
+#pragma unroll 1
+    for (int d = 0; d < 3; d++) {
+        T       *upr = up + 2 * d * field_stride_c + roff;
+        const T *ur  = u + 2 * d * field_stride_c + roff;
+        cplx<T> *out = reinterpret_cast<cplx<T> *>(upr);
+        r2c_row<T, M>(
+            t,
+            [&](int n) {
+                if (!ok) return cplx<T>{0, 0};
+                const cplx<T> a = load_pair<T>(upr, n), b = load_pair<T>(ur, n), f = load_pair<T>(ph, n);
+                const T       f0 = f.re < (T)1 ? f.re : (T)1, f1 = f.im < (T)1 ? f.im : (T)1;
+                return cplx<T>{a.re - f0 * b.re, a.im - f1 * b.im};
+            },
+            s[r], twM, twN,
+            [&](int k, cplx<T> X) {
+                if (ok) out[k] = X;
+            });
+        if (ok)
+            for (int k = M + 1 + t; k < hnzp; k += P) out[k] = cplx<T>{0, 0};
     }
 }
 

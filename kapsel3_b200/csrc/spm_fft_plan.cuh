@@ -23,7 +23,50 @@ struct FFTPlan {
         return (int)(32768 / (m * sizeof(cplx<T>))) >= 16 ? 16 : (int)(32768 / (m * sizeof(cplx<T>)));
     }
 
+    // rows per CTA of the fused products kernel (three real rows + workspace
+    // per row, kept within 64 KB of dynamic shared memory)
+    static constexpr int prows(int m) {
+        return (int)(65536 / (8 * m * sizeof(T))) >= 16 ? 16 : (int)(65536 / (8 * m * sizeof(T)));
+    }
+    static constexpr size_t psmem(int m) {
+        return (size_t)prows(m) * (3 * 2 * m * sizeof(T) + (m + 1) * sizeof(cplx<T>));
+    }
+
     static bool size_ok(int n) { return n >= 8 && n <= 512 && (n & (n - 1)) == 0; }
+
+    // Fused inverse-z / advection products / forward-z pass over five slots.
+    cudaError_t z_products(cplx<T> *io, size_t fs_c, cudaStream_t st) const {
+        const int nrows = g.nx * g.ny;
+        const T   scale = (T)(1.0 / ((double)g.nx * g.ny * g.nz));
+        switch (g.nz / 2) {
+#define SPM_ZP(MM)                                                                                        \
+    case MM: {                                                                                            \
+        constexpr int RR = prows(MM);                                                                     \
+        fft_z_products_kernel<T, MM, RR><<<(nrows + RR - 1) / RR, RR * Split<MM>::N1, psmem(MM), st>>>( \
+            io, fs_c, nrows, g.hnzp, tw_zm, tw_zn, scale);                                                \
+    } break;
+            SPM_ZP(4) SPM_ZP(8) SPM_ZP(16) SPM_ZP(32) SPM_ZP(64) SPM_ZP(128) SPM_ZP(256)
+#undef SPM_ZP
+            default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
+    // Fused f = up - min(phi_sum,1) u and forward z pass (three fields).
+    cudaError_t z_makef(T *up, const T *u, const T *phis, size_t fs_c, cudaStream_t st) const {
+        const int nrows = g.nx * g.ny;
+        switch (g.nz / 2) {
+#define SPM_ZF(MM)                                                                                    \
+    case MM: {                                                                                        \
+        constexpr int RR = zrows(MM);                                                                 \
+        fft_z_makef_kernel<T, MM, RR><<<(nrows + RR - 1) / RR, RR * Split<MM>::N1, 0, st>>>(          \
+            up, u, phis, fs_c, nrows, g.hnzp, tw_zm, tw_zn);                                          \
+    } break;
+            SPM_ZF(4) SPM_ZF(8) SPM_ZF(16) SPM_ZF(32) SPM_ZF(64) SPM_ZF(128) SPM_ZF(256)
+#undef SPM_ZF
+            default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
 
     cudaError_t create(const Grid &grid) {
         g = grid;
@@ -129,8 +172,17 @@ struct FFTPlan {
         return cudaFuncSetAttribute(fft_strided_kernel<T, NN, W, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)(NN * W * sizeof(cplx<T>)));
     }
+    template <int MM>
+    static cudaError_t attr_products() {
+        return cudaFuncSetAttribute(fft_z_products_kernel<T, MM, prows(MM)>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem(MM));
+    }
     static cudaError_t set_smem_attrs() {
         cudaError_t e = cudaSuccess;
+#define SPM_PATTR(MM) \
+    if ((e = attr_products<MM>()) != cudaSuccess) return e;
+        SPM_PATTR(4) SPM_PATTR(8) SPM_PATTR(16) SPM_PATTR(32) SPM_PATTR(64) SPM_PATTR(128) SPM_PATTR(256)
+#undef SPM_PATTR
 #define SPM_ATTR(NN)                                               \
     if ((e = attr_one<NN, -1>()) != cudaSuccess) return e;          \
     if ((e = attr_one<NN, +1>()) != cudaSuccess) return e;

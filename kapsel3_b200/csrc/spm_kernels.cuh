@@ -280,6 +280,61 @@ __global__ void k_u_to_zeta(Grid g, const cplx<T> *__restrict__ u0, const cplx<T
 }
 
 // ---------------------------------------------------------------------------
+// Rigidity projection closed in k space.  The reference forms u_real + f_sole
+// in real space and transforms it (Make_f_particle_dt_sole, Add_f_particle,
+// U2zeta_k; sp_3d_ns.cxx:172-192, f_particle.h:60-84, operate_omega.h:208).
+// Because u_real is the inverse transform of the truncated u_hat rebuilt from
+// zeta, the same zeta follows pointwise from
+//   u_hat_new = Zeta_k2u_k(zeta) + P T f_hat,  zeta_new = U_k2zeta_k(u_hat_new)
+// which skips three inverse and three forward transforms.  uk_dc (the k = 0
+// mode, not touched by the projection) is updated in FP64:
+//   uk_dc += Re f_hat(0).
+// Modes outside the 2/3 box come out exactly zero (the reference leaves
+// round-off there, which its next step truncates before use).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_project_add_curl(Grid g, const cplx<T> *__restrict__ f0p, const cplx<T> *__restrict__ f1p,
+                                   const cplx<T> *__restrict__ f2p, cplx<T> *__restrict__ z0p,
+                                   cplx<T> *__restrict__ z1p, double *__restrict__ uk_dc) {
+    const size_t n = g.field_elems_c();
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        KPoint p;
+        size_t row;
+        if (!k_point(g, idx, p, row) || !p.keep) {
+            z0p[idx] = z1p[idx] = cplx<T>{0, 0};
+            continue;
+        }
+        if (idx == 0) {
+            uk_dc[0] += (double)f0p[0].re;
+            uk_dc[1] += (double)f1p[0].re;
+            uk_dc[2] += (double)f2p[0].re;
+            z0p[0] = z1p[0] = cplx<T>{0, 0};
+            continue;
+        }
+        const T kx = (T)p.kx, ky = (T)p.ky, kz = (T)p.kz, ik2 = ik2_of<T>(p);
+        cplx<T> f[3] = {f0p[idx], f1p[idx], f2p[idx]};
+        const T dr = ik2 * (f[0].re * kx + f[1].re * ky + f[2].re * kz);
+        const T di = ik2 * (f[0].im * kx + f[1].im * ky + f[2].im * kz);
+        f[0].re -= dr * kx;
+        f[0].im -= di * kx;
+        f[1].re -= dr * ky;
+        f[1].im -= di * ky;
+        f[2].re -= dr * kz;
+        f[2].im -= di * kz;
+        cplx<T> om[3], u[3];
+        zeta_to_omega<T>(p, z0p[idx], z1p[idx], om);
+        i_cross<T>(kx * ik2, ky * ik2, kz * ik2, om, u);
+#pragma unroll
+        for (int d = 0; d < 3; d++) u[d] = cadd(u[d], f[d]);
+        i_cross<T>(kx, ky, kz, u, om);
+        cplx<T> a, b;
+        omega_to_zeta<T>(p, om, a, b);
+        z0p[idx] = a;
+        z1p[idx] = b;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Real-space field updates.
 // f = up - min(phi_sum, 1) u   (Make_f_particle_dt_nonsole, f_particle.h:35-54)
 // written in place over up.
@@ -612,17 +667,19 @@ __device__ __forceinline__ double min_image(const Phys &ph, const double *xa, co
 // multiplicity, so no atomics are needed.  lj_stress[n] receives particle n's
 // share of sum f_x r_y over the pairs where it is the higher index, as the
 // reference accumulates dev_shear_stress_lj.
+// One warp per particle: lanes stride over the partners, then a warp sum.
 __global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int n    = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (n >= ph.np) return;
     double f[3]   = {0.0, 0.0, 0.0};
     double stress = 0.0;
     if (ph.lj_on) {
-        for (int m = 0; m < ph.np; m++) {
+        for (int m = lane; m < ph.np; m += 32) {
             if (m == n) continue;
-            const int     hi = n > m ? n : m, lo = n > m ? m : n;
-            double        r[3], rr;  // r = x_other - x_n (with the periodic image rule)
-            int           mult = 1;
+            const int hi = n > m ? n : m, lo = n > m ? m : n;
+            double    r[3], rr;  // r = x_other - x_n (with the periodic image rule)
+            int       mult = 1;
             if (all_pairs_le) {
                 // O(N^2) loop with Distance0_OBL(x_lo, x_hi) (md_force.cxx:198-304,
                 // interaction.h:50-72): y image first, then the x shift of the
@@ -638,7 +695,7 @@ __global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift) {
                 x12 -= (double)nint_d(x12 / ph.L[0]) * ph.L[0];
                 double z12 = x2[2] - x1[2];
                 z12 -= (double)nint_d(z12 / ph.L[2]) * ph.L[2];
-                rr = sqrt(y12 * y12 + x12 * x12 + z12 * z12);
+                rr              = sqrt(y12 * y12 + x12 * x12 + z12 * z12);
                 const double sg = (n == lo) ? 1.0 : -1.0;
                 r[0]            = sg * x12;
                 r[1]            = sg * y12;
@@ -660,8 +717,17 @@ __global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift) {
             if (n == hi) stress += (double)mult * (-dmy_r * r[0]) * r[1];
         }
     }
-    for (int d = 0; d < 3; d++) s.fr[3 * n + d] += f[d] + ph.body_force[d];
-    s.lj_stress[n] = stress;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        f[0] += __shfl_xor_sync(0xffffffffu, f[0], o);
+        f[1] += __shfl_xor_sync(0xffffffffu, f[1], o);
+        f[2] += __shfl_xor_sync(0xffffffffu, f[2], o);
+        stress += __shfl_xor_sync(0xffffffffu, stress, o);
+    }
+    if (lane == 0) {
+        for (int d = 0; d < 3; d++) s.fr[3 * n + d] += f[d] + ph.body_force[d];
+        s.lj_stress[n] = stress;
+    }
 }
 
 // MD_solver_velocity_Euler / _AB2_hydro (particle_solver.cxx:103-142,

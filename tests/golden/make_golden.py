@@ -1,0 +1,107 @@
+"""Generates the golden fixtures of tests/golden/ by running the reference
+program itself (oracle/_ref, built from the unmodified KAPSEL sources by
+oracle/ref_build/Makefile) on seeded inputs.
+
+    python tests/golden/make_golden.py
+
+Each fixture stores the run's UDF-level description (SPMConfig fields + the
+seeded initial particle state) and, for every step, the particle state the
+reference dumped (x, v, omega, q, f_hydro_previous, torque_hydro_previous),
+plus at a few steps the retained (2/3-rule) modes of zeta, uk_dc and
+checksums of the velocity field.  Only this script reads the reference; the
+tests read the .npz files.
+"""
+from __future__ import annotations
+
+import dataclasses
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from kapsel3_b200.udf import SPMConfig, make_particles, write_udf_keys  # noqa: E402
+from oracle import ref_runner  # noqa: E402
+
+CASES = {
+    # C1 of the benchmark plan: 32^3, two spheres a=4, body force 1e-3 along x
+    "c1_32_two_spheres_body_force": dict(
+        cfg=dict(npx=5, npy=5, npz=5, n_particles=2, a=4.0, a_xi=2.0, dt=0.05, body_force=(1e-3, 0.0, 0.0),
+                 num_snap=100),
+        init=dict(seed=1, v_sd=0.0, random_orientation=False), field_steps=(1, 100)),
+    # thermostat (MT19937 + polar Box-Muller) with random orientations
+    "thermostat_32_four_spheres": dict(
+        cfg=dict(npx=5, npy=5, npz=5, n_particles=4, a=4.0, a_xi=2.0, dt=0.05, kbt=1e-4, num_snap=40),
+        init=dict(seed=7, v_sd=1e-3, random_orientation=True), field_steps=(40,)),
+    # non-cubic grid, lc = 1 on y (LJ pair multiplicity 3 per axis), close pairs
+    "noncubic_lj_multiplicity": dict(
+        cfg=dict(npx=5, npy=4, npz=6, n_particles=5, a=3.0, a_xi=2.0, dt=0.05, kbt=1e-5,
+                 body_force=(0.0, 2e-3, -1e-3), num_snap=30),
+        init=dict(seed=5, v_sd=2e-3, random_orientation=True, min_dist_factor=0.92), field_steps=(30,)),
+}
+
+
+def retained_modes(cfg: SPMConfig, zeta: np.ndarray) -> np.ndarray:
+    d = cfg.derived()
+    nx, ny, nz = cfg.shape
+    kx = np.arange(nx)
+    kx = np.where(kx > nx // 2, kx - nx, kx)
+    ky = np.arange(ny)
+    ky = np.where(ky > ny // 2, ky - ny, ky)
+    ix = np.where(np.abs(kx) < d["TRN_X"])[0]
+    iy = np.where(np.abs(ky) < d["TRN_Y"])[0]
+    return zeta[:, ix][:, :, iy][:, :, :, :d["TRN_Z"]]
+
+
+def make_case(name, spec):
+    cfg = SPMConfig(**spec["cfg"])
+    init = dict(spec["init"])
+    parts = make_particles(cfg, **init)
+    with tempfile.TemporaryDirectory() as td:
+        keys = os.path.join(td, "run.keys")
+        dump = os.path.join(td, "run.dump")
+        write_udf_keys(keys, cfg, parts, out_dir=os.path.join(td, "avs"))
+        ref_runner.run_reference(keys, dump_path=dump, fields_every=1, body_force=cfg.body_force)
+        d = ref_runner.read_dump(dump)
+    frames = d["frames"]
+    out = {"config_json": np.array(json.dumps(dataclasses.asdict(cfg))),
+           "init_json": np.array(json.dumps(init))}
+    for k in ("x", "v", "omega"):
+        out["init_" + k] = parts[k]
+    out["init_q"] = parts["q"]
+    for k in ("x", "x_nopbc", "v", "omega", "q", "f_hydro_previous", "torque_hydro_previous", "fr_previous"):
+        out["traj_" + k] = np.stack([f[k] for f in frames])
+    out["traj_uk_dc"] = np.stack([f["uk_dc"] for f in frames])
+    out["traj_ts"] = np.array([f["ts"] for f in frames])
+    fs = [s for s in spec["field_steps"] if s < len(frames)]
+    out["field_steps"] = np.array(fs)
+    for s in fs:
+        f = frames[s]
+        out[f"zeta_retained_{s}"] = retained_modes(cfg, f["zeta"])
+        u = f["u"]
+        out[f"u_checksums_{s}"] = np.array([np.sum(u[c]) for c in range(3)] +
+                                           [np.sum(u[c] ** 2) for c in range(3)] +
+                                           [np.abs(u).max()])
+        out[f"u_plane_{s}"] = u[:, :, :, 0].copy()       # z = 0 plane of every component
+        out[f"phi_plane_{s}"] = f["phi"][:, :, 0].copy()
+        out[f"phi_sum_{s}"] = np.array(f["phi"].sum())
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **out)
+    print(f"{path}: {os.path.getsize(path)} bytes, {len(frames)} frames")
+
+
+def main():
+    if not ref_runner.available():
+        raise SystemExit("build the reference first: make -C oracle/ref_build")
+    names = sys.argv[1:] or sorted(CASES)
+    for n in names:
+        make_case(n, CASES[n])
+
+
+if __name__ == "__main__":
+    main()
