@@ -66,6 +66,7 @@ struct spm_ctx {
     bool                     prof_on = false;
     std::vector<cudaEvent_t> prof_ev;
     double                   prof_bytes = 0.0;
+    bool                     use_tma    = true;  // SPM_NO_TMA=1 selects the direct-load passes
 
     bool fp64() const { return P.precision == SPM_PREC_FP64; }
     template <typename T>
@@ -214,6 +215,17 @@ FFTPlan<float> &plan_of<float>(spm_ctx *c) {
     return c->plan32;
 }
 
+// Strided (Y/X) FFT pass: the persistent TMA kernel when it applies, else the
+// direct-load kernel.
+template <typename T, int DIR>
+cudaError_t strided_dispatch(spm_ctx *c, int slot, int nf, int axis) {
+    if (c->use_tma) {
+        cudaError_t e = plan_of<T>(c).template strided_tma<DIR>(c->cx<T>(slot), nf, c->fstride_c, axis, c->st);
+        if (e != cudaErrorNotSupported) return e;
+    }
+    return plan_of<T>(c).template strided<DIR>(c->cx<T>(slot), nf, c->fstride_c, axis, c->st);
+}
+
 // Strided (Y/X) FFT pass, bracketed by CUDA events when profiling is on.
 template <typename T, int DIR>
 int fft_strided_pass(spm_ctx *c, int slot, int nf, int axis) {
@@ -222,13 +234,13 @@ int fft_strided_pass(spm_ctx *c, int slot, int nf, int axis) {
         SPM_CUDA_CHECK(cudaEventCreate(&a));
         SPM_CUDA_CHECK(cudaEventCreate(&b));
         SPM_CUDA_CHECK(cudaEventRecord(a, c->st));
-        SPM_CUDA_CHECK(plan_of<T>(c).template strided<DIR>(c->cx<T>(slot), nf, c->fstride_c, axis, c->st));
+        SPM_CUDA_CHECK((strided_dispatch<T, DIR>(c, slot, nf, axis)));
         SPM_CUDA_CHECK(cudaEventRecord(b, c->st));
         c->prof_ev.push_back(a);
         c->prof_ev.push_back(b);
         c->prof_bytes += 2.0 * nf * (double)c->g.nx * c->g.ny * c->g.hnz * sizeof(cplx<T>);
     } else {
-        SPM_CUDA_CHECK(plan_of<T>(c).template strided<DIR>(c->cx<T>(slot), nf, c->fstride_c, axis, c->st));
+        SPM_CUDA_CHECK((strided_dispatch<T, DIR>(c, slot, nf, axis)));
     }
     c->launches++;
     return SPM_OK;
@@ -569,6 +581,11 @@ int spm_create(const spm_params *p, void *stream, spm_ctx **out) {
         return fail(SPM_ERR_NOMEM, std::string("field arena: ") + cudaGetErrorString(e));
     }
     e = c->fp64() ? c->plan64.create(c->g) : c->plan32.create(c->g);
+    c->plan64.sm_count = c->plan32.sm_count = c->sm_count;
+    {
+        const char *nt = getenv("SPM_NO_TMA");
+        c->use_tma     = !(nt && nt[0] == '1');
+    }
     if (e != cudaSuccess) {
         spm_destroy(c);
         return fail(SPM_ERR_CUDA, std::string("FFT plan: ") + cudaGetErrorString(e));
@@ -584,6 +601,7 @@ int spm_create(const spm_params *p, void *stream, spm_ctx **out) {
         spm_destroy(c);
         return fail(SPM_ERR_NOMEM, "small device buffers");
     }
+    c->plan64.err = c->plan32.err = c->err;
     cudaMemcpy(c->cells, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemset(c->err, 0, sizeof(unsigned int));
     cudaMemset(c->pbuf, 0, (size_t)np * kPWords * sizeof(double));

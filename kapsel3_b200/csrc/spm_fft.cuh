@@ -22,6 +22,7 @@
 #pragma once
 
 #include "spm_dft.cuh"
+#include "spm_tma.cuh"
 
 namespace spm {
 
@@ -36,7 +37,7 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
                        size_t outer_stride, size_t axis_stride, const cplx<T> *__restrict__ twN) {
     constexpr int N1 = Split<N>::N1;
     constexpr int N2 = Split<N>::N2;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     cplx<T> *s = reinterpret_cast<cplx<T> *>(smem_raw);
 
     const int c   = threadIdx.x % W;
@@ -80,6 +81,119 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
             for (int k2 = 0; k2 < N1; k2++) base[(size_t)(k1 + N2 * k2) * axis_stride] = u[k2];
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Strided complex pass, persistent and TMA-pipelined.
+// The field is a 4D tensor of T: {2*hnz (kz re/im), NY, NX, nfields}.  A tile
+// is W kz-columns x N lines (box {2W, N, 1, 1} on the Y pass, {2W, 1, N, 1}
+// on the X pass); in shared memory both arrive as [n][W] complex.  Each CTA
+// walks its tiles through an S-deep ring of buffers: TMA loads run S-1 tiles
+// ahead of the four-step FFT, results go back with TMA stores from the same
+// buffer.  Columns >= hnz are outside the tensor: loads zero-fill them and
+// stores clip them.
+// ---------------------------------------------------------------------------
+template <typename T, int N, int W, int DIR, int S>
+__global__ void __launch_bounds__(W *Split<N>::N1)
+    fft_strided_tma_kernel(const __grid_constant__ CUtensorMap map, int axis, int n_outer, int col_tiles,
+                           int ntiles, const cplx<T> *__restrict__ twN, unsigned int *err) {
+    constexpr int      N1         = Split<N>::N1;
+    constexpr int      N2         = Split<N>::N2;
+    constexpr unsigned tile_bytes = N * W * sizeof(cplx<T>);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    cplx<T>           *buf = reinterpret_cast<cplx<T> *>(smem_raw);
+    __shared__ __align__(8) uint64_t full[S];
+
+    const int tid = threadIdx.x;
+    const int c   = tid % W;
+    const int g   = tid / W;
+    auto coords = [&](int t, int &c0, int &c1, int &c2, int &c3) {
+        const int ct = t % col_tiles, rest = t / col_tiles;
+        const int o = rest % n_outer, f = rest / n_outer;
+        c0 = 2 * ct * W;
+        c3 = f;
+        if (axis == 1) {
+            c1 = 0;
+            c2 = o;
+        } else {
+            c1 = o;
+            c2 = 0;
+        }
+    };
+    if (tid == 0) {
+        for (int b = 0; b < S; b++) mbar_init(&full[b], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int b = 0; b < S; b++) {
+            const int t = blockIdx.x + b * gridDim.x;
+            if (t < ntiles) {
+                int c0, c1, c2, c3;
+                coords(t, c0, c1, c2, c3);
+                mbar_expect_tx(&full[b], tile_bytes);
+                tma_load_4d(buf + (size_t)b * N * W, &map, c0, c1, c2, c3, &full[b]);
+            }
+        }
+    }
+    int it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+        const int b  = it % S;
+        cplx<T>  *B  = buf + (size_t)b * N * W;
+        const bool w = mbar_wait(&full[b], (unsigned)((it / S) & 1), err);
+        if (!__syncthreads_and(w)) break;
+        // step 1: N2-point DFTs over n2 for n1 = g, in place
+        cplx<T> v[N2];
+#pragma unroll
+        for (int m = 0; m < N2; m++) v[m] = B[(g + N1 * m) * W + c];
+        dft_reg<T, N2, DIR>(v);
+#pragma unroll
+        for (int k1 = 1; k1 < N2; k1++) {
+            cplx<T> tw = twN[(g * k1) & (N - 1)];
+            if (DIR > 0) tw.im = -tw.im;
+            v[k1] = cmul(v[k1], tw);
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < N2; k1++) B[(g + N1 * k1) * W + c] = v[k1];
+        __syncthreads();
+        // step 2: N1-point DFTs over n1, results back in natural order
+        cplx<T> out[N2 / N1][N1];
+#pragma unroll
+        for (int i = 0; i < N2 / N1; i++) {
+            const int k1 = g + N1 * i;
+#pragma unroll
+            for (int n1 = 0; n1 < N1; n1++) out[i][n1] = B[(n1 + N1 * k1) * W + c];
+            dft_reg<T, N1, DIR>(out[i]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < N2 / N1; i++) {
+            const int k1 = g + N1 * i;
+#pragma unroll
+            for (int k2 = 0; k2 < N1; k2++) B[(k1 + N2 * k2) * W + c] = out[i][k2];
+        }
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            int c0, c1, c2, c3;
+            coords(t, c0, c1, c2, c3);
+            tma_store_4d(&map, c0, c1, c2, c3, B);
+            bulk_commit();
+            // refill the buffer of the previous iteration with the tile S
+            // iterations after it, once its store has read shared memory
+            if (it >= 1) {
+                const int tn = t + (S - 1) * (int)gridDim.x;
+                if (tn < ntiles) {
+                    const int bp = (it - 1) % S;
+                    bulk_wait_read<1>();
+                    coords(tn, c0, c1, c2, c3);
+                    mbar_expect_tx(&full[bp], tile_bytes);
+                    tma_load_4d(buf + (size_t)bp * N * W, &map, c0, c1, c2, c3, &full[bp]);
+                }
+            }
+        }
+    }
+    if (tid == 0) bulk_wait_all();
 }
 
 // ---------------------------------------------------------------------------
@@ -276,7 +390,7 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
     fft_z_products_kernel(cplx<T> *io, size_t field_stride_c, int nrows, int hnzp,
                           const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale) {
     constexpr int P = Split<M>::N1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     T       *U  = reinterpret_cast<T *>(smem_raw);                   // [3][R][2M]
     cplx<T> *ws = reinterpret_cast<cplx<T> *>(U + 3 * R * 2 * M);     // [R][M+1]
     const int r   = threadIdx.x / P;

@@ -2,6 +2,7 @@
 // dispatch from runtime sizes to the compile-time kernels of spm_fft.cuh.
 #pragma once
 
+#include <algorithm>
 #include <vector>
 
 #include "spm_fft.cuh"
@@ -133,6 +134,46 @@ struct FFTPlan {
         }
         return cudaGetLastError();
     }
+    // Persistent TMA-pipelined strided pass (N <= 256): tile W_T columns,
+    // S_T-deep buffer ring.  Returns cudaErrorNotSupported when it cannot run
+    // (size or missing driver entry point); the caller then uses strided().
+    static constexpr int W_T = sizeof(T) == 8 ? 8 : 16;
+    static constexpr int S_T = 3;
+    unsigned int *err = nullptr;  // device error word (set by the owner)
+    int           ctas_per_sm = 2;
+    int           sm_count    = 148;
+
+    template <int DIR>
+    cudaError_t strided_tma(cplx<T> *data, int nfields, size_t fs_c, int axis, cudaStream_t st) const {
+        const int n = axis == 1 ? g.ny : g.nx;
+        if (n > 256 || !encode_tiled_fn()) return cudaErrorNotSupported;
+        const int outer     = axis == 1 ? g.nx : g.ny;
+        const int col_tiles = (g.hnz + W_T - 1) / W_T;
+        const int ntiles    = nfields * outer * col_tiles;
+        CUtensorMap   map;
+        const uint64_t dims[4] = {(uint64_t)2 * g.hnz, (uint64_t)g.ny, (uint64_t)g.nx, (uint64_t)nfields};
+        const uint64_t strides[3] = {(uint64_t)2 * g.hnzp * sizeof(T), (uint64_t)g.ny * 2 * g.hnzp * sizeof(T),
+                                     (uint64_t)fs_c * sizeof(cplx<T>)};
+        const uint32_t box[4] = {(uint32_t)(2 * W_T), axis == 1 ? (uint32_t)n : 1u, axis == 1 ? 1u : (uint32_t)n,
+                                 1u};
+        if (!make_map_4d<T>(&map, data, dims, strides, box)) return cudaErrorNotSupported;
+        const cplx<T> *tw   = axis == 1 ? tw_y : tw_x;
+        const int      grid = std::min(ntiles, sm_count * ctas_per_sm);
+        switch (n) {
+#define SPM_TMA(NN)                                                                                            \
+    case NN:                                                                                                   \
+        fft_strided_tma_kernel<T, NN, W_T, DIR, S_T>                                                           \
+            <<<grid, W_T * Split<NN>::N1, (size_t)S_T * NN * W_T * sizeof(cplx<T>), st>>>(map, axis, outer,    \
+                                                                                          col_tiles, ntiles, tw, \
+                                                                                          err);                \
+        break;
+            SPM_TMA(8) SPM_TMA(16) SPM_TMA(32) SPM_TMA(64) SPM_TMA(128) SPM_TMA(256)
+#undef SPM_TMA
+            default: return cudaErrorNotSupported;
+        }
+        return cudaGetLastError();
+    }
+
     // axis 1 = Y, axis 0 = X
     template <int DIR>
     cudaError_t strided(cplx<T> *data, int nfields, size_t fs_c, int axis, cudaStream_t st) const {
@@ -172,6 +213,12 @@ struct FFTPlan {
         return cudaFuncSetAttribute(fft_strided_kernel<T, NN, W, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)(NN * W * sizeof(cplx<T>)));
     }
+    template <int NN, int DIR>
+    static cudaError_t attr_tma() {
+        return cudaFuncSetAttribute(fft_strided_tma_kernel<T, NN, W_T, DIR, S_T>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)((size_t)S_T * NN * W_T * sizeof(cplx<T>)));
+    }
     template <int MM>
     static cudaError_t attr_products() {
         return cudaFuncSetAttribute(fft_z_products_kernel<T, MM, prows(MM)>,
@@ -179,6 +226,11 @@ struct FFTPlan {
     }
     static cudaError_t set_smem_attrs() {
         cudaError_t e = cudaSuccess;
+#define SPM_TATTR(NN)                                         \
+    if ((e = attr_tma<NN, -1>()) != cudaSuccess) return e;      \
+    if ((e = attr_tma<NN, +1>()) != cudaSuccess) return e;
+        SPM_TATTR(8) SPM_TATTR(16) SPM_TATTR(32) SPM_TATTR(64) SPM_TATTR(128) SPM_TATTR(256)
+#undef SPM_TATTR
 #define SPM_PATTR(MM) \
     if ((e = attr_products<MM>()) != cudaSuccess) return e;
         SPM_PATTR(4) SPM_PATTR(8) SPM_PATTR(16) SPM_PATTR(32) SPM_PATTR(64) SPM_PATTR(128) SPM_PATTR(256)
