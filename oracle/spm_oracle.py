@@ -535,3 +535,429 @@ class OracleSPM:
         """Real-space velocity of the current state, as rebuilt from zeta
         (Zeta_k2u_k + U_k2u)."""
         return self.ifft(self.zeta_k2u_k(self.zeta, self.uk_dc))
+
+
+# ============================================================================
+# Lees-Edwards (oblique coordinates) step: Time_evolution_hydro_OBL
+# (sp_3d_ns.cxx:328-433) for Shear_Navier_Stokes_Lees_Edwards with DC shear.
+# ============================================================================
+class OracleSPMLE(OracleSPM):
+    """Sheared suspension: the velocity field is held in oblique (sheared)
+    coordinates with contravariant components; degree_oblique grows by
+    Shear_rate * dt per step."""
+
+    def __init__(self, cfg, particles):
+        self.gamma = 0.0            # degree_oblique (zero-initialised global)
+        self.srate_eff = 0.0        # Shear_rate_eff (zero until the first step)
+        self.strain = 0.0           # Shear_strain_realized (input.cxx:808)
+        self.stress = {}
+        super().__init__(cfg, particles)
+        self.xy_aspect = self.NX / self.NY
+        # Show_parameter zeroes v_x and omega_z of every particle of a sheared
+        # run after the initial projection (init_particle.cxx:767-781).
+        self.v[:, 0] = 0.0
+        self.v_old[:, 0] = 0.0
+        self.omega[:, 2] = 0.0
+        self.omega_old[:, 2] = 0.0
+
+    # ---- metric helpers -------------------------------------------------
+    def contra2co(self, v):
+        """contra2co_single (fft_wrapper.h:613-622)."""
+        g = self.gamma
+        return np.stack([v[0] + g * v[1], g * v[0] + (1.0 + g * g) * v[1], v[2]])
+
+    def update_k2_obl(self):
+        """Update_K2_OBL (fluid_solver.h:342-361)."""
+        self.K2 = self.kx ** 2 + (self.ky - self.kx * self.gamma) ** 2 + self.kz ** 2
+        with np.errstate(divide="ignore"):
+            self.IK2 = np.where(self.K2 > 0.0, 1.0 / np.where(self.K2 > 0, self.K2, 1.0), 0.0)
+
+    def zeta_k2u_k_obl(self, zeta, uk_dc):
+        """Zeta_k2u_k_OBL (fft_wrapper.cxx:690-768): case split on KX / KZ,
+        omega contra -> co, u = i k x omega_co / K2."""
+        kx, ky, kz, ik2 = self.kx, self.ky, self.kz, self.IK2
+        z0, z1 = zeta[0], zeta[1]
+        cx = self.KX != 0
+        cz = (self.KX == 0) & (self.KZ != 0)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            inv_kx = np.where(cx, 1.0 / np.where(cx, kx, 1.0), 0.0)
+            dmy = np.where(self.KZ != 0, -(ky / np.where(self.KZ != 0, kz, 1.0)), 0.0)
+        om = np.stack([np.where(cx, -inv_kx * (ky * z0 + kz * z1), np.where(cz, z1, z0)),
+                       np.where(cx, z0, np.where(cz, z0, 0.0)),
+                       np.where(cx, z1, np.where(cz, dmy * z0, z1))])
+        om = self.contra2co(om)
+        kx, ky, kz = kx * ik2, ky * ik2, kz * ik2
+        u = np.stack([1j * (ky * om[2] - kz * om[1]), 1j * (kz * om[0] - kx * om[2]),
+                      1j * (kx * om[1] - ky * om[0])])
+        for d in range(3):
+            u[d, 0, 0, 0] = complex(uk_dc[d], u[d, 0, 0, 0].imag)
+        return u
+
+    def zeta_k2omega_k_obl(self, zeta):
+        """Zeta_k2omega_k_OBL (fft_wrapper.cxx:806-845)."""
+        kx, ky, kz = self.kx, self.ky, self.kz
+        z0, z1 = zeta[0], zeta[1]
+        cx = self.KX != 0
+        cz = (self.KX == 0) & (self.KZ != 0)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            inv_kx = np.where(cx, 1.0 / np.where(cx, kx, 1.0), 0.0)
+            dmy = np.where(self.KZ != 0, -(ky / np.where(self.KZ != 0, kz, 1.0)), 0.0)
+        om = np.stack([np.where(cx, -inv_kx * (ky * z0 + kz * z1), np.where(cz, z1, z0)),
+                       np.where(cx, z0, np.where(cz, z0, 0.0)),
+                       np.where(cx, z1, np.where(cz, dmy * z0, z1))])
+        om[:, 0, 0, 0] = 1j * om[:, 0, 0, 0].imag   # omega[d][0] = 0 (real part only)
+        return om
+
+    def omega_to_zeta_obl(self, om):
+        """Omega_k2zeta_k_OBL (fft_wrapper.cxx:265-292)."""
+        cx = self.KX != 0
+        cz = (self.KX == 0) & (self.KZ != 0)
+        return np.stack([np.where(cx, om[1], np.where(cz, om[1], om[0])),
+                         np.where(cx, om[2], np.where(cz, om[0], om[2]))])
+
+    def u_k2zeta_k_obl(self, uk):
+        """U_k2zeta_k_OBL (fft_wrapper.cxx:528-589)."""
+        uk_dc = np.array([uk[d, 0, 0, 0].real for d in range(3)])
+        uc = self.contra2co(uk)
+        kx, ky, kz = self.kx, self.ky, self.kz
+        om = np.stack([1j * (ky * uc[2] - kz * uc[1]), 1j * (kz * uc[0] - kx * uc[2]),
+                       1j * (kx * uc[1] - ky * uc[0])])
+        return self.omega_to_zeta_obl(om), uk_dc
+
+    def solenoidal_uk_obl(self, uk):
+        """Solenoidal_uk_OBL (operate_omega.cxx:197-227)."""
+        g = self.gamma
+        kx, ky, kz = self.kx, self.ky, self.kz
+        kxc = (1.0 + g * g) * kx - g * ky
+        kyc = -g * kx + ky
+        dmy = self.IK2 * (uk[0] * kx + uk[1] * ky + uk[2] * kz)
+        return np.stack([uk[0] - dmy * kxc, uk[1] - dmy * kyc, uk[2] - dmy * kz])
+
+    # ---- oblique <-> Cartesian grids ------------------------------------
+    def _shift_params(self, j, to_oblique):
+        g = self.gamma
+        dj = j - self.NY // 2
+        sign = float(dj) if g >= 0.0 else float(-dj)
+        if dj != 0:
+            sign = sign / abs(sign)
+        base = float(int(sign * g * dj))
+        if to_oblique:   # orth2obl (fft_wrapper.h:315-327)
+            io = base * sign
+            alpha = (g * dj - io) * sign
+        else:            # obl2orth (fft_wrapper.h:328-340)
+            io = base * sign + sign
+            alpha = (io - g * dj) * sign
+        return io, alpha, sign
+
+    def u_oblique2u(self, uu):
+        """U_oblique2u (fft_wrapper.h:515-546), mean flow added."""
+        NX, NY = self.NX, self.NY
+        out = np.empty_like(uu)
+        i = np.arange(NX)
+        for j in range(NY):
+            io, alpha, sign = self._shift_params(j, False)
+            beta = 1.0 - alpha
+            i_ob = np.fmod(i + io + 4.0 * NX, NX).astype(int)
+            i_p = np.fmod(i + sign + 2.0 * NX, NX).astype(int)
+            for d in range(3):
+                out[d, i_ob, j, :] = beta * uu[d, i, j, :] + alpha * uu[d, i_p, j, :]
+            out[0, i_ob, j, :] += self.gamma * out[1, i_ob, j, :]
+            out[0, i_ob, j, :] += self.srate_eff * (j - NY / 2.0)
+        return out
+
+    def u2u_oblique(self, uu):
+        """U2u_oblique (fft_wrapper.h:486-512), mean flow not removed."""
+        NX, NY = self.NX, self.NY
+        out = np.empty_like(uu)
+        i = np.arange(NX)
+        for j in range(NY):
+            io, alpha, sign = self._shift_params(j, True)
+            beta = 1.0 - alpha
+            i_o = np.fmod(i + io + 4.0 * NX, NX).astype(int)
+            i_op = np.fmod(i_o + sign + 4.0 * NX, NX).astype(int)
+            for d in range(3):
+                out[d, :, j, :] = beta * uu[d, i_o, j, :] + alpha * uu[d, i_op, j, :]
+            out[0, :, j, :] -= self.gamma * out[1, :, j, :]
+        return out
+
+    def reset_u_obl(self, u, flg):
+        """Reset_U_OBL (fluid_solver.h:312-337)."""
+        NX, NY = self.NX, self.NY
+        delta = self.xy_aspect if flg == 0 else -self.xy_aspect
+        out = np.empty_like(u)
+        i = np.arange(NX)
+        for j in range(NY):
+            s = float(j - NY // 2)
+            if s != 0:
+                s = s / abs(s)
+            io = float(int(s * (j - NY // 2)) * s)
+            i_obl = np.fmod(i + delta * io + 4.0 * NX, NX).astype(int)
+            out[0, i_obl, j, :] = u[0, i, j, :] + delta * u[1, i, j, :]
+            out[1, i_obl, j, :] = u[1, i, j, :]
+            out[2, i_obl, j, :] = u[2, i, j, :]
+        return out
+
+    # ---- stencil geometry with the Lees-Edwards image ---------------------
+    def stencil_geometry_obl(self, x):
+        """Particle_cell + Relative_coord_check_stepover_Y + Distance_OBL
+        (make_phi.h:114-139, 229-265; interaction.h:50-72)."""
+        dx = self.DX
+        NX, NY, NZ = self.NX, self.NY, self.NZ
+        Lx, Ly, Lz = self.L
+        g = self.gamma
+        dmy = x * (1.0 / dx)
+        x_int = np.trunc(dmy).astype(np.int64)
+        residue = (dmy - x_int) * dx
+        cell = self.cells[None, :, :]
+        yy = x_int[:, None, 1] + cell[..., 1]
+        rm1 = (yy + NY) % NY
+        sgn = np.sign(yy - rm1).astype(np.int64)
+        fx = np.fmod(x_int[:, None, 0] - sgn * g * NY + residue[:, None, 0] / dx + cell[..., 0] + 4 * NX, NX)
+        rm0 = fx.astype(np.int64)
+        xres = fx - rm0
+        rm2 = (x_int[:, None, 2] + cell[..., 2] + NZ) % NZ
+        r = np.stack([cell[..., 0] * dx - xres * dx, cell[..., 1] * dx - residue[:, None, 1],
+                      cell[..., 2] * dx - residue[:, None, 2]], axis=-1)
+        # Distance_OBL(x_mesh, x_p)
+        xm = np.stack([rm0, rm1, rm2], axis=-1) * dx
+        y12 = x[:, None, 1] - xm[..., 1]
+        sy = y12.copy()
+        y12 = y12 - nint(y12 / Ly) * Ly
+        sy = sy - y12
+        s = np.trunc(sy).astype(np.int64)
+        s = np.sign(s)
+        x12 = x[:, None, 0] - (xm[..., 0] + s * g * Ly)
+        x12 = x12 - nint(x12 / Lx) * Lx
+        z12 = x[:, None, 2] - xm[..., 2]
+        z12 = z12 - nint(z12 / Lz) * Lz
+        dist = np.sqrt(y12 ** 2 + x12 ** 2 + z12 ** 2)
+        flat = (rm0 * NY + rm1) * NZ + rm2
+        return flat, r, dist, sgn, rm1
+
+    def make_phi_particle_sum_obl(self):
+        """Make_phi_particle_sum_OBL (make_phi.cxx:262-311)."""
+        flat, r, dist, sgn, rm1 = self.stencil_geometry_obl(self.x)
+        ph = self.profile(dist)
+        phi_sum = np.zeros(self.NX * self.NY * self.NZ)
+        np.add.at(phi_sum, flat.ravel(), ph.ravel())
+        self.phi_sum = phi_sum.reshape(self.NX, self.NY, self.NZ)
+        self.phi = np.minimum(self.phi_sum, 1.0)
+
+    def calc_f_hydro_obl(self, ucp):
+        """Calc_f_hydro_correct_precision_OBL (md_force.cxx:508-745), with the
+        sums of the Hydro_force / Hydro_force_new fields that
+        Mean_shear_stress reduces (fluid_solver.h:253-279)."""
+        flat, r, dist, sgn, rm1 = self.stencil_geometry_obl(self.x)
+        Ly = self.L[1]
+        rr = np.sqrt(r[..., 0] ** 2 + r[..., 1] ** 2 + r[..., 2] ** 2)
+        w = self.profile(rr) / np.maximum(self.phi_sum.ravel()[flat], 1.0)
+        ug = ucp.reshape(3, -1)[:, flat]
+        vs = self._v_surface(self.v, self.omega, r)
+        vs[..., 0] = vs[..., 0] - sgn * self.srate_eff * Ly
+        dmy_fp = (vs - np.moveaxis(ug, 0, -1)) * w[..., None]
+        force = dmy_fp.sum(axis=1)
+        torque = np.stack([r[..., 1] * dmy_fp[..., 2] - r[..., 2] * dmy_fp[..., 1],
+                           r[..., 2] * dmy_fp[..., 0] - r[..., 0] * dmy_fp[..., 2],
+                           r[..., 0] * dmy_fp[..., 1] - r[..., 1] * dmy_fp[..., 0]], axis=-1).sum(axis=1)
+        volume = w.sum(axis=1)
+        itrace = (w * rr ** 2).sum(axis=1) * (2.0 / 3.0)
+        dmy_ry = rm1 + sgn * Ly
+        rho_p = self.cfg.mass_ratio * self.cfg.rho
+        A = (dmy_fp[..., 0] * dmy_ry * rho_p).sum(axis=1)
+        Y = (dmy_ry * w).sum(axis=1)
+        mdf = self.momentum_depend_fr[:, 0]
+        sv = -self.cfg.rho * force[:, 0] / volume
+        swz = -self.cfg.rho * (torque[:, 1][:, None] * r[..., 2] - torque[:, 2][:, None] * r[..., 1]) / itrace[:, None]
+        hf_new = A.sum() + (sv * Y).sum() + (swz * dmy_ry * w).sum()
+        sum_force = force[:, 0].sum()
+        sum_volume = volume.sum() / self.cfg.rho
+        hf_old = A.sum() - ((mdf / volume) * Y).sum() - (sum_force / sum_volume) * Y.sum()
+        dmy = -self.d["DX3"] * self.cfg.rho / self.dt
+        self.f_hydro = dmy * force
+        if self.cfg.rotation:
+            self.torque_hydro = dmy * torque
+        ivol = self.d["Ivolume"] * self.DX ** 3
+        self.stress["hydro_old"] = -hf_old * ivol / self.dt
+        self.stress["hydro_new"] = -hf_new * ivol / self.dt
+
+    def make_u_particle_sum_obl(self):
+        """Make_u_particle_sum_OBL (make_phi.cxx:356-402)."""
+        flat, r, dist, sgn, rm1 = self.stencil_geometry_obl(self.x)
+        w = self.profile(dist) / np.maximum(self.phi_sum.ravel()[flat], 1.0)
+        vs = self._v_surface(self.v, self.omega, r)
+        vs[..., 0] = vs[..., 0] - sgn * self.srate_eff * self.L[1]
+        vs = vs * w[..., None]
+        up = np.zeros((3, self.NX * self.NY * self.NZ))
+        for dd in range(3):
+            np.add.at(up[dd], flat.ravel(), vs[..., dd].ravel())
+        return up.reshape(3, self.NX, self.NY, self.NZ)
+
+    def pbc_obl(self):
+        """MD_solver_position_*_OBL wrap: PBC_OBL (periodic_boundary.h:26-45)."""
+        Lx, Ly, Lz = self.L
+        for n in range(self.np):
+            sy = self.x[n, 1]
+            self.x[n, 1] = math.fmod(self.x[n, 1] + Ly, Ly)
+            s = int(sy - self.x[n, 1])
+            if s != 0:
+                s = s // abs(s)
+            self.x[n, 0] -= s * self.gamma * Ly
+            self.x[n, 0] = math.fmod(self.x[n, 0] + Lx, Lx)
+            self.x[n, 2] = math.fmod(self.x[n, 2] + Lz, Lz)
+            dvx = -s * self.srate_eff * Ly
+            self.v[n, 0] += dvx
+            self.v_old[n, 0] += dvx
+
+    def calc_f_lennard_jones_obl(self):
+        """Calc_f_Lennard_Jones_shear_cap_primitive with Distance0_OBL
+        (md_force.cxx:198-304, interaction.h:50-72)."""
+        d = self.d
+        sigma, cutoff, eps = d["LJ_dia"], d["A_R_cutoff"] * d["LJ_dia"], self.cfg.epsilon
+        Lx, Ly, Lz = self.L
+        ss0 = 0.0
+        for n in range(self.np):
+            for m in range(n + 1, self.np):
+                x1, x2 = self.x[n], self.x[m]
+                y12 = x2[1] - x1[1]
+                sy = y12
+                y12 -= nint(np.array(y12 / Ly)) * Ly
+                sy -= y12
+                s = int(sy)
+                if s != 0:
+                    s = s // abs(s)
+                x12 = x2[0] - (x1[0] + s * self.gamma * Ly)
+                x12 -= nint(np.array(x12 / Lx)) * Lx
+                z12 = x2[2] - x1[2]
+                z12 -= nint(np.array(z12 / Lz)) * Lz
+                rij = math.sqrt(y12 * y12 + x12 * x12 + z12 * z12)
+                if rij < cutoff:
+                    sg = sigma / rij
+                    s6 = (sg * sg) * (sg * sg) * (sg * sg)
+                    lj = 24.0 * eps / (rij * rij) * (2.0 * s6 * s6 - s6)
+                    dmy_r = min(DBL_MAX / rij, lj)
+                    fn = dmy_r * -np.array([float(x12), float(y12), float(z12)])
+                    self.fr[m] -= fn
+                    self.fr[n] += fn
+                    ss0 += fn[0] * float(y12)
+        self.dev_shear_stress_lj = ss0
+
+    def velocity_obl(self, euler):
+        """MD_solver_velocity_*_OBL (particle_solver.cxx:336-432) with Force_OBL
+        (particle_solver.h:113-128)."""
+        self.dev_shear_stress_lj = 0.0
+        if self.cfg.lj_truncate in ("ON", "OFF"):
+            self.calc_f_lennard_jones_obl()
+        if any(f != 0.0 for f in self.cfg.body_force):
+            self.fr += np.array(self.cfg.body_force)[None, :]
+        self.dev_shear_stress_lj *= self.d["Ivolume"]
+        imass, imoi = self.d["IMASS"], self.d["IMOI"]
+        h = self.dt if euler else self.hdt
+        self.v_old, self.omega_old = self.v.copy(), self.omega.copy()
+        if euler:
+            self.v = self.v + h * imass * (self.f_hydro + self.fr)
+            self.omega = self.omega + h * imoi * (self.torque_hydro + self.torque_r)
+            self.momentum_depend_fr = self.dt * self.fr
+        else:
+            self.v = self.v + h * imass * (2.0 * self.f_hydro + self.fr + self.fr_previous)
+            self.omega = self.omega + h * imoi * (2.0 * self.torque_hydro + self.torque_r + self.torque_r_previous)
+            self.momentum_depend_fr = self.hdt * (self.fr + self.fr_previous)
+        self.reset_forces()
+
+    def reynolds_stress(self, ucp):
+        """Calc_Reynolds_shear_stress (fluid_solver.h:165-183)."""
+        j = np.arange(self.NY)[None, :, None]
+        dy = (j - self.NY // 2) * self.DX
+        s = np.sum((ucp[0] - self.srate_eff * dy) * ucp[1])
+        return -(self.d["Ivolume"] * self.DX ** 3) * self.cfg.rho * s
+
+    def shear_rate_correction(self, u0):
+        """Calc_shear_rate_eff (sp_3d_ns.h:166-203)."""
+        g = self.gamma
+        ip = np.roll(u0, -1, axis=0)
+        im = np.roll(u0, 1, axis=0)
+        f_p1 = 0.5 * ((1 - g) * np.roll(ip, -1, axis=1) + (1 + g) * np.roll(im, -1, axis=1))
+        f_m1 = 0.5 * ((1 - g) * np.roll(im, 1, axis=1) + (1 + g) * np.roll(ip, 1, axis=1))
+        s = np.sum((f_p1 - f_m1) * (1.0 / (2.0 * self.DX)))
+        return s * self.d["Ivolume"] * self.DX ** 3
+
+    def step(self):
+        if self.cfg.equation != "Shear_Navier_Stokes_Lees_Edwards":
+            return super().step()
+        cfg = self.cfg
+        if not hasattr(self, "momentum_depend_fr"):
+            self.momentum_depend_fr = np.zeros((self.np, 3))
+        # NS_solver_slavedEuler_Shear_OBL with Zeta_k2advection_k_OBL
+        # (fluid_solver.cxx:411-437, operate_omega.cxx:100-155)
+        self.zeta = self.truncate(self.zeta)
+        uk = self.zeta_k2u_k_obl(self.zeta, self.uk_dc)
+        uky = uk[1].copy()
+        u = self.ifft(uk)
+        w = self.ifft(self.zeta_k2omega_k_obl(self.zeta))
+        a = np.stack([u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]])
+        ak = self.fft(a)
+        ak[0] = ak[0] - 2.0 * self.srate_eff * uky
+        ak[1] = ak[1] - 2.0 * self.srate_eff * self.gamma * uky
+        kx, ky, kz = self.kx, self.ky, self.kz
+        rot = np.stack([1j * (ky * ak[2] - kz * ak[1]), 1j * (kz * ak[0] - kx * ak[2]), 1j * (kx * ak[1] - ky * ak[0])])
+        f_ns0 = self.omega_to_zeta_obl(rot)
+        nu = cfg.eta / cfg.rho
+        dmy = np.exp((-nu * self.dt) * self.K2) - 1.0
+        upd = self.zeta + dmy * (self.zeta - ((1.0 / nu) * self.IK2) * f_ns0)
+        self.zeta = np.where(self.keep, upd, self.zeta)
+        # FIX_CELL (y always fixed under Lees-Edwards, input.cxx:1893-1896)
+        for dd in range(3):
+            if cfg.fix_cell[dd] or dd == 1:
+                self.uk_dc[dd] = 0.0
+        u = self.ifft(self.zeta_k2u_k_obl(self.zeta, self.uk_dc))
+        self.srate_eff = cfg.shear_rate
+        self.gamma += self.srate_eff * self.dt
+        if self.gamma >= self.xy_aspect:
+            u = self.reset_u_obl(u, 0)
+            self.gamma -= self.xy_aspect
+        elif self.gamma <= -self.xy_aspect:
+            u = self.reset_u_obl(u, 1)
+            self.gamma += self.xy_aspect
+        self.update_k2_obl()
+        ucp = self.u_oblique2u(u)
+        self.srate_eff += self.shear_rate_correction(u[0])
+        # particles
+        euler = self.ts == 0
+        self.x_previous = self.x.copy()
+        dxp = self.dt * self.v if euler else self.hdt * (3.0 * self.v - self.v_old)
+        self.x_nopbc = self.x_nopbc + dxp
+        self.x = self.x + dxp
+        self.pbc_obl()
+        if cfg.rotation:
+            if euler:
+                self.q_old = self.q.copy()
+                self.q = qtn_normalize(self.q + qdot_space(self.q, self.omega) * self.dt)
+            else:
+                dq = qdot_space(self.q, self.omega)
+                dq_old = qdot_space(self.q_old, self.omega_old)
+                self.q_old = self.q.copy()
+                self.q = qtn_normalize((self.q + dq * (3.0 * self.hdt)) + dq_old * (-self.hdt))
+        self.make_phi_particle_sum_obl()
+        self.calc_f_hydro_obl(ucp)
+        self.stress["reynolds"] = self.reynolds_stress(ucp)
+        self.velocity_obl(euler)
+        if cfg.kbt > 0.0:
+            self.thermostat()
+        up = self.make_u_particle_sum_obl()
+        f = up - self.phi[None] * ucp
+        u = u + self.u2u_oblique(f)
+        uk = self.solenoidal_uk_obl(self.fft(u))
+        self.zeta, self.uk_dc = self.u_k2zeta_k_obl(uk)
+        self.u = u
+        self.ts += 1
+        self.time += self.dt
+        # main loop bookkeeping and Mean_shear_stress (sp_3d_ns.cxx:960-965,
+        # sp_3d_ns.h:296-339)
+        self.strain += self.srate_eff * self.dt
+        fluid = cfg.eta * self.srate_eff
+        self.stress.update(dict(time=self.time, shear_rate=self.srate_eff, degree_oblique=self.gamma,
+                                strain=self.strain, lj=self.dev_shear_stress_lj, fluid=fluid))
+        self.stress["apparent"] = self.stress["hydro_new"] + self.stress["reynolds"] + self.dev_shear_stress_lj + fluid
+
+    def velocity_field_obl(self):
+        """Oblique (contravariant) real-space velocity rebuilt from zeta."""
+        return self.ifft(self.zeta_k2u_k_obl(self.zeta, self.uk_dc))

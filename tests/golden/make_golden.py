@@ -25,7 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from kapsel3_b200.udf import SPMConfig, make_particles, write_udf_keys  # noqa: E402
+from kapsel3_b200.udf import EQ_LE, SPMConfig, make_particles, write_udf_keys  # noqa: E402
 from oracle import ref_runner  # noqa: E402
 
 CASES = {
@@ -43,6 +43,17 @@ CASES = {
         cfg=dict(npx=5, npy=4, npz=6, n_particles=5, a=3.0, a_xi=2.0, dt=0.05, kbt=1e-5,
                  body_force=(0.0, 2e-3, -1e-3), num_snap=30),
         init=dict(seed=5, v_sd=2e-3, random_orientation=True, min_dist_factor=0.92), field_steps=(30,)),
+    # Lees-Edwards: one sphere crosses the sheared y boundary, thermostat on
+    "le_32_boundary_crossing": dict(
+        cfg=dict(npx=5, npy=5, npz=5, n_particles=5, a=3.5, a_xi=2.0, dt=0.05, kbt=1e-5, equation=EQ_LE,
+                 shear_rate=0.02, num_snap=40),
+        init=dict(seed=13, v_sd=1e-3, random_orientation=True), field_steps=(40,),
+        tweak=dict(index=0, x=(6.3, 31.998, 16.2), v=(0.0, 0.08, 0.0))),
+    # Lees-Edwards: strain passes XYaspect = 1, the oblique grid is remapped
+    "le_32_strain_remap": dict(
+        cfg=dict(npx=5, npy=5, npz=5, n_particles=3, a=3.0, a_xi=2.0, dt=0.05, equation=EQ_LE, shear_rate=0.6,
+                 num_snap=40),
+        init=dict(seed=17, v_sd=1e-3, random_orientation=False), field_steps=(40,)),
 }
 
 
@@ -62,11 +73,15 @@ def make_case(name, spec):
     cfg = SPMConfig(**spec["cfg"])
     init = dict(spec["init"])
     parts = make_particles(cfg, **init)
+    if "tweak" in spec:
+        t = spec["tweak"]
+        parts["x"][t["index"]] = t["x"]
+        parts["v"][t["index"]] = t["v"]
     with tempfile.TemporaryDirectory() as td:
         keys = os.path.join(td, "run.keys")
         dump = os.path.join(td, "run.dump")
         write_udf_keys(keys, cfg, parts, out_dir=os.path.join(td, "avs"))
-        ref_runner.run_reference(keys, dump_path=dump, fields_every=1, body_force=cfg.body_force)
+        err = ref_runner.run_reference(keys, dump_path=dump, fields_every=1, body_force=cfg.body_force)
         d = ref_runner.read_dump(dump)
     frames = d["frames"]
     out = {"config_json": np.array(json.dumps(dataclasses.asdict(cfg))),
@@ -78,11 +93,22 @@ def make_case(name, spec):
         out["traj_" + k] = np.stack([f[k] for f in frames])
     out["traj_uk_dc"] = np.stack([f["uk_dc"] for f in frames])
     out["traj_ts"] = np.array([f["ts"] for f in frames])
+    out["traj_degree_oblique"] = np.array([f["degree_oblique"] for f in frames])
+    if cfg.equation == EQ_LE:
+        # Mean_shear_stress lines (sp_3d_ns.h:325-339): time, shear_rate,
+        # degree_oblique, strain, lj, hydro_old, hydro_new, reynolds, fluid,
+        # interfacial, apparent, viscosity
+        rows = [[float(v) for v in l.split()] for l in err.splitlines()
+                if l and not l.startswith("#") and len(l.split()) == 12]
+        out["stress_lines"] = np.array(rows)
     fs = [s for s in spec["field_steps"] if s < len(frames)]
     out["field_steps"] = np.array(fs)
     for s in fs:
         f = frames[s]
         out[f"zeta_retained_{s}"] = retained_modes(cfg, f["zeta"])
+        if "u" not in f:
+            out[f"phi_plane_{s}"] = f["phi"][:, :, 0].copy()
+            continue
         u = f["u"]
         out[f"u_checksums_{s}"] = np.array([np.sum(u[c]) for c in range(3)] +
                                            [np.sum(u[c] ** 2) for c in range(3)] +

@@ -8,6 +8,8 @@ import numpy as np
 from kapsel3_b200.udf import SPMConfig
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+# columns of the reference's Lees-Edwards stress line (sp_3d_ns.h:325-339)
+STRESS_KEYS = ("time", "shear_rate", "degree_oblique", "strain", "lj", "hydro_old", "hydro_new", "reynolds", "fluid")
 
 
 def fixture_names():

@@ -4,8 +4,9 @@ any machine, with or without the reference sources."""
 import numpy as np
 import pytest
 
-from oracle.spm_oracle import OracleSPM
-from tests.golden_util import check_state, fixture_names, load
+from kapsel3_b200.udf import EQ_LE
+from oracle.spm_oracle import OracleSPM, OracleSPMLE
+from tests.golden_util import STRESS_KEYS, check_state, fixture_names, load
 
 TOL = 1e-12
 
@@ -13,17 +14,25 @@ TOL = 1e-12
 @pytest.mark.parametrize("name", fixture_names())
 def test_oracle_matches_reference_fixture(name):
     cfg, parts, z = load(name)
-    o = OracleSPM(cfg, parts)
+    le = cfg.equation == EQ_LE
+    o = (OracleSPMLE if le else OracleSPM)(cfg, parts)
     nframes = len(z["traj_ts"])
     steps = set(int(s) for s in z["field_steps"])
     for ts in range(nframes):
         want_fields = ts in steps
-        u = o.velocity_field() if want_fields else None
+        u = o.velocity_field() if (want_fields and not le) else None
         worst, errs = check_state(z, ts, cfg, o.x, o.v, o.omega, o.q, o.f_hydro_previous,
                                   zeta=o.zeta if want_fields else None, u=u)
         assert worst < TOL, (name, ts, errs)
+        if le:
+            assert abs(o.gamma - z["traj_degree_oblique"][ts]) < 1e-14
         if ts + 1 < nframes:
             o.step()
+            if le:
+                # the reference prints 8 significant digits
+                ref = z["stress_lines"][ts]
+                for i, k in enumerate(STRESS_KEYS):
+                    assert abs(o.stress[k] - ref[i]) <= 6e-8 * abs(ref[i]) + 1e-20, (name, ts, k, o.stress[k], ref[i])
 
 
 def test_fixtures_present():
