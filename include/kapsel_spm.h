@@ -116,8 +116,11 @@ int spm_get_velocity(spm_ctx *ctx, double *u0, double *u1, double *u2);
 int spm_get_phi(spm_ctx *ctx, double *phi);
 int spm_get_time(spm_ctx *ctx, int *ts, double *time);
 /* Lees-Edwards bookkeeping: degree_oblique and the last step's shear-stress
- * terms (sp_3d_ns.h:247-339). */
-int spm_get_shear_state(spm_ctx *ctx, double *degree_oblique, double stress[4]);
+ * line of Mean_shear_stress (sp_3d_ns.h:296-339): stress[0..7] =
+ * {Shear_rate_eff, strain, lj, hydro_old, hydro_new, reynolds, fluid,
+ * apparent}.  For a Lees-Edwards run spm_get_velocity returns the oblique
+ * (contravariant) velocity on the sheared grid. */
+int spm_get_shear_state(spm_ctx *ctx, double *degree_oblique, double stress[8]);
 
 /* ---- reference solver boundaries (host arrays, reference layout) -------- */
 /* NS_solver_slavedEuler (fluid_solver.h:77-82, fluid_solver.cxx:348-374):

@@ -33,9 +33,9 @@ int fail(int code, const std::string &msg) {
     } while (0)
 
 // Doubles per particle in the device particle buffer: 12 three-vectors and
-// two quaternions of the record, x_previous, torque_r, torque_r_previous and
-// lj_stress.
-constexpr int kPWords = 12 * 3 + 2 * 4 + 3 * 3 + 1;
+// two quaternions of the record, x_previous, torque_r, torque_r_previous,
+// momentum_depend_fr and lj_stress.
+constexpr int kPWords = 12 * 3 + 2 * 4 + 4 * 3 + 1;
 
 // Field slots of the context arena (consecutive, fstride complex apart).
 enum Slot { Z0 = 0, Z1, U0, U1, U2, A0, A1, UP0, UP1, UP2, PHIS, NSLOT };
@@ -366,7 +366,7 @@ int step_ns(spm_ctx *c) {
     LAUNCH(c, k_fix_cell, 1, 32, 0, c->uk_dc, c->ph.fix_cell[0], c->ph.fix_cell[1], c->ph.fix_cell[2]);
     if ((rc = zeta_to_velocity<T>(c, 1)) != SPM_OK) return rc;
     const int euler = c->ts == 0 ? 1 : 0;
-    if (c->ph.np > 0) LAUNCH(c, p_position, particle_blocks(c), 128, 0, c->ph, c->ps, euler);
+    if (c->ph.np > 0) LAUNCH(c, p_position, particle_blocks(c), 128, 0, c->ph, c->ps, euler, 1);
     if ((rc = phi_sum_scatter<T>(c)) != SPM_OK) return rc;
     if (c->ph.np > 0) {
         LAUNCH(c, s_hydro_force<T>, c->ph.np, 256, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
@@ -394,17 +394,19 @@ int initialize_impl(spm_ctx *c) {
     if ((rc = zeta_to_velocity<T>(c, 1)) != SPM_OK) return rc;
     if ((rc = rigidity_projection<T>(c)) != SPM_OK) return rc;
     LAUNCH(c, k_zero3, 1, 32, 0, c->uk_dc);
+    if (c->le.enabled && c->ph.np > 0) LAUNCH(c, p_le_zero_vx, particle_blocks(c), 128, 0, c->ph, c->ps);
     c->ts   = 0;
     c->time = 0.0;
     return SPM_OK;
 }
 
+}  // namespace
+#include "spm_le_step.inc"
+namespace {
+
 template <typename T>
 int step_impl(spm_ctx *c) {
-    if (c->P.equation == SPM_EQ_LEES_EDWARDS) {
-        const int rc = step_le<T>(c);
-        return rc < 0 ? fail(SPM_ERR_ARG, "Lees-Edwards step unavailable") : rc;
-    }
+    if (c->P.equation == SPM_EQ_LEES_EDWARDS) return step_le_impl<T>(c);
     return step_ns<T>(c);
 }
 
@@ -473,6 +475,7 @@ int upload_particles(spm_ctx *c, const double *rec, bool normalize_q) {
     SPM_CUDA_CHECK(cudaMemsetAsync(c->ps.torque_r, 0, (size_t)np * 3 * sizeof(double), c->st));
     SPM_CUDA_CHECK(cudaMemsetAsync(c->ps.torque_r_previous, 0, (size_t)np * 3 * sizeof(double), c->st));
     SPM_CUDA_CHECK(cudaMemsetAsync(c->ps.lj_stress, 0, (size_t)np * sizeof(double), c->st));
+    SPM_CUDA_CHECK(cudaMemsetAsync(c->ps.mdf, 0, (size_t)np * 3 * sizeof(double), c->st));
     SPM_CUDA_CHECK(cudaStreamSynchronize(c->st));
     return SPM_OK;
 }
@@ -630,8 +633,18 @@ int spm_create(const spm_params *p, void *stream, spm_ctx **out) {
     c->ps.x_previous            = c->ps.q_old + (size_t)np * 4;
     c->ps.torque_r              = c->ps.x_previous + (size_t)np * 3;
     c->ps.torque_r_previous     = c->ps.torque_r + (size_t)np * 3;
-    c->ps.lj_stress             = c->ps.torque_r_previous + (size_t)np * 3;
+    c->ps.mdf                   = c->ps.torque_r_previous + (size_t)np * 3;
+    c->ps.lj_stress             = c->ps.mdf + (size_t)np * 3;
     le_init(c->le, c->g, c->ph, *p);
+    if (c->le.enabled) {
+        if (cudaMalloc(&c->le.dev, sizeof(LEDev)) != cudaSuccess ||
+            cudaMalloc(&c->le.ppart, (size_t)np * 6 * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&c->le.partial, (size_t)c->grid_blocks() * sizeof(double)) != cudaSuccess) {
+            spm_destroy(c);
+            return fail(SPM_ERR_NOMEM, "Lees-Edwards buffers");
+        }
+        cudaMemset(c->le.dev, 0, sizeof(LEDev));
+    }
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         spm_destroy(c);
@@ -652,6 +665,9 @@ int spm_destroy(spm_ctx *c) {
     cudaFree(c->pbuf);
     cudaFree(c->mt);
     cudaFree(c->err);
+    cudaFree(c->le.dev);
+    cudaFree(c->le.ppart);
+    cudaFree(c->le.partial);
     if (c->own_stream && c->st) cudaStreamDestroy(c->st);
     delete c;
     return SPM_OK;
@@ -717,7 +733,8 @@ int spm_set_zeta(spm_ctx *c, const double *z0, const double *z1, const double uk
 
 int spm_get_velocity(spm_ctx *c, double *u0, double *u1, double *u2) {
     if (!c || !u0 || !u1 || !u2) return fail(SPM_ERR_ARG, "bad argument");
-    int rc = c->fp64() ? zeta_to_velocity<double>(c, 0) : zeta_to_velocity<float>(c, 0);
+    int rc = c->le.enabled ? (c->fp64() ? le_velocity<double>(c) : le_velocity<float>(c))
+                           : (c->fp64() ? zeta_to_velocity<double>(c, 0) : zeta_to_velocity<float>(c, 0));
     if (rc != SPM_OK) return rc;
     if ((rc = spm_synchronize(c)) != SPM_OK) return rc;
     if ((rc = download_field(c, U0, u0)) != SPM_OK) return rc;
@@ -727,7 +744,8 @@ int spm_get_velocity(spm_ctx *c, double *u0, double *u1, double *u2) {
 
 int spm_get_phi(spm_ctx *c, double *phi) {
     if (!c || !phi) return fail(SPM_ERR_ARG, "bad argument");
-    int rc = c->fp64() ? phi_sum_scatter<double>(c) : phi_sum_scatter<float>(c);
+    int rc = c->le.enabled ? (c->fp64() ? le_phi_sum<double>(c) : le_phi_sum<float>(c))
+                           : (c->fp64() ? phi_sum_scatter<double>(c) : phi_sum_scatter<float>(c));
     if (rc != SPM_OK) return rc;
     if (c->fp64())
         LAUNCH(c, r_phi_clamp<double>, c->grid_blocks(), 256, 0, c->g, c->real<double>(PHIS), c->real<double>(A0));
@@ -744,11 +762,11 @@ int spm_get_time(spm_ctx *c, int *ts, double *time) {
     return SPM_OK;
 }
 
-int spm_get_shear_state(spm_ctx *c, double *degree_oblique, double stress[4]) {
+int spm_get_shear_state(spm_ctx *c, double *degree_oblique, double stress[8]) {
     if (!c) return fail(SPM_ERR_ARG, "null context");
     int rc = spm_synchronize(c);
     if (rc != SPM_OK) return rc;
-    return le_get_state(c->le, degree_oblique, stress);
+    return le_get_state(c, degree_oblique, stress);
 }
 
 int spm_fft_forward_dev(spm_ctx *c, void *data, int nfields, size_t field_stride) {

@@ -558,6 +558,7 @@ struct PState {
     double *q, *q_old;  // [Np][4]: s, v0, v1, v2
     double *f_hydro, *f_hydro_previous, *torque_hydro, *torque_hydro_previous;
     double *fr, *fr_previous, *torque_r, *torque_r_previous;
+    double *mdf;        // momentum_depend_fr [Np][3] (particle_solver.cxx:336-432)
     double *lj_stress;  // [Np] per-particle share of sum f_x r_y (LE stress)
 };
 
@@ -581,7 +582,8 @@ __device__ __forceinline__ void qtn_normalize_d(double *q) {
 // MD_solver_position_Euler / _AB2 (particle_solver.cxx:39-85) with the
 // orientation updates (particle_rotation_solver.h:23-29, 72-81) and PBC
 // (periodic_boundary.h:9-16).
-__global__ void p_position(Phys ph, PState s, int euler) {
+// wrap = 0 leaves the periodic wrap to p_le_wrap (Lees-Edwards image).
+__global__ void p_position(Phys ph, PState s, int euler, int wrap) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= ph.np) return;
     for (int d = 0; d < 3; d++) {
@@ -589,7 +591,7 @@ __global__ void p_position(Phys ph, PState s, int euler) {
         s.x_previous[i]   = s.x[i];
         const double dlt  = euler ? ph.dt * s.v[i] : ph.hdt * (3.0 * s.v[i] - s.v_old[i]);
         s.x_nopbc[i] += dlt;
-        s.x[i] = fmod(s.x[i] + dlt + ph.L[d], ph.L[d]);
+        s.x[i] = wrap ? fmod(s.x[i] + dlt + ph.L[d], ph.L[d]) : s.x[i] + dlt;
     }
     if (ph.rotation) {
         double *q = s.q + 4 * n, *qo = s.q_old + 4 * n;
@@ -741,6 +743,40 @@ __global__ void p_velocity(Phys ph, PState s, int euler) {
         const int i      = 3 * n + d;
         s.v_old[i]       = s.v[i];
         s.omega_old[i]   = s.omega[i];
+        if (euler) {
+            s.v[i] += dmy * (s.f_hydro[i] + s.fr[i]);
+            s.omega[i] += dmr * (s.torque_hydro[i] + s.torque_r[i]);
+        } else {
+            s.v[i] += dmy * (2.0 * s.f_hydro[i] + s.fr[i] + s.fr_previous[i]);
+            s.omega[i] += dmr * (2.0 * s.torque_hydro[i] + s.torque_r[i] + s.torque_r_previous[i]);
+        }
+        s.fr_previous[i]           = s.fr[i];
+        s.fr[i]                    = 0.0;
+        s.f_hydro_previous[i]      = s.f_hydro[i];
+        s.f_hydro[i]               = 0.0;
+        s.torque_r_previous[i]     = s.torque_r[i];
+        s.torque_r[i]              = 0.0;
+        s.torque_hydro_previous[i] = s.torque_hydro[i];
+        s.torque_hydro[i]          = 0.0;
+    }
+}
+
+// The Lees-Edwards velocity update also records momentum_depend_fr, the LJ
+// and body-force impulse used by the next step's hydrodynamic stress
+// (MD_solver_velocity_*_OBL, particle_solver.cxx:336-432).
+__global__ void p_velocity_mdf(Phys ph, PState s, int euler) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ph.np) return;
+    for (int d = 0; d < 3; d++) {
+        const int i = 3 * n + d;
+        s.mdf[i]    = euler ? ph.dt * s.fr[i] : ph.hdt * (s.fr[i] + s.fr_previous[i]);
+    }
+    const double dmy = (euler ? ph.dt : ph.hdt) * ph.imass;
+    const double dmr = (euler ? ph.dt : ph.hdt) * ph.imoi;
+    for (int d = 0; d < 3; d++) {
+        const int i    = 3 * n + d;
+        s.v_old[i]     = s.v[i];
+        s.omega_old[i] = s.omega[i];
         if (euler) {
             s.v[i] += dmy * (s.f_hydro[i] + s.fr[i]);
             s.omega[i] += dmr * (s.torque_hydro[i] + s.torque_r[i]);

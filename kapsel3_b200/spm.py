@@ -190,7 +190,7 @@ class SPMRun:
         return ts.value, t.value
 
     def shear_state(self):
-        deg, st = C.c_double(), np.zeros(4)
+        deg, st = C.c_double(), np.zeros(8)
         N.check(self.L.spm_get_shear_state(self.h, C.byref(deg), N.dptr(st)), "spm_get_shear_state")
         return deg.value, st
 
