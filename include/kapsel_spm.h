@@ -159,6 +159,23 @@ int spm_calc_f_hydro_correct_precision_host(spm_ctx *ctx, double *particles_host
  * particle records (cell-list pair multiplicity of the reference). */
 int spm_calc_f_lennard_jones_host(spm_ctx *ctx, double *particles_host);
 
+/* Allocation-free Make_f_particle_dt_sole on caller-owned DEVICE buffers.
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc (their device memory comes from their own pool or another
+ * runtime, or their steady-state loop must stay free of allocator calls).
+ * All ten pointers are device arrays in the reference layout
+ * (double[NX*NY*NZ_]); the result f = P(up - min(phi,1) u) is written to
+ * f0..f2.  FP64 only; grids of 8..64 points per axis (npx/npy/npz in 3..6),
+ * larger grids are rejected with SPM_ERR_ARG.  Working memory is one
+ * file-scope device array of about 6.5 MB that every GPU loading this
+ * library keeps until the process exits; the first call on a device looks
+ * up its address (make that call before any stream capture).  Every call
+ * shares that array: calls that overlap on the GPU race.  `stream` is a
+ * cudaStream_t (NULL: the legacy default stream). */
+int spm_make_f_particle_dt_sole_noalloc(const double *u0, const double *u1, const double *u2, const double *up0,
+                                        const double *up1, const double *up2, const double *phi, double *f0,
+                                        double *f1, double *f2, int npx, int npy, int npz, void *stream);
+
 /* ---- 3D FFT on device buffers ------------------------------------------- */
 /* In-place transforms of nfields device fields of the context's precision,
  * consecutive fields `field_stride` complex elements apart. */

@@ -88,6 +88,7 @@ _SIGS = {
     "spm_time_steps": (C.c_int, [_P, C.c_int, C.POINTER(C.c_float)]),
     "spm_kernel_launches": (C.c_int, [_P, C.POINTER(C.c_longlong), C.c_int]),
     "spm_profile_pass": (C.c_int, [_P, C.c_int, _D, _D, C.POINTER(C.c_longlong)]),
+    "spm_make_f_particle_dt_sole_noalloc": (C.c_int, [_P] * 10 + [C.c_int, C.c_int, C.c_int, _P]),
 }
 
 

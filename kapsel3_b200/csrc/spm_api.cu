@@ -23,6 +23,9 @@ int fail(int code, const std::string &msg) {
 }
 }  // namespace
 
+// Error reporting for the other translation units of the library.
+int spm_internal_fail(int code, const char *msg) { return fail(code, msg); }
+
 #undef SPM_CUDA_CHECK
 #define SPM_CUDA_CHECK(expr)                                                                             \
     do {                                                                                                 \

@@ -197,6 +197,10 @@ struct FFTPlan {
         return cudaGetLastError();
     }
 
+    // Sets the shared-memory limits of every FFT kernel (process-wide
+    // function attributes; no allocation).
+    static cudaError_t configure_kernels() { return set_smem_attrs(); }
+
   private:
     static cudaError_t make_table(cplx<T> **dst, int n, int count) {
         std::vector<cplx<T>> h(count);
