@@ -185,6 +185,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream leg")
+    ap.add_argument("--serve-runs", type=int, default=256)
     ap.add_argument("--profile-run", choices=["fp32", "fp64"], default=None,
                     help="only run warm-up + timed steps of one precision (for ncu captures)")
     args = ap.parse_args()
@@ -267,6 +269,7 @@ def main():
     # accuracy: FP32-mixed vs FP64 after W+K steps from the same state (+ the 2 e2e warm-up + K e2e steps on fp32:
     # recompute both on an equal footing below)
     acc = accuracy_check(cfg, parts, steps=W + K)
+    serving = None if args.no_serve else serving_leg(rank, world, args.serve_runs, barrier, max_over_ranks)
 
     if rank != 0:
         if world > 1:
@@ -298,12 +301,69 @@ def main():
         "clocks": fp32["clocks"],
         "gpu_launches": fp32["launches"],
     }
+    if serving is not None:
+        line["serving"] = serving
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, parts)
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def serving_leg(rank, world, n_runs, barrier, max_over_ranks):
+    """The serving stream: n_runs requests, exponential inter-arrivals at
+    20/s, cubic side uniform over {32, 64, 128}, Np uniform in [1, 300]
+    capped per side by packability, a=4, xi=2, 200 FP32-mixed steps each,
+    device-memory budget 150 GB.  Each replica (GPU) serves every world-th
+    request of the stream through its own native request loop; arrivals are
+    real time.  A sample of each replica's runs (the first of each grid side)
+    keeps its final velocity and is re-run alone in FP64 for its error."""
+    from kapsel3_b200 import _native as N
+    from kapsel3_b200.serve import Server, partition, run_stream, serving_workload
+    from kapsel3_b200.spm import SPMRun, unpack_particles
+
+    w = serving_workload(n_runs=n_runs, rate_per_s=20.0, sides=(32, 64, 128), np_max=300, a=4.0, a_xi=2.0,
+                         nsteps=200, seed=2024)
+    mine = partition(w["requests"], rank, world)
+    sample, seen = set(), set()
+    for i, r in enumerate(mine):
+        if r.cfg.shape[0] not in seen:
+            seen.add(r.cfg.shape[0])
+            sample.add(i)
+    barrier()
+    with Server(budget_bytes=150 << 30, use_graph=True, pool_capacity=8) as srv:
+        res = run_stream(srv, mine, realtime=True, keep_velocity_ids=sample)
+    errs = {}
+    for i in sorted(sample):
+        r, out = mine[i], res["results"][i]
+        if out["state"] != N.SPM_REQ_DONE:
+            continue
+        with SPMRun(r.cfg, precision=N.SPM_PREC_FP64) as run:
+            run.initialize(unpack_particles(r.particles))
+            run.step(r.nsteps)
+            u64 = run.velocity()
+        d = np.linalg.norm(out["velocity"] - u64) / max(np.linalg.norm(u64), 1e-300)
+        errs[str(r.cfg.shape[0])] = max(errs.get(str(r.cfg.shape[0]), 0.0), float(d))
+    st = res["stats"]
+    lat = res["latencies"]
+    busy = max_over_ranks(st["busy_s"])
+    steps_total = st["run_steps"] * world  # equal shares up to one request
+    done = sum(1 for o in res["results"] if o["state"] == N.SPM_REQ_DONE)
+    return {
+        "runs": n_runs, "completed_rank0": done, "requested_rank0": len(mine),
+        "arrivals": "exponential, 20/s, seeded", "sides": [32, 64, 128], "np_cap": w["np_cap"],
+        "steps_per_run": 200, "dtype": "f32 fields / f64 particle reductions", "budget_gb": 150,
+        "steps_per_s": steps_total / busy if busy > 0 else None,
+        "step_latency_ms": {"p50": float(np.percentile(lat, 50)) if len(lat) else None,
+                            "p99": max_over_ranks(float(np.percentile(lat, 99))) if len(lat) else None,
+                            "max": float(lat.max()) if len(lat) else None},
+        "pool_step_device_ms": {"p50": st["pool_step_device_p50_ms"], "p99": st["pool_step_device_p99_ms"]},
+        "max_resident_runs": st["max_active"], "graph_captures": st["graph_captures"],
+        "peak_device_gb": st["peak_bytes"] / 1e9, "wall_s": res["wall_s"],
+        "fp64_rel_velocity_error_sampled": errs,
+        "latency_definition": "host time between consecutive step completions of a run (first: from admission)",
+    }
 
 
 def profile_run(args):

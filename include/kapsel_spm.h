@@ -76,6 +76,7 @@ typedef struct spm_params {
 } spm_params;
 
 typedef struct spm_ctx spm_ctx;
+typedef struct spm_pool spm_pool;
 
 /* ---- context ----------------------------------------------------------- */
 const char *spm_last_error(void);
@@ -194,6 +195,99 @@ int spm_time_steps(spm_ctx *ctx, int nsteps, float *ms);
 int spm_profile_pass(spm_ctx *ctx, int nsteps, double *avg_us, double *bytes_per_launch, long long *count);
 /* Launches of this library's kernels since the last reset. */
 int spm_kernel_launches(spm_ctx *ctx, long long *count, int reset);
+
+/* ---- serving pool (no reference counterpart) ----------------------------
+ * A pool holds independent Navier_Stokes runs of one grid size, DX and
+ * precision.  Their fields share one slot-major device arena so each FFT
+ * stage and each k-space pointwise kernel of a pool step is one launch over
+ * all runs; particle kernels run per run on the pool's stream.  The pool step
+ * can be replayed from a CUDA graph captured once per membership.  A run of
+ * a pool is an spm_ctx: the whole-run getters above work on it (between
+ * steps); spm_destroy refuses it (use spm_pool_release).  Releasing a run
+ * moves the pool's last run into its slot; run handles stay valid. */
+/* Device bytes of a pool arena of `capacity` runs of this grid, and of the
+ * per-run particle buffers for grid->n_particles particles. */
+int spm_pool_device_bytes(const spm_params *grid, int capacity, size_t *arena_bytes, size_t *run_bytes);
+/* `stream`: cudaStream_t of the pool (NULL: a new non-blocking stream). */
+int spm_pool_create(const spm_params *grid, int capacity, void *stream, spm_pool **out);
+int spm_pool_destroy(spm_pool *pool);
+/* Adds a run and runs its initialisation (as spm_initialize).  The pool
+ * doubles its arena when full. */
+int spm_pool_admit(spm_pool *pool, const spm_params *p, const double *particles_host, spm_ctx **run);
+int spm_pool_release(spm_pool *pool, spm_ctx *run);
+int spm_pool_size(spm_pool *pool, int *runs, int *capacity);
+int spm_pool_run(spm_pool *pool, int index, spm_ctx **run);
+int spm_pool_stream(spm_pool *pool, void **stream);
+/* Enqueues nsteps steps of every run (asynchronous); use_graph != 0 replays
+ * a graph of the step captured for the current membership. */
+int spm_pool_step(spm_pool *pool, int nsteps, int use_graph);
+/* done = 1 when the steps enqueued last have finished. */
+int spm_pool_query(spm_pool *pool, int *done);
+/* Waits for the pool; last_ms = device time of the last spm_pool_step call;
+ * errors[r] (optional, one per run slot) = run r's device error bits. */
+int spm_pool_synchronize(spm_pool *pool, float *last_ms, unsigned int *errors);
+int spm_pool_stats(spm_pool *pool, long long *graph_kernels, int *captures);
+/* Host-side fault injection: the next `count` device allocations of contexts
+ * and pools fail with SPM_ERR_NOMEM (0 switches it off). */
+int spm_debug_fail_allocations(int count);
+
+/* ---- serving loop (no reference counterpart) -----------------------------
+ * A persistent worker thread admits submitted Navier_Stokes runs by device-
+ * memory budget into per-grid pools, steps every pool continuously (pools of
+ * different grids on their own streams, overlapping on the GPU), retires runs
+ * at their step count and records per-step latency: for every run step, the
+ * host time between the completion of the run's previous step (or its
+ * admission) and this one. */
+#define SPM_REQ_QUEUED 0
+#define SPM_REQ_RUNNING 1
+#define SPM_REQ_DONE 2
+#define SPM_REQ_FAILED 3
+#define SPM_REQ_CANCELLED 4
+#define SPM_REQ_KEEP_VELOCITY 1 /* submit flag: keep the final velocity field */
+
+typedef struct spm_server spm_server;
+typedef struct spm_server_config {
+    size_t budget_bytes;        /* device bytes the server may hold (pools + runs) */
+    int    pool_initial_capacity; /* run slots of a new pool's arena */
+    int    use_graph;           /* replay each pool step from a captured CUDA graph */
+    int    steps_per_launch;    /* steps enqueued per pool launch (1: per-step latency) */
+    int    poll_us;             /* worker sleep when nothing progressed */
+    int    device;              /* CUDA device index */
+} spm_server_config;
+typedef struct spm_server_stats {
+    long long submitted, rejected, admitted, completed, failed, cancelled, queued;
+    long long run_steps;        /* steps summed over runs */
+    long long graph_captures;
+    int       max_active;       /* most runs resident at once */
+    size_t    used_bytes, peak_bytes;
+    double    busy_s;           /* first admission to last retirement */
+    double    step_latency_p50_ms, step_latency_p99_ms, step_latency_max_ms;
+    double    pool_step_device_p50_ms, pool_step_device_p99_ms;
+} spm_server_stats;
+
+int spm_server_config_default(spm_server_config *cfg);
+int spm_server_create(const spm_server_config *cfg, spm_server **out);
+/* Stops the worker: cancels queued and running requests, frees all pools. */
+int spm_server_destroy(spm_server *server);
+/* Queues a run of nsteps steps (particle records as spm_initialize).
+ * Rejected at once (nonzero status): bad parameters, Lees-Edwards runs,
+ * particles outside the box, or a run larger than the whole budget. */
+int spm_server_submit(spm_server *server, const spm_params *p, const double *particles_host, int nsteps, int flags,
+                      long long *request_id);
+int spm_server_cancel(spm_server *server, long long request_id);
+/* Waits until the request is DONE, FAILED or CANCELLED (timeout_s < 0:
+ * no limit); state = its state on return. */
+int spm_server_wait(spm_server *server, long long request_id, double timeout_s, int *state);
+int spm_server_status(spm_server *server, long long request_id, int *state, int *status, int *steps_done,
+                      char *message, size_t message_len);
+/* Final particle records, optional velocity (SPM_REQ_KEEP_VELOCITY), time,
+ * and submission-to-completion latency of a DONE request. */
+int spm_server_result(spm_server *server, long long request_id, double *particles_host, double *u0, double *u1,
+                      double *u2, double *time, double *latency_s);
+int spm_server_forget(spm_server *server, long long request_id);
+int spm_server_get_stats(spm_server *server, spm_server_stats *stats);
+/* Per-step latency samples in ms (up to cap; n = number recorded). */
+int spm_server_latencies(spm_server *server, float *out, size_t cap, size_t *n);
 
 #ifdef __cplusplus
 }

@@ -43,6 +43,37 @@ class SpmParams(C.Structure):
     ]
 
 
+class SpmServerConfig(C.Structure):
+    _fields_ = [
+        ("budget_bytes", C.c_size_t),
+        ("pool_initial_capacity", C.c_int),
+        ("use_graph", C.c_int),
+        ("steps_per_launch", C.c_int),
+        ("poll_us", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
+class SpmServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_longlong), ("rejected", C.c_longlong), ("admitted", C.c_longlong),
+        ("completed", C.c_longlong), ("failed", C.c_longlong), ("cancelled", C.c_longlong),
+        ("queued", C.c_longlong),
+        ("run_steps", C.c_longlong),
+        ("graph_captures", C.c_longlong),
+        ("max_active", C.c_int),
+        ("used_bytes", C.c_size_t), ("peak_bytes", C.c_size_t),
+        ("busy_s", C.c_double),
+        ("step_latency_p50_ms", C.c_double), ("step_latency_p99_ms", C.c_double),
+        ("step_latency_max_ms", C.c_double),
+        ("pool_step_device_p50_ms", C.c_double), ("pool_step_device_p99_ms", C.c_double),
+    ]
+
+
+SPM_REQ_QUEUED, SPM_REQ_RUNNING, SPM_REQ_DONE, SPM_REQ_FAILED, SPM_REQ_CANCELLED = range(5)
+SPM_REQ_KEEP_VELOCITY = 1
+
+
 class SpmError(RuntimeError):
     pass
 
@@ -89,13 +120,40 @@ _SIGS = {
     "spm_kernel_launches": (C.c_int, [_P, C.POINTER(C.c_longlong), C.c_int]),
     "spm_profile_pass": (C.c_int, [_P, C.c_int, _D, _D, C.POINTER(C.c_longlong)]),
     "spm_make_f_particle_dt_sole_noalloc": (C.c_int, [_P] * 10 + [C.c_int, C.c_int, C.c_int, _P]),
+    "spm_pool_device_bytes": (C.c_int, [C.POINTER(SpmParams), C.c_int, C.POINTER(C.c_size_t),
+                                        C.POINTER(C.c_size_t)]),
+    "spm_pool_create": (C.c_int, [C.POINTER(SpmParams), C.c_int, _P, C.POINTER(_P)]),
+    "spm_pool_destroy": (C.c_int, [_P]),
+    "spm_pool_admit": (C.c_int, [_P, C.POINTER(SpmParams), _D, C.POINTER(_P)]),
+    "spm_pool_release": (C.c_int, [_P, _P]),
+    "spm_pool_size": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "spm_pool_run": (C.c_int, [_P, C.c_int, C.POINTER(_P)]),
+    "spm_pool_stream": (C.c_int, [_P, C.POINTER(_P)]),
+    "spm_pool_step": (C.c_int, [_P, C.c_int, C.c_int]),
+    "spm_pool_query": (C.c_int, [_P, C.POINTER(C.c_int)]),
+    "spm_pool_synchronize": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_uint)]),
+    "spm_pool_stats": (C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
+    "spm_debug_fail_allocations": (C.c_int, [C.c_int]),
+    "spm_server_config_default": (C.c_int, [C.POINTER(SpmServerConfig)]),
+    "spm_server_create": (C.c_int, [C.POINTER(SpmServerConfig), C.POINTER(_P)]),
+    "spm_server_destroy": (C.c_int, [_P]),
+    "spm_server_submit": (C.c_int, [_P, C.POINTER(SpmParams), _D, C.c_int, C.c_int, C.POINTER(C.c_longlong)]),
+    "spm_server_cancel": (C.c_int, [_P, C.c_longlong]),
+    "spm_server_wait": (C.c_int, [_P, C.c_longlong, C.c_double, C.POINTER(C.c_int)]),
+    "spm_server_status": (C.c_int, [_P, C.c_longlong, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_int), C.c_char_p, C.c_size_t]),
+    "spm_server_result": (C.c_int, [_P, C.c_longlong, _D, _D, _D, _D, _D, _D]),
+    "spm_server_forget": (C.c_int, [_P, C.c_longlong]),
+    "spm_server_get_stats": (C.c_int, [_P, C.POINTER(SpmServerStats)]),
+    "spm_server_latencies": (C.c_int, [_P, C.POINTER(C.c_float), C.c_size_t, C.POINTER(C.c_size_t)]),
 }
 
 
 def declared_symbols():
     """Every function the public header declares."""
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"\b(spm_[a-z0-9_]+)\s*\(", text)) - {"spm_params", "spm_ctx"})
+    return sorted(set(re.findall(r"\b(spm_[a-z0-9_]+)\s*\(", text))
+                  - {"spm_params", "spm_ctx", "spm_pool", "spm_server", "spm_server_config", "spm_server_stats"})
 
 
 def lib(build_if_missing: bool = True):

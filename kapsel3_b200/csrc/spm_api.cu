@@ -1,5 +1,6 @@
 // C ABI of the B200 SPM step: context management, the whole step on
 // device-resident state, and the reference-boundary entry points.
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -26,6 +27,24 @@ int fail(int code, const std::string &msg) {
 // Error reporting for the other translation units of the library.
 int spm_internal_fail(int code, const char *msg) { return fail(code, msg); }
 
+namespace {
+// Device allocations of contexts and pools go through dev_alloc, which can be
+// told to fail the next n calls (host-side fault injection for the serving
+// tests; spm_debug_fail_allocations).
+std::atomic<int> g_fail_allocs{0};
+cudaError_t      dev_alloc(void **p, size_t bytes) {
+    for (int n = g_fail_allocs.load(); n > 0; n = g_fail_allocs.load())
+        if (g_fail_allocs.compare_exchange_weak(n, n - 1)) {
+            *p = nullptr;
+            return cudaErrorMemoryAllocation;
+        }
+    return cudaMalloc(p, bytes);
+}
+void dev_free(void *p) {
+    if (p) cudaFree(p);
+}
+}  // namespace
+
 #undef SPM_CUDA_CHECK
 #define SPM_CUDA_CHECK(expr)                                                                             \
     do {                                                                                                 \
@@ -43,23 +62,34 @@ constexpr int kPWords = 12 * 3 + 2 * 4 + 4 * 3 + 1;
 // Field slots of the context arena (consecutive, fstride complex apart).
 enum Slot { Z0 = 0, Z1, U0, U1, U2, A0, A1, UP0, UP1, UP2, PHIS, NSLOT };
 
+struct spm_pool;
+
 struct spm_ctx {
     spm_params   P{};
     Grid         g{};
     Phys         ph{};
     cudaStream_t st         = nullptr;
     bool         own_stream = false;
-    void *       arena      = nullptr;  // NSLOT fields
+    void *       arena      = nullptr;  // slot 0 of this run's fields
     size_t       fstride_c  = 0;        // complex elements per field
+    size_t       slot_stride_c = 0;     // complex elements between two slots of this run
+    bool         owns_arena = true;     // false for runs living in a pool's arena
+    int          fft_runs   = 1;        // runs batched by this context's FFT stages (pool lead)
+    RunWords *   rw         = nullptr;  // uk_dc, step counter, FIX_CELL mask (device)
+    bool         owns_rw    = true;     // false for runs of a pool
+    int *        ts_dev     = nullptr;  // &rw->ts
     FFTPlan<double> plan64;
     FFTPlan<float>  plan32;
+    FFTPlan<double> *pp64 = &plan64;  // the plans in use (a pool's runs use the lead's)
+    FFTPlan<float>  *pp32 = &plan32;
+    spm_pool        *pool = nullptr;  // pool this run belongs to (null for a lone run)
     int *        cells   = nullptr;
     int          ncells  = 0;
-    double *     uk_dc   = nullptr;  // device [3]
+    double *     uk_dc   = nullptr;  // rw->uk_dc
     double *     pbuf    = nullptr;  // particle state arrays
     PState       ps{};
     unsigned int *mt  = nullptr;  // 625 words
-    unsigned int *err = nullptr;  // device error word
+    unsigned int *err = nullptr;  // device error word (&rw->err)
     int          ts   = 0;
     double       time = 0.0;
     long long    launches = 0;
@@ -74,7 +104,7 @@ struct spm_ctx {
     bool fp64() const { return P.precision == SPM_PREC_FP64; }
     template <typename T>
     T *real(int slot) const {
-        return reinterpret_cast<T *>(static_cast<char *>(arena) + (size_t)slot * fstride_c * 2 * sizeof(T));
+        return reinterpret_cast<T *>(static_cast<char *>(arena) + (size_t)slot * slot_stride_c * 2 * sizeof(T));
     }
     template <typename T>
     cplx<T> *cx(int slot) const {
@@ -83,6 +113,13 @@ struct spm_ctx {
     size_t elem_bytes() const { return fp64() ? sizeof(double) : sizeof(float); }
     size_t field_bytes() const { return fstride_c * 2 * elem_bytes(); }
     int    grid_blocks() const { return sm_count * 16; }
+    // blocks of 256 threads per run for the run-batched k-space kernels
+    int pw_blocks() const {
+        const size_t need = (fstride_c + 255) / 256;
+        const int    cap  = std::max(1, grid_blocks() / std::max(1, fft_runs));
+        return (int)std::min<size_t>(need, (size_t)cap);
+    }
+    dim3 pw_grid() const { return dim3(pw_blocks(), fft_runs); }
 };
 
 #define LAUNCH(ctx, kern, grid, block, smem, ...)                                           \
@@ -192,6 +229,17 @@ void mt_init(unsigned int seed, unsigned int *mt) {
 }
 
 
+// Point uk_dc / ts_dev into the run's RunWords and write its initial words.
+void set_run_words(spm_ctx *c) {
+    c->uk_dc  = c->rw->uk_dc;
+    c->ts_dev = &c->rw->ts;
+    c->err    = &c->rw->err;
+    RunWords h{};
+    const bool le = c->P.equation == SPM_EQ_LEES_EDWARDS;
+    h.fix_mask    = (c->ph.fix_cell[0] ? 1 : 0) | ((c->ph.fix_cell[1] || le) ? 2 : 0) | (c->ph.fix_cell[2] ? 4 : 0);
+    cudaMemcpy(c->rw, &h, sizeof(h), cudaMemcpyHostToDevice);
+}
+
 int check_device_error(spm_ctx *c) {
     unsigned int e = 0;
     SPM_CUDA_CHECK(cudaMemcpyAsync(&e, c->err, sizeof(e), cudaMemcpyDeviceToHost, c->st));
@@ -211,22 +259,33 @@ template <typename T>
 FFTPlan<T> &plan_of(spm_ctx *c);
 template <>
 FFTPlan<double> &plan_of<double>(spm_ctx *c) {
-    return c->plan64;
+    return *c->pp64;
 }
 template <>
 FFTPlan<float> &plan_of<float>(spm_ctx *c) {
-    return c->plan32;
+    return *c->pp32;
 }
 
-// Strided (Y/X) FFT pass: the persistent TMA kernel when it applies, else the
-// direct-load kernel.
+// Strided (Y/X) FFT pass over `nf` slots of this context: the persistent TMA
+// kernel when it applies, else the direct-load kernel.  A pool lead batches
+// the same slots of all its runs (run-consecutive within a slot) into one
+// launch per slot.
 template <typename T, int DIR>
 cudaError_t strided_dispatch(spm_ctx *c, int slot, int nf, int axis) {
-    if (c->use_tma) {
-        cudaError_t e = plan_of<T>(c).template strided_tma<DIR>(c->cx<T>(slot), nf, c->fstride_c, axis, c->st);
-        if (e != cudaErrorNotSupported) return e;
+    auto one = [&](cplx<T> *base, int nfields, size_t stride) {
+        if (c->use_tma) {
+            cudaError_t e = plan_of<T>(c).template strided_tma<DIR>(base, nfields, stride, axis, c->st);
+            if (e != cudaErrorNotSupported) return e;
+        }
+        return plan_of<T>(c).template strided<DIR>(base, nfields, stride, axis, c->st);
+    };
+    if (c->fft_runs == 1) return one(c->cx<T>(slot), nf, c->slot_stride_c);
+    for (int k = 0; k < nf; k++) {
+        cudaError_t e = one(c->cx<T>(slot + k), c->fft_runs, c->fstride_c);
+        if (e != cudaSuccess) return e;
+        c->launches += k > 0;
     }
-    return plan_of<T>(c).template strided<DIR>(c->cx<T>(slot), nf, c->fstride_c, axis, c->st);
+    return cudaSuccess;
 }
 
 // Strided (Y/X) FFT pass, bracketed by CUDA events when profiling is on.
@@ -241,18 +300,36 @@ int fft_strided_pass(spm_ctx *c, int slot, int nf, int axis) {
         SPM_CUDA_CHECK(cudaEventRecord(b, c->st));
         c->prof_ev.push_back(a);
         c->prof_ev.push_back(b);
-        c->prof_bytes += 2.0 * nf * (double)c->g.nx * c->g.ny * c->g.hnz * sizeof(cplx<T>);
+        c->prof_bytes += 2.0 * nf * c->fft_runs * (double)c->g.nx * c->g.ny * c->g.hnz * sizeof(cplx<T>);
     } else {
         SPM_CUDA_CHECK((strided_dispatch<T, DIR>(c, slot, nf, axis)));
     }
     c->launches++;
     return SPM_OK;
 }
+// z passes over `nf` slots (one launch per slot when batching runs)
+template <typename T>
+int z_pass(spm_ctx *c, int slot, int nf, bool forward) {
+    const T scale = (T)(1.0 / ((double)c->g.nx * c->g.ny * c->g.nz));
+    auto    one   = [&](int s, int nfields, size_t stride) {
+        return forward ? plan_of<T>(c).z_r2c(c->real<T>(s), c->cx<T>(s), nfields, 2 * stride, stride, c->st)
+                       : plan_of<T>(c).z_c2r(c->cx<T>(s), c->real<T>(s), nfields, stride, 2 * stride, scale, c->st);
+    };
+    if (c->fft_runs == 1) {
+        SPM_CUDA_CHECK(one(slot, nf, c->slot_stride_c));
+        c->launches++;
+        return SPM_OK;
+    }
+    for (int k = 0; k < nf; k++) {
+        SPM_CUDA_CHECK(one(slot + k, c->fft_runs, c->fstride_c));
+        c->launches++;
+    }
+    return SPM_OK;
+}
 template <typename T>
 int fft_fwd(spm_ctx *c, int slot, int nf) {
-    SPM_CUDA_CHECK(plan_of<T>(c).z_r2c(c->real<T>(slot), c->cx<T>(slot), nf, 2 * c->fstride_c, c->fstride_c, c->st));
-    c->launches++;
     int rc;
+    if ((rc = z_pass<T>(c, slot, nf, true)) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, -1>(c, slot, nf, 1)) != SPM_OK) return rc;
     return fft_strided_pass<T, -1>(c, slot, nf, 0);
 }
@@ -261,55 +338,51 @@ int fft_inv(spm_ctx *c, int slot, int nf) {
     int rc;
     if ((rc = fft_strided_pass<T, +1>(c, slot, nf, 0)) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, +1>(c, slot, nf, 1)) != SPM_OK) return rc;
-    SPM_CUDA_CHECK(plan_of<T>(c).z_c2r(c->cx<T>(slot), c->real<T>(slot), nf, c->fstride_c, 2 * c->fstride_c,
-                                       (T)(1.0 / ((double)c->g.nx * c->g.ny * c->g.nz)), c->st));
-    c->launches++;
-    return SPM_OK;
+    return z_pass<T>(c, slot, nf, false);
 }
 
-__global__ void k_fix_cell(double *uk_dc, int fx, int fy, int fz) {
-    if (threadIdx.x == 0) {
-        if (fx) uk_dc[0] = 0.0;
-        if (fy) uk_dc[1] = 0.0;
-        if (fz) uk_dc[2] = 0.0;
-    }
-}
 __global__ void k_zero3(double *uk_dc) {
     if (threadIdx.x < 3) uk_dc[threadIdx.x] = 0.0;
 }
 
 // ---------------------------------------------------------------------------
-// Building blocks of the step (templated on the field type).
+// Building blocks of the step (templated on the field type).  The `_runs`
+// forms advance runs R[0..nr) that share one grid: per-run kernels go to each
+// run, FFT stages to L, which is either the run itself or a pool lead whose
+// FFT launches cover the same slots of every run of the pool.
 // ---------------------------------------------------------------------------
 template <typename T>
-int zeta_to_velocity(spm_ctx *c, int truncate) {
-    LAUNCH(c, k_zeta_to_u<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(Z0), c->cx<T>(Z1), c->uk_dc, c->cx<T>(U0),
-           c->cx<T>(U1), c->cx<T>(U2), truncate);
-    return fft_inv<T>(c, U0, 3);
+int zeta_to_velocity(spm_ctx *L, int truncate) {
+    LAUNCH(L, k_zeta_to_u<T>, L->pw_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
+           L->cx<T>(U1), L->cx<T>(U2), truncate, L->fstride_c);
+    return fft_inv<T>(L, U0, 3);
 }
 
-// NS_solver_slavedEuler on the context's zeta (fluid_solver.cxx:348-374).
+// NS_solver_slavedEuler (fluid_solver.cxx:348-374).
 template <typename T>
-int ns_solver(spm_ctx *c) {
+int ns_solver(spm_ctx *L) {
     int rc;
     // zeta -> u_hat (truncated) -> inverse x, y passes
-    LAUNCH(c, k_zeta_to_u<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(Z0), c->cx<T>(Z1), c->uk_dc, c->cx<T>(U0),
-           c->cx<T>(U1), c->cx<T>(U2), 1);
-    if ((rc = fft_strided_pass<T, +1>(c, U0, 3, 0)) != SPM_OK) return rc;
-    if ((rc = fft_strided_pass<T, +1>(c, U0, 3, 1)) != SPM_OK) return rc;
+    LAUNCH(L, k_zeta_to_u<T>, L->pw_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
+           L->cx<T>(U1), L->cx<T>(U2), 1, L->fstride_c);
+    if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 0)) != SPM_OK) return rc;
+    if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 1)) != SPM_OK) return rc;
     // inverse z + products + forward z in one pass, then forward y, x passes
-    SPM_CUDA_CHECK(plan_of<T>(c).z_products(c->cx<T>(U0), c->fstride_c, c->st));
-    c->launches++;
-    if ((rc = fft_strided_pass<T, -1>(c, U0, 5, 1)) != SPM_OK) return rc;
-    if ((rc = fft_strided_pass<T, -1>(c, U0, 5, 0)) != SPM_OK) return rc;
-    LAUNCH(c, k_ns_update<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(Z0), c->cx<T>(Z1), c->cx<T>(U0),
-           c->cx<T>(U1), c->cx<T>(U2), c->cx<T>(A0), c->cx<T>(A1), c->ph.nu, c->ph.dt);
+    SPM_CUDA_CHECK(plan_of<T>(L).z_products(L->cx<T>(U0), L->slot_stride_c, L->fft_runs, L->fstride_c, L->st));
+    L->launches++;
+    if ((rc = fft_strided_pass<T, -1>(L, U0, 5, 1)) != SPM_OK) return rc;
+    if ((rc = fft_strided_pass<T, -1>(L, U0, 5, 0)) != SPM_OK) return rc;
+    LAUNCH(L, k_ns_update<T>, L->pw_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->cx<T>(U0), L->cx<T>(U1),
+           L->cx<T>(U2), L->cx<T>(A0), L->cx<T>(A1), L->ph.nu, L->ph.dt, L->fstride_c);
     return SPM_OK;
 }
 
+// Shared-profile scatters (Make_phi_particle_sum, make_phi.cxx:226-247;
+// Make_phi_u_particle, make_phi.cxx:335-379 with phi taken from PHIS).
+// `clear` zeroes the target slots first; the step clears them all at once.
 template <typename T>
-int phi_sum_scatter(spm_ctx *c) {
-    SPM_CUDA_CHECK(cudaMemsetAsync(c->real<T>(PHIS), 0, c->field_bytes(), c->st));
+int phi_sum_scatter(spm_ctx *c, bool clear = true) {
+    if (clear) SPM_CUDA_CHECK(cudaMemsetAsync(c->real<T>(PHIS), 0, c->field_bytes(), c->st));
     if (c->ph.np == 0) return SPM_OK;
     dim3 grid((c->ncells + 127) / 128, c->ph.np);
     LAUNCH(c, s_phi_scatter<T>, grid, 128, 0, c->g, c->ph, c->ps.x, c->cells, c->ncells, c->real<T>(PHIS), c->err);
@@ -317,8 +390,9 @@ int phi_sum_scatter(spm_ctx *c) {
 }
 
 template <typename T>
-int up_scatter(spm_ctx *c) {
-    SPM_CUDA_CHECK(cudaMemsetAsync(c->real<T>(UP0), 0, 3 * c->field_bytes(), c->st));
+int up_scatter(spm_ctx *c, bool clear = true) {
+    if (clear)
+        for (int d = 0; d < 3; d++) SPM_CUDA_CHECK(cudaMemsetAsync(c->real<T>(UP0 + d), 0, c->field_bytes(), c->st));
     if (c->ph.np == 0) return SPM_OK;
     dim3 grid((c->ncells + 127) / 128, c->ph.np);
     LAUNCH(c, s_up_scatter<T>, grid, 128, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells, c->ncells,
@@ -326,70 +400,75 @@ int up_scatter(spm_ctx *c) {
     return SPM_OK;
 }
 
+// Zero UP0, UP1, UP2 and PHIS of every run of L in one memset (the slots are
+// consecutive; in a pool the span also covers free run slots).
+template <typename T>
+int clear_scatter_slots(spm_ctx *L) {
+    const size_t nc = (size_t)(PHIS - UP0) * L->slot_stride_c + (size_t)L->fft_runs * L->fstride_c;
+    SPM_CUDA_CHECK(cudaMemsetAsync(L->real<T>(UP0), 0, nc * 2 * sizeof(T), L->st));
+    return SPM_OK;
+}
+
 // Rigidity projection of the step: f = up - phi u formed inside the forward z
 // pass, forward y, x passes, then the projection and the update of zeta and
 // uk_dc closed in k space (k_project_add_curl).
 template <typename T>
-int rigidity_projection(spm_ctx *c) {
+int rigidity_projection(spm_ctx *L) {
     int rc;
-    SPM_CUDA_CHECK(plan_of<T>(c).z_makef(c->real<T>(UP0), c->real<T>(U0), c->real<T>(PHIS), c->fstride_c, c->st));
-    c->launches++;
-    if ((rc = fft_strided_pass<T, -1>(c, UP0, 3, 1)) != SPM_OK) return rc;
-    if ((rc = fft_strided_pass<T, -1>(c, UP0, 3, 0)) != SPM_OK) return rc;
-    LAUNCH(c, k_project_add_curl<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(UP0), c->cx<T>(UP1), c->cx<T>(UP2),
-           c->cx<T>(Z0), c->cx<T>(Z1), c->uk_dc);
-    return SPM_OK;
-}
-
-// The same projection in the reference's order (real-space f_sole, u += f,
-// forward transform of u, U_k2zeta_k); kept as the unfused reference path.
-template <typename T>
-int rigidity_projection_unfused(spm_ctx *c) {
-    int rc;
-    LAUNCH(c, r_make_f<T>, c->grid_blocks(), 256, 0, c->g, c->real<T>(UP0), c->real<T>(UP1), c->real<T>(UP2),
-           c->real<T>(U0), c->real<T>(U1), c->real<T>(U2), c->real<T>(PHIS));
-    if ((rc = fft_fwd<T>(c, UP0, 3)) != SPM_OK) return rc;
-    LAUNCH(c, k_truncate_project<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(UP0), c->cx<T>(UP1), c->cx<T>(UP2), 1);
-    if ((rc = fft_inv<T>(c, UP0, 3)) != SPM_OK) return rc;
-    LAUNCH(c, r_add3<T>, c->grid_blocks(), 256, 0, c->g, c->real<T>(U0), c->real<T>(U1), c->real<T>(U2),
-           c->real<T>(UP0), c->real<T>(UP1), c->real<T>(UP2));
-    if ((rc = fft_fwd<T>(c, U0, 3)) != SPM_OK) return rc;
-    LAUNCH(c, k_u_to_zeta<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(U0), c->cx<T>(U1), c->cx<T>(U2),
-           c->cx<T>(Z0), c->cx<T>(Z1), c->uk_dc);
+    SPM_CUDA_CHECK(plan_of<T>(L).z_makef(L->real<T>(UP0), L->real<T>(U0), L->real<T>(PHIS), L->slot_stride_c,
+                                         L->fft_runs, L->fstride_c, L->st));
+    L->launches++;
+    if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 1)) != SPM_OK) return rc;
+    if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 0)) != SPM_OK) return rc;
+    LAUNCH(L, k_project_add_curl<T>, L->pw_grid(), 256, 0, L->g, L->cx<T>(UP0), L->cx<T>(UP1), L->cx<T>(UP2),
+           L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->fstride_c);
     return SPM_OK;
 }
 
 int particle_blocks(spm_ctx *c) { return (c->ph.np + 127) / 128; }
 
-// Time_evolution_hydro (sp_3d_ns.cxx:41-194), Navier_Stokes with free spheres.
+// Time_evolution_hydro (sp_3d_ns.cxx:41-194), Navier_Stokes with free
+// spheres.  L batches the grid stages of runs R[0..nr), which are L's runs in
+// order (L is the run itself for a single context); particle kernels go to
+// each run on the shared stream.
 template <typename T>
-int step_ns(spm_ctx *c) {
+int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
     int rc;
-    if ((rc = ns_solver<T>(c)) != SPM_OK) return rc;
-    LAUNCH(c, k_fix_cell, 1, 32, 0, c->uk_dc, c->ph.fix_cell[0], c->ph.fix_cell[1], c->ph.fix_cell[2]);
-    if ((rc = zeta_to_velocity<T>(c, 1)) != SPM_OK) return rc;
-    const int euler = c->ts == 0 ? 1 : 0;
-    if (c->ph.np > 0) LAUNCH(c, p_position, particle_blocks(c), 128, 0, c->ph, c->ps, euler, 1);
-    if ((rc = phi_sum_scatter<T>(c)) != SPM_OK) return rc;
-    if (c->ph.np > 0) {
+    if ((rc = ns_solver<T>(L)) != SPM_OK) return rc;
+    LAUNCH(L, k_fix_cell, (nr + 127) / 128, 128, 0, L->rw, nr);
+    if ((rc = zeta_to_velocity<T>(L, 1)) != SPM_OK) return rc;
+    if ((rc = clear_scatter_slots<T>(L)) != SPM_OK) return rc;
+    for (int r = 0; r < nr; r++) {
+        spm_ctx *c = R[r];
+        if (c->ph.np == 0) continue;
+        LAUNCH(c, p_position, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev, 1);
+        if ((rc = phi_sum_scatter<T>(c, false)) != SPM_OK) return rc;
         LAUNCH(c, s_hydro_force<T>, c->ph.np, 256, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
                c->ncells, c->real<T>(PHIS), c->real<T>(U0), c->real<T>(U1), c->real<T>(U2), c->ps.f_hydro,
                c->ps.torque_hydro);
         LAUNCH(c, p_forces, (c->ph.np + 3) / 4, 128, 0, c->ph, c->ps, 0, 0.0);
-        LAUNCH(c, p_velocity, particle_blocks(c), 128, 0, c->ph, c->ps, euler);
+        LAUNCH(c, p_velocity, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev);
         if (c->P.kbt > 0.0) LAUNCH(c, p_thermostat_serial, 1, 32, 0, c->ph, c->ps, c->mt);
+        if ((rc = up_scatter<T>(c, false)) != SPM_OK) return rc;
     }
-    if ((rc = up_scatter<T>(c)) != SPM_OK) return rc;
-    if ((rc = rigidity_projection<T>(c)) != SPM_OK) return rc;
-    c->ts++;
-    c->time += c->ph.dt;
+    if ((rc = rigidity_projection<T>(L)) != SPM_OK) return rc;
+    LAUNCH(L, k_ts_advance, (nr + 127) / 128, 128, 0, L->rw, nr);
+    for (int r = 0; r < nr; r++) {
+        R[r]->ts++;
+        R[r]->time += R[r]->ph.dt;
+    }
     return SPM_OK;
+}
+template <typename T>
+int step_ns(spm_ctx *c) {
+    return step_ns_runs<T>(c, &c, 1);
 }
 
 template <typename T>
 int initialize_impl(spm_ctx *c) {
     int rc;
-    SPM_CUDA_CHECK(cudaMemsetAsync(c->arena, 0, NSLOT * c->field_bytes(), c->st));
+    for (int sl = 0; sl < NSLOT; sl++) SPM_CUDA_CHECK(cudaMemsetAsync(c->real<T>(sl), 0, c->field_bytes(), c->st));
+    SPM_CUDA_CHECK(cudaMemsetAsync(c->ts_dev, 0, sizeof(int), c->st));
     LAUNCH(c, k_zero3, 1, 32, 0, c->uk_dc);
     if ((rc = phi_sum_scatter<T>(c)) != SPM_OK) return rc;
     if ((rc = up_scatter<T>(c)) != SPM_OK) return rc;
@@ -502,6 +581,162 @@ int download_particles(spm_ctx *c, double *rec) {
     return SPM_OK;
 }
 
+void destroy_ctx(spm_ctx *c) {
+    if (!c) return;
+    if (c->st) cudaStreamSynchronize(c->st);
+    c->plan64.destroy();
+    c->plan32.destroy();
+    if (c->owns_arena) dev_free(c->arena);
+    if (c->owns_rw) dev_free(c->rw);
+    dev_free(c->cells);
+    dev_free(c->pbuf);
+    dev_free(c->mt);
+    dev_free(c->le.dev);
+    dev_free(c->le.ppart);
+    dev_free(c->le.partial);
+    if (c->own_stream && c->st) cudaStreamDestroy(c->st);
+    delete c;
+}
+
+// Creates a context of one of three kinds:
+//  - a lone run (pool_cap == 0, lead == nullptr): own arena of NSLOT fields,
+//    own RunWords and FFT plan;
+//  - a pool lead (pool_cap > 0, lead == nullptr): no particles; arena of
+//    NSLOT x pool_cap fields, slot-major, RunWords[pool_cap + 1] (the last one
+//    holds the lead's own error word) and the FFT plan the pool's runs share;
+//  - a pool run (lead != nullptr) at run slot `slot` of the lead's arena.
+int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *lead, int slot, spm_ctx **out) {
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SPM_ERR_NO_DEVICE, "no CUDA device visible");
+    spm_ctx *c = new spm_ctx();
+    c->P       = p;
+    if (pool_cap > 0) c->P.n_particles = 0;
+    int rc = derive(c->P, c->g, c->ph);
+    if (rc != SPM_OK) {
+        delete c;
+        return rc;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (stream) {
+        c->st = stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+            delete c;
+            return fail(SPM_ERR_CUDA, "stream creation failed");
+        }
+        c->own_stream = true;
+    }
+    c->fstride_c    = (size_t)c->g.nx * c->g.ny * c->g.hnzp;
+    const int nslot = (p.equation == SPM_EQ_LEES_EDWARDS) ? NSLOT + LE_EXTRA_SLOTS : NSLOT;
+    {
+        const char *nt = getenv("SPM_NO_TMA");
+        c->use_tma     = !(nt && nt[0] == '1');
+    }
+    cudaError_t e = cudaSuccess;
+    if (lead) {
+        c->owns_arena    = false;
+        c->owns_rw       = false;
+        c->slot_stride_c = lead->slot_stride_c;
+        const size_t es  = c->elem_bytes();
+        c->arena         = static_cast<char *>(lead->arena) + (size_t)slot * c->fstride_c * 2 * es;
+        c->rw            = lead->rw + slot;
+        c->pp64          = lead->pp64;
+        c->pp32          = lead->pp32;
+        c->use_tma       = lead->use_tma;
+    } else {
+        const int nruns  = pool_cap > 0 ? pool_cap : 1;
+        c->slot_stride_c = (size_t)nruns * c->fstride_c;
+        e                = dev_alloc(&c->arena, (size_t)nslot * nruns * c->field_bytes());
+        if (e != cudaSuccess) {
+            destroy_ctx(c);
+            return fail(SPM_ERR_NOMEM, std::string("field arena: ") + cudaGetErrorString(e));
+        }
+        e = dev_alloc((void **)&c->rw, (size_t)(pool_cap > 0 ? pool_cap + 1 : 1) * sizeof(RunWords));
+        if (e != cudaSuccess) {
+            destroy_ctx(c);
+            return fail(SPM_ERR_NOMEM, "run words");
+        }
+        e = c->fp64() ? c->plan64.create(c->g) : c->plan32.create(c->g);
+        c->plan64.sm_count = c->plan32.sm_count = c->sm_count;
+        if (e != cudaSuccess) {
+            destroy_ctx(c);
+            return fail(SPM_ERR_CUDA, std::string("FFT plan: ") + cudaGetErrorString(e));
+        }
+        if (pool_cap > 0) {
+            cudaMemset(c->rw, 0, (size_t)(pool_cap + 1) * sizeof(RunWords));
+            c->uk_dc  = c->rw->uk_dc;
+            c->ts_dev = &c->rw->ts;
+            c->err    = &c->rw[pool_cap].err;
+            c->plan64.err = c->plan32.err = c->err;
+            if (cudaDeviceSynchronize() != cudaSuccess) {
+                destroy_ctx(c);
+                return fail(SPM_ERR_CUDA, "pool lead setup");
+            }
+            *out = c;
+            return SPM_OK;
+        }
+    }
+    set_run_words(c);
+    if (!lead) c->plan64.err = c->plan32.err = c->err;
+    std::vector<int> cells = sekibun(p);
+    c->ncells              = (int)cells.size();
+    const int np           = std::max(p.n_particles, 1);
+    if (dev_alloc((void **)&c->cells, cells.size() * sizeof(int)) != cudaSuccess ||
+        dev_alloc((void **)&c->pbuf, (size_t)np * kPWords * sizeof(double)) != cudaSuccess ||
+        dev_alloc((void **)&c->mt, 625 * sizeof(unsigned int)) != cudaSuccess) {
+        destroy_ctx(c);
+        return fail(SPM_ERR_NOMEM, "small device buffers");
+    }
+    cudaMemcpy(c->cells, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemset(c->pbuf, 0, (size_t)np * kPWords * sizeof(double));
+    unsigned int mt[625];
+    mt_init(p.mt_seed, mt);
+    cudaMemcpy(c->mt, mt, sizeof(mt), cudaMemcpyHostToDevice);
+    // particle arrays: 12 three-vectors in record order, then q, q_old, then
+    // x_previous, torque_r, torque_r_previous (3-vectors) and lj_stress
+    double *b = c->pbuf;
+    auto    v3 = [&](int i) { return b + (size_t)i * np * 3; };
+    c->ps.x                     = v3(0);
+    c->ps.x_nopbc               = v3(1);
+    c->ps.v                     = v3(2);
+    c->ps.v_old                 = v3(3);
+    c->ps.omega                 = v3(4);
+    c->ps.omega_old             = v3(5);
+    c->ps.f_hydro               = v3(6);
+    c->ps.f_hydro_previous      = v3(7);
+    c->ps.torque_hydro          = v3(8);
+    c->ps.torque_hydro_previous = v3(9);
+    c->ps.fr                    = v3(10);
+    c->ps.fr_previous           = v3(11);
+    c->ps.q                     = b + (size_t)12 * np * 3;
+    c->ps.q_old                 = c->ps.q + (size_t)np * 4;
+    c->ps.x_previous            = c->ps.q_old + (size_t)np * 4;
+    c->ps.torque_r              = c->ps.x_previous + (size_t)np * 3;
+    c->ps.torque_r_previous     = c->ps.torque_r + (size_t)np * 3;
+    c->ps.mdf                   = c->ps.torque_r_previous + (size_t)np * 3;
+    c->ps.lj_stress             = c->ps.mdf + (size_t)np * 3;
+    le_init(c->le, c->g, c->ph, p);
+    if (c->le.enabled) {
+        if (dev_alloc((void **)&c->le.dev, sizeof(LEDev)) != cudaSuccess ||
+            dev_alloc((void **)&c->le.ppart, (size_t)np * 6 * sizeof(double)) != cudaSuccess ||
+            dev_alloc((void **)&c->le.partial, (size_t)c->grid_blocks() * sizeof(double)) != cudaSuccess) {
+            destroy_ctx(c);
+            return fail(SPM_ERR_NOMEM, "Lees-Edwards buffers");
+        }
+        cudaMemset(c->le.dev, 0, sizeof(LEDev));
+    }
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        destroy_ctx(c);
+        return fail(SPM_ERR_CUDA, std::string("create: ") + cudaGetErrorString(e));
+    }
+    *out = c;
+    return SPM_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -557,122 +792,13 @@ int spm_device_bytes(const spm_params *p, size_t *bytes) {
 
 int spm_create(const spm_params *p, void *stream, spm_ctx **out) {
     if (!p || !out) return fail(SPM_ERR_ARG, "null argument");
-    *out = nullptr;
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SPM_ERR_NO_DEVICE, "no CUDA device visible");
-    spm_ctx *c = new spm_ctx();
-    c->P       = *p;
-    int rc     = derive(*p, c->g, c->ph);
-    if (rc != SPM_OK) {
-        delete c;
-        return rc;
-    }
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, dev);
-    if (stream) {
-        c->st = static_cast<cudaStream_t>(stream);
-    } else {
-        if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
-            delete c;
-            return fail(SPM_ERR_CUDA, "stream creation failed");
-        }
-        c->own_stream = true;
-    }
-    c->fstride_c      = (size_t)c->g.nx * c->g.ny * c->g.hnzp;
-    const int nslot   = (p->equation == SPM_EQ_LEES_EDWARDS) ? NSLOT + LE_EXTRA_SLOTS : NSLOT;
-    cudaError_t e     = cudaMalloc(&c->arena, (size_t)nslot * c->field_bytes());
-    if (e != cudaSuccess) {
-        spm_destroy(c);
-        return fail(SPM_ERR_NOMEM, std::string("field arena: ") + cudaGetErrorString(e));
-    }
-    e = c->fp64() ? c->plan64.create(c->g) : c->plan32.create(c->g);
-    c->plan64.sm_count = c->plan32.sm_count = c->sm_count;
-    {
-        const char *nt = getenv("SPM_NO_TMA");
-        c->use_tma     = !(nt && nt[0] == '1');
-    }
-    if (e != cudaSuccess) {
-        spm_destroy(c);
-        return fail(SPM_ERR_CUDA, std::string("FFT plan: ") + cudaGetErrorString(e));
-    }
-    std::vector<int> cells = sekibun(*p);
-    c->ncells              = (int)cells.size();
-    const int np           = std::max(p->n_particles, 1);
-    if (cudaMalloc(&c->cells, cells.size() * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&c->uk_dc, 4 * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&c->pbuf, (size_t)np * kPWords * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&c->mt, 625 * sizeof(unsigned int)) != cudaSuccess ||
-        cudaMalloc(&c->err, sizeof(unsigned int)) != cudaSuccess) {
-        spm_destroy(c);
-        return fail(SPM_ERR_NOMEM, "small device buffers");
-    }
-    c->plan64.err = c->plan32.err = c->err;
-    cudaMemcpy(c->cells, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice);
-    cudaMemset(c->err, 0, sizeof(unsigned int));
-    cudaMemset(c->pbuf, 0, (size_t)np * kPWords * sizeof(double));
-    cudaMemset(c->uk_dc, 0, 4 * sizeof(double));
-    unsigned int mt[625];
-    mt_init(p->mt_seed, mt);
-    cudaMemcpy(c->mt, mt, sizeof(mt), cudaMemcpyHostToDevice);
-    // particle arrays: 12 three-vectors in record order, then q, q_old, then
-    // x_previous, torque_r, torque_r_previous (3-vectors) and lj_stress
-    double *b = c->pbuf;
-    auto    v3 = [&](int i) { return b + (size_t)i * np * 3; };
-    c->ps.x                     = v3(0);
-    c->ps.x_nopbc               = v3(1);
-    c->ps.v                     = v3(2);
-    c->ps.v_old                 = v3(3);
-    c->ps.omega                 = v3(4);
-    c->ps.omega_old             = v3(5);
-    c->ps.f_hydro               = v3(6);
-    c->ps.f_hydro_previous      = v3(7);
-    c->ps.torque_hydro          = v3(8);
-    c->ps.torque_hydro_previous = v3(9);
-    c->ps.fr                    = v3(10);
-    c->ps.fr_previous           = v3(11);
-    c->ps.q                     = b + (size_t)12 * np * 3;
-    c->ps.q_old                 = c->ps.q + (size_t)np * 4;
-    c->ps.x_previous            = c->ps.q_old + (size_t)np * 4;
-    c->ps.torque_r              = c->ps.x_previous + (size_t)np * 3;
-    c->ps.torque_r_previous     = c->ps.torque_r + (size_t)np * 3;
-    c->ps.mdf                   = c->ps.torque_r_previous + (size_t)np * 3;
-    c->ps.lj_stress             = c->ps.mdf + (size_t)np * 3;
-    le_init(c->le, c->g, c->ph, *p);
-    if (c->le.enabled) {
-        if (cudaMalloc(&c->le.dev, sizeof(LEDev)) != cudaSuccess ||
-            cudaMalloc(&c->le.ppart, (size_t)np * 6 * sizeof(double)) != cudaSuccess ||
-            cudaMalloc(&c->le.partial, (size_t)c->grid_blocks() * sizeof(double)) != cudaSuccess) {
-            spm_destroy(c);
-            return fail(SPM_ERR_NOMEM, "Lees-Edwards buffers");
-        }
-        cudaMemset(c->le.dev, 0, sizeof(LEDev));
-    }
-    e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) {
-        spm_destroy(c);
-        return fail(SPM_ERR_CUDA, std::string("create: ") + cudaGetErrorString(e));
-    }
-    *out = c;
-    return SPM_OK;
+    return create_ctx(*p, static_cast<cudaStream_t>(stream), 0, nullptr, 0, out);
 }
 
 int spm_destroy(spm_ctx *c) {
     if (!c) return SPM_OK;
-    if (c->st) cudaStreamSynchronize(c->st);
-    c->plan64.destroy();
-    c->plan32.destroy();
-    cudaFree(c->arena);
-    cudaFree(c->cells);
-    cudaFree(c->uk_dc);
-    cudaFree(c->pbuf);
-    cudaFree(c->mt);
-    cudaFree(c->err);
-    cudaFree(c->le.dev);
-    cudaFree(c->le.ppart);
-    cudaFree(c->le.partial);
-    if (c->own_stream && c->st) cudaStreamDestroy(c->st);
-    delete c;
+    if (c->pool) return fail(SPM_ERR_ARG, "the run belongs to a pool: release it with spm_pool_release");
+    destroy_ctx(c);
     return SPM_OK;
 }
 
@@ -774,8 +900,8 @@ int spm_get_shear_state(spm_ctx *c, double *degree_oblique, double stress[8]) {
 
 int spm_fft_forward_dev(spm_ctx *c, void *data, int nfields, size_t field_stride) {
     if (!c || !data || nfields < 1) return fail(SPM_ERR_ARG, "bad argument");
-    cudaError_t e = c->fp64() ? c->plan64.forward((double *)data, nfields, field_stride, c->st)
-                              : c->plan32.forward((float *)data, nfields, field_stride, c->st);
+    cudaError_t e = c->fp64() ? c->pp64->forward((double *)data, nfields, field_stride, c->st)
+                              : c->pp32->forward((float *)data, nfields, field_stride, c->st);
     c->launches += 3;
     SPM_CUDA_CHECK(e);
     return SPM_OK;
@@ -783,8 +909,8 @@ int spm_fft_forward_dev(spm_ctx *c, void *data, int nfields, size_t field_stride
 
 int spm_fft_inverse_dev(spm_ctx *c, void *data, int nfields, size_t field_stride) {
     if (!c || !data || nfields < 1) return fail(SPM_ERR_ARG, "bad argument");
-    cudaError_t e = c->fp64() ? c->plan64.inverse((cplx<double> *)data, nfields, field_stride, c->st)
-                              : c->plan32.inverse((cplx<float> *)data, nfields, field_stride, c->st);
+    cudaError_t e = c->fp64() ? c->pp64->inverse((cplx<double> *)data, nfields, field_stride, c->st)
+                              : c->pp32->inverse((cplx<float> *)data, nfields, field_stride, c->st);
     c->launches += 3;
     SPM_CUDA_CHECK(e);
     return SPM_OK;
@@ -845,3 +971,4 @@ int spm_kernel_launches(spm_ctx *c, long long *count, int reset) {
 }  // extern "C"
 
 #include "spm_api_boundary.inc"
+#include "spm_pool.inc"

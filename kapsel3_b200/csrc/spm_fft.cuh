@@ -387,9 +387,10 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
 // ---------------------------------------------------------------------------
 template <typename T, int M, int R>
 __global__ void __launch_bounds__(R *Split<M>::N1)
-    fft_z_products_kernel(cplx<T> *io, size_t field_stride_c, int nrows, int hnzp,
+    fft_z_products_kernel(cplx<T> *io, size_t field_stride_c, size_t run_stride_c, int nrows, int hnzp,
                           const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale) {
     constexpr int P = Split<M>::N1;
+    io += (size_t)blockIdx.y * run_stride_c;  // run of a batched pool
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T       *U  = reinterpret_cast<T *>(smem_raw);                   // [3][R][2M]
     cplx<T> *ws = reinterpret_cast<cplx<T> *>(U + 3 * R * 2 * M);     // [R][M+1]
@@ -442,8 +443,12 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
 template <typename T, int M, int R>
 __global__ void __launch_bounds__(R *Split<M>::N1)
     fft_z_makef_kernel(T *up, const T *__restrict__ u, const T *__restrict__ phi_sum, size_t field_stride_c,
-                       int nrows, int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN) {
+                       size_t run_stride_c, int nrows, int hnzp, const cplx<T> *__restrict__ twM,
+                       const cplx<T> *__restrict__ twN) {
     constexpr int P = Split<M>::N1;
+    up += (size_t)blockIdx.y * 2 * run_stride_c;  // run of a batched pool
+    u += (size_t)blockIdx.y * 2 * run_stride_c;
+    phi_sum += (size_t)blockIdx.y * 2 * run_stride_c;
     __shared__ __align__(16) cplx<T> s[R][M];
     const int r   = threadIdx.x / P;
     const int t   = threadIdx.x % P;

@@ -36,15 +36,16 @@ struct FFTPlan {
     static bool size_ok(int n) { return n >= 8 && n <= 512 && (n & (n - 1)) == 0; }
 
     // Fused inverse-z / advection products / forward-z pass over five slots.
-    cudaError_t z_products(cplx<T> *io, size_t fs_c, cudaStream_t st) const {
+    cudaError_t z_products(cplx<T> *io, size_t fs_c, int nruns, size_t run_stride_c, cudaStream_t st) const {
         const int nrows = g.nx * g.ny;
         const T   scale = (T)(1.0 / ((double)g.nx * g.ny * g.nz));
         switch (g.nz / 2) {
-#define SPM_ZP(MM)                                                                                        \
-    case MM: {                                                                                            \
-        constexpr int RR = prows(MM);                                                                     \
-        fft_z_products_kernel<T, MM, RR><<<(nrows + RR - 1) / RR, RR * Split<MM>::N1, psmem(MM), st>>>( \
-            io, fs_c, nrows, g.hnzp, tw_zm, tw_zn, scale);                                                \
+#define SPM_ZP(MM)                                                                                  \
+    case MM: {                                                                                      \
+        constexpr int RR = prows(MM);                                                               \
+        fft_z_products_kernel<T, MM, RR>                                                            \
+            <<<dim3((nrows + RR - 1) / RR, nruns), RR * Split<MM>::N1, psmem(MM), st>>>(            \
+                io, fs_c, run_stride_c, nrows, g.hnzp, tw_zm, tw_zn, scale);                        \
     } break;
             SPM_ZP(4) SPM_ZP(8) SPM_ZP(16) SPM_ZP(32) SPM_ZP(64) SPM_ZP(128) SPM_ZP(256)
 #undef SPM_ZP
@@ -53,14 +54,15 @@ struct FFTPlan {
         return cudaGetLastError();
     }
     // Fused f = up - min(phi_sum,1) u and forward z pass (three fields).
-    cudaError_t z_makef(T *up, const T *u, const T *phis, size_t fs_c, cudaStream_t st) const {
+    cudaError_t z_makef(T *up, const T *u, const T *phis, size_t fs_c, int nruns, size_t run_stride_c,
+                        cudaStream_t st) const {
         const int nrows = g.nx * g.ny;
         switch (g.nz / 2) {
-#define SPM_ZF(MM)                                                                                    \
-    case MM: {                                                                                        \
-        constexpr int RR = zrows(MM);                                                                 \
-        fft_z_makef_kernel<T, MM, RR><<<(nrows + RR - 1) / RR, RR * Split<MM>::N1, 0, st>>>(          \
-            up, u, phis, fs_c, nrows, g.hnzp, tw_zm, tw_zn);                                          \
+#define SPM_ZF(MM)                                                                                         \
+    case MM: {                                                                                             \
+        constexpr int RR = zrows(MM);                                                                      \
+        fft_z_makef_kernel<T, MM, RR><<<dim3((nrows + RR - 1) / RR, nruns), RR * Split<MM>::N1, 0, st>>>( \
+            up, u, phis, fs_c, run_stride_c, nrows, g.hnzp, tw_zm, tw_zn);                                 \
     } break;
             SPM_ZF(4) SPM_ZF(8) SPM_ZF(16) SPM_ZF(32) SPM_ZF(64) SPM_ZF(128) SPM_ZF(256)
 #undef SPM_ZF

@@ -8,6 +8,19 @@
 
 namespace spm {
 
+// Small per-run device words: uk_dc (the k = 0 velocity, FP64), the step
+// counter (0 selects the Euler start of the integrators), the FIX_CELLxyz
+// mask and the run's device error word.  Runs of a pool keep theirs in one
+// array, run-consecutive, so one copy reads every run's counter and errors.
+struct RunWords {
+    double       uk_dc[4];
+    int          ts;
+    int          fix_mask;
+    unsigned int err;
+    int          pad;
+};
+constexpr int kRunWordStride = sizeof(RunWords) / sizeof(double);
+
 // ---------------------------------------------------------------------------
 // Physical constants of one run, passed by value to every kernel.
 // ---------------------------------------------------------------------------
@@ -113,7 +126,10 @@ __device__ __forceinline__ void i_cross(T kx, T ky, T kz, const cplx<T> a[3], cp
 template <typename T>
 __global__ void k_zeta_to_u(Grid g, const cplx<T> *__restrict__ z0p, const cplx<T> *__restrict__ z1p,
                             const double *__restrict__ uk_dc, cplx<T> *__restrict__ u0, cplx<T> *__restrict__ u1,
-                            cplx<T> *__restrict__ u2, int truncate) {
+                            cplx<T> *__restrict__ u2, int truncate, size_t run_stride_c) {
+    const size_t ro = blockIdx.y * run_stride_c;
+    z0p += ro, z1p += ro, u0 += ro, u1 += ro, u2 += ro;
+    uk_dc += blockIdx.y * kRunWordStride;
     const size_t n = g.field_elems_c();
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
         KPoint p;
@@ -173,7 +189,9 @@ template <typename T>
 __global__ void k_ns_update(Grid g, cplx<T> *__restrict__ z0p, cplx<T> *__restrict__ z1p,
                             const cplx<T> *__restrict__ p_u2u3, const cplx<T> *__restrict__ p_u3u1,
                             const cplx<T> *__restrict__ p_u1u2, const cplx<T> *__restrict__ p_a0,
-                            const cplx<T> *__restrict__ p_a1, double nu, double dt) {
+                            const cplx<T> *__restrict__ p_a1, double nu, double dt, size_t run_stride_c) {
+    const size_t ro = blockIdx.y * run_stride_c;
+    z0p += ro, z1p += ro, p_u2u3 += ro, p_u3u1 += ro, p_u1u2 += ro, p_a0 += ro, p_a1 += ro;
     const size_t n = g.field_elems_c();
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
         KPoint p;
@@ -295,7 +313,10 @@ __global__ void k_u_to_zeta(Grid g, const cplx<T> *__restrict__ u0, const cplx<T
 template <typename T>
 __global__ void k_project_add_curl(Grid g, const cplx<T> *__restrict__ f0p, const cplx<T> *__restrict__ f1p,
                                    const cplx<T> *__restrict__ f2p, cplx<T> *__restrict__ z0p,
-                                   cplx<T> *__restrict__ z1p, double *__restrict__ uk_dc) {
+                                   cplx<T> *__restrict__ z1p, double *__restrict__ uk_dc, size_t run_stride_c) {
+    const size_t ro = blockIdx.y * run_stride_c;
+    f0p += ro, f1p += ro, f2p += ro, z0p += ro, z1p += ro;
+    uk_dc += blockIdx.y * kRunWordStride;
     const size_t n = g.field_elems_c();
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
         KPoint p;
@@ -583,9 +604,12 @@ __device__ __forceinline__ void qtn_normalize_d(double *q) {
 // orientation updates (particle_rotation_solver.h:23-29, 72-81) and PBC
 // (periodic_boundary.h:9-16).
 // wrap = 0 leaves the periodic wrap to p_le_wrap (Lees-Edwards image).
-__global__ void p_position(Phys ph, PState s, int euler, int wrap) {
+// The Euler start (ts == 0) is read from the run's device step counter, so a
+// captured step graph serves every step.
+__global__ void p_position(Phys ph, PState s, const int *__restrict__ ts_dev, int wrap) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= ph.np) return;
+    const int euler = *ts_dev == 0;
     for (int d = 0; d < 3; d++) {
         const int i       = 3 * n + d;
         s.x_previous[i]   = s.x[i];
@@ -734,9 +758,10 @@ __global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift) {
 
 // MD_solver_velocity_Euler / _AB2_hydro (particle_solver.cxx:103-142,
 // 239-281) followed by reset_Forces (particle_solver.cxx:11-37).
-__global__ void p_velocity(Phys ph, PState s, int euler) {
+__global__ void p_velocity(Phys ph, PState s, const int *__restrict__ ts_dev) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= ph.np) return;
+    const int euler = *ts_dev == 0;
     const double dmy = (euler ? ph.dt : ph.hdt) * ph.imass;
     const double dmr = (euler ? ph.dt : ph.hdt) * ph.imoi;
     for (int d = 0; d < 3; d++) {
@@ -764,9 +789,10 @@ __global__ void p_velocity(Phys ph, PState s, int euler) {
 // The Lees-Edwards velocity update also records momentum_depend_fr, the LJ
 // and body-force impulse used by the next step's hydrodynamic stress
 // (MD_solver_velocity_*_OBL, particle_solver.cxx:336-432).
-__global__ void p_velocity_mdf(Phys ph, PState s, int euler) {
+__global__ void p_velocity_mdf(Phys ph, PState s, const int *__restrict__ ts_dev) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= ph.np) return;
+    const int euler = *ts_dev == 0;
     for (int d = 0; d < 3; d++) {
         const int i = 3 * n + d;
         s.mdf[i]    = euler ? ph.dt * s.fr[i] : ph.hdt * (s.fr[i] + s.fr_previous[i]);
@@ -793,6 +819,23 @@ __global__ void p_velocity_mdf(Phys ph, PState s, int euler) {
         s.torque_hydro_previous[i] = s.torque_hydro[i];
         s.torque_hydro[i]          = 0.0;
     }
+}
+
+// Advances the device step counters of `nr` consecutive runs (end of every
+// step).
+__global__ void k_ts_advance(RunWords *rw, int nr) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nr) rw[r].ts += 1;
+}
+
+// FIX_CELLxyz (sp_3d_ns.cxx:45-51): zero the selected uk_dc components of
+// `nr` consecutive runs, each with its own mask (bit d = axis d).
+__global__ void k_fix_cell(RunWords *rw, int nr) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nr) return;
+    const int m = rw[r].fix_mask;
+    for (int d = 0; d < 3; d++)
+        if (m & (1 << d)) rw[r].uk_dc[d] = 0.0;
 }
 
 // ---------------------------------------------------------------------------

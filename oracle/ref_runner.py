@@ -34,19 +34,23 @@ PARTICLE_FIELDS = [("x", 3), ("x_nopbc", 3), ("v", 3), ("v_old", 3), ("omega", 3
 PARTICLE_WORDS = sum(n for _, n in PARTICLE_FIELDS)
 
 
-def ref_binary(omp: bool = False) -> Optional[str]:
-    p = os.path.join(REF_DIR, "kapsel_ref_omp" if omp else "kapsel_ref")
+def ref_binary(omp: bool = False, gpu_shim: bool = False) -> Optional[str]:
+    """kapsel_ref (serial), kapsel_ref_omp (OpenMP) or kapsel_gpu (serial, with
+    the reference's boundary functions linked to the B200 library through
+    kapsel3_b200/shim)."""
+    name = "kapsel_gpu" if gpu_shim else ("kapsel_ref_omp" if omp else "kapsel_ref")
+    p = os.path.join(REF_DIR, name)
     return p if os.access(p, os.X_OK) else None
 
 
-def available(omp: bool = False) -> bool:
-    return ref_binary(omp) is not None
+def available(omp: bool = False, gpu_shim: bool = False) -> bool:
+    return ref_binary(omp, gpu_shim) is not None
 
 
 def run_reference(keys_path: str, dump_path: Optional[str] = None, fields_every: int = 1,
                   body_force=(0.0, 0.0, 0.0), omp: bool = False, threads: Optional[int] = None,
-                  step_times_path: Optional[str] = None, timeout: float = 3600.0) -> str:
-    exe = ref_binary(omp)
+                  step_times_path: Optional[str] = None, timeout: float = 3600.0, gpu_shim: bool = False) -> str:
+    exe = ref_binary(omp, gpu_shim)
     if exe is None:
         raise FileNotFoundError("oracle/_ref is not built (make -C oracle/ref_build)")
     env = dict(os.environ)

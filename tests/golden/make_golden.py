@@ -49,6 +49,14 @@ CASES = {
                  shear_rate=0.02, num_snap=40),
         init=dict(seed=13, v_sd=1e-3, random_orientation=True), field_steps=(40,),
         tweak=dict(index=0, x=(6.3, 31.998, 16.2), v=(0.0, 0.08, 0.0))),
+    # C2 of the benchmark plan: 128^3, 200 spheres a=5, random orientations,
+    # Gaussian velocities, thermostat kT=1e-4 (MT19937 seed 0), 1000 steps;
+    # particle state every 50 steps (GTS=50), velocity checksums and the z=0
+    # plane of u at steps 500 and 1000 (zeta modes are not stored at this size)
+    "c2_128_200_spheres_thermostat": dict(
+        cfg=dict(npx=7, npy=7, npz=7, n_particles=200, a=5.0, a_xi=2.0, dt=0.05, kbt=1e-4, gts=50, num_snap=20),
+        init=dict(seed=2, v_sd=1e-3, random_orientation=True), field_steps=(500, 1000), fields_every=10,
+        zeta=False),
     # Lees-Edwards: strain passes XYaspect = 1, the oblique grid is remapped
     "le_32_strain_remap": dict(
         cfg=dict(npx=5, npy=5, npz=5, n_particles=3, a=3.0, a_xi=2.0, dt=0.05, equation=EQ_LE, shear_rate=0.6,
@@ -81,7 +89,8 @@ def make_case(name, spec):
         keys = os.path.join(td, "run.keys")
         dump = os.path.join(td, "run.dump")
         write_udf_keys(keys, cfg, parts, out_dir=os.path.join(td, "avs"))
-        err = ref_runner.run_reference(keys, dump_path=dump, fields_every=1, body_force=cfg.body_force)
+        err = ref_runner.run_reference(keys, dump_path=dump, fields_every=spec.get("fields_every", 1),
+                                       body_force=cfg.body_force, timeout=4 * 3600.0)
         d = ref_runner.read_dump(dump)
     frames = d["frames"]
     out = {"config_json": np.array(json.dumps(dataclasses.asdict(cfg))),
@@ -101,11 +110,13 @@ def make_case(name, spec):
         rows = [[float(v) for v in l.split()] for l in err.splitlines()
                 if l and not l.startswith("#") and len(l.split()) == 12]
         out["stress_lines"] = np.array(rows)
-    fs = [s for s in spec["field_steps"] if s < len(frames)]
+    by_ts = {int(f["ts"]): f for f in frames}
+    fs = [s for s in spec["field_steps"] if s in by_ts]
     out["field_steps"] = np.array(fs)
     for s in fs:
-        f = frames[s]
-        out[f"zeta_retained_{s}"] = retained_modes(cfg, f["zeta"])
+        f = by_ts[s]
+        if spec.get("zeta", True):
+            out[f"zeta_retained_{s}"] = retained_modes(cfg, f["zeta"])
         if "u" not in f:
             out[f"phi_plane_{s}"] = f["phi"][:, :, 0].copy()
             continue

@@ -16,6 +16,16 @@ def fixture_names():
     return sorted(os.path.splitext(os.path.basename(p))[0] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
 
 
+def small_fixture_names(max_points=64 ** 3):
+    """Fixtures on grids the numpy oracle steps in well under a second."""
+    out = []
+    for n in fixture_names():
+        c = json.loads(str(np.load(os.path.join(GOLDEN, n + ".npz"))["config_json"]))
+        if (1 << c["npx"]) * (1 << c["npy"]) * (1 << c["npz"]) <= max_points:
+            out.append(n)
+    return out
+
+
 def load(name):
     z = np.load(os.path.join(GOLDEN, name + ".npz"))
     c = json.loads(str(z["config_json"]))
@@ -43,11 +53,14 @@ def rel(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / (nb if nb > 0 else 1.0))
 
 
-def check_state(z, ts, cfg, x, v, omega, q, fh_prev, zeta=None, u=None, tol=1e-10):
-    """Compares one state against frame ts of a fixture; returns the worst
-    relative error and a dict of all."""
-    errs = {"x": rel(x, z["traj_x"][ts]), "v": rel(v, z["traj_v"][ts]), "omega": rel(omega, z["traj_omega"][ts]),
-            "q": rel(q, z["traj_q"][ts]), "f_hydro": rel(fh_prev, z["traj_f_hydro_previous"][ts])}
+def check_state(z, frame, cfg, x, v, omega, q, fh_prev, zeta=None, u=None, tol=1e-10, ts=None):
+    """Compares one state against trajectory frame `frame` of a fixture (step
+    ts, default ts = frame for fixtures that store every step); returns the
+    worst relative error and a dict of all."""
+    ts = frame if ts is None else ts
+    i = frame
+    errs = {"x": rel(x, z["traj_x"][i]), "v": rel(v, z["traj_v"][i]), "omega": rel(omega, z["traj_omega"][i]),
+            "q": rel(q, z["traj_q"][i]), "f_hydro": rel(fh_prev, z["traj_f_hydro_previous"][i])}
     if zeta is not None and f"zeta_retained_{ts}" in z.files:
         errs["zeta"] = rel(retained(cfg, zeta), z[f"zeta_retained_{ts}"])
     if u is not None and f"u_plane_{ts}" in z.files:
