@@ -61,45 +61,70 @@ def config_block():
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML on a thread while
+    the timed region runs.  start() returns once the first sample is taken
+    and stop() takes a last one, so even a short timed region is covered."""
+
     def __init__(self):
         self.samples = []
         self._stop = threading.Event()
+        self._ready = threading.Event()
         self._t = None
+        self._h = None
+        self._nvml = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            idx = int(os.environ.get("LOCAL_RANK", "0"))
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(idx if vis is None else 0 if "," not in vis else idx)
+            self._smax = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self._nvml = pynvml
+        except Exception as e:  # no NVML: report that
+            self.error = str(e)
+
+    def _sample(self):
+        n = self._nvml
+        sm = n.nvmlDeviceGetClockInfo(self._h, n.NVML_CLOCK_SM)
+        reasons = n.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+        self.samples.append((sm, self._smax, reasons))
 
     def start(self):
+        if self._nvml is None:
+            return
+
         def run():
             try:
-                import pynvml
-                pynvml.nvmlInit()
-                idx = int(os.environ.get("LOCAL_RANK", "0"))
-                vis = os.environ.get("CUDA_VISIBLE_DEVICES")
-                h = pynvml.nvmlDeviceGetHandleByIndex(idx if vis is None else 0 if "," not in vis else idx)
-                smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+                self._sample()
+                self._ready.set()
                 while not self._stop.is_set():
-                    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
-                    reasons = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
-                    self.samples.append((sm, smax, reasons))
-                    time.sleep(0.05)
-            except Exception as e:  # no NVML: report that
-                self.samples.append(("error", str(e), 0))
+                    time.sleep(0.02)
+                    self._sample()
+            except Exception:
+                self._ready.set()
         self._t = threading.Thread(target=run, daemon=True)
         self._t.start()
+        self._ready.wait(timeout=5)
 
     def stop(self):
         self._stop.set()
         if self._t:
             self._t.join(timeout=2)
-        good = [s for s in self.samples if s[0] != "error"]
-        if not good:
+        if self._nvml is not None:
+            try:
+                self._sample()
+            except Exception:
+                pass
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
         names = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
                  0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
                  0x100: "display_clock_setting"}
         mask = 0
-        for s in good:
+        for s in self.samples:
             mask |= int(s[2])
-        return {"sm_mhz": float(np.median([s[0] for s in good])), "sm_max_mhz": float(good[0][1]),
-                "reasons": [v for k, v in names.items() if mask & k], "samples": len(good)}
+        return {"sm_mhz": float(np.median([s[0] for s in self.samples])), "sm_max_mhz": float(self.samples[0][1]),
+                "reasons": [v for k, v in names.items() if mask & k], "samples": len(self.samples)}
 
 
 # --------------------------------------------------------------- reference
@@ -181,7 +206,7 @@ def run_reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -61,6 +61,16 @@ constexpr int kPWords = 12 * 3 + 2 * 4 + 4 * 3 + 1;
 
 // Field slots of the context arena (consecutive, fstride complex apart).
 enum Slot { Z0 = 0, Z1, U0, U1, U2, A0, A1, UP0, UP1, UP2, PHIS, NSLOT };
+// FP32-mixed Navier_Stokes runs keep zeta as an unevaluated sum hi + lo of two
+// FP32 fields: Z0/Z1 hold hi (the value every transform reads) and ZL0/ZL1
+// the compensation term of the Kahan-style (TwoSum) updates.
+constexpr int ZL0 = NSLOT, ZL1 = NSLOT + 1;
+
+// Field slots a run needs.
+int slots_for(const spm_params &p) {
+    if (p.equation == SPM_EQ_LEES_EDWARDS) return NSLOT + LE_EXTRA_SLOTS;
+    return p.precision == SPM_PREC_FP32_MIXED ? NSLOT + 2 : NSLOT;
+}
 
 struct spm_pool;
 
@@ -100,8 +110,16 @@ struct spm_ctx {
     std::vector<cudaEvent_t> prof_ev;
     double                   prof_bytes = 0.0;
     bool                     use_tma    = true;  // SPM_NO_TMA=1 selects the direct-load passes
+    bool                     zeta_dirty = false;  // zeta set by the host since the last NS step
+    int                      nslots     = NSLOT;  // field slots of this run (slots_for)
 
     bool fp64() const { return P.precision == SPM_PREC_FP64; }
+    // zeta kept as a compensated FP32 pair (FP32-mixed Navier_Stokes)
+    bool compensated() const { return !fp64() && P.equation == SPM_EQ_NAVIER_STOKES; }
+    template <typename T>
+    cplx<T> *zl(int d) const {
+        return compensated() ? cx<T>(ZL0 + d) : nullptr;
+    }
     template <typename T>
     T *real(int slot) const {
         return reinterpret_cast<T *>(static_cast<char *>(arena) + (size_t)slot * slot_stride_c * 2 * sizeof(T));
@@ -120,6 +138,12 @@ struct spm_ctx {
         return (int)std::min<size_t>(need, (size_t)cap);
     }
     dim3 pw_grid() const { return dim3(pw_blocks(), fft_runs); }
+    // the same for kernels that visit the retained 2/3 box only
+    dim3 box_grid() const {
+        const size_t need = (g.box_elems() + 255) / 256;
+        const int    cap  = std::max(1, grid_blocks() / std::max(1, fft_runs));
+        return dim3((unsigned)std::min<size_t>(need, (size_t)cap), fft_runs);
+    }
 };
 
 #define LAUNCH(ctx, kern, grid, block, smem, ...)                                           \
@@ -271,13 +295,13 @@ FFTPlan<float> &plan_of<float>(spm_ctx *c) {
 // the same slots of all its runs (run-consecutive within a slot) into one
 // launch per slot.
 template <typename T, int DIR>
-cudaError_t strided_dispatch(spm_ctx *c, int slot, int nf, int axis) {
+cudaError_t strided_dispatch(spm_ctx *c, int slot, int nf, int axis, PassPrune pr) {
     auto one = [&](cplx<T> *base, int nfields, size_t stride) {
         if (c->use_tma) {
-            cudaError_t e = plan_of<T>(c).template strided_tma<DIR>(base, nfields, stride, axis, c->st);
+            cudaError_t e = plan_of<T>(c).template strided_tma<DIR>(base, nfields, stride, axis, c->st, pr);
             if (e != cudaErrorNotSupported) return e;
         }
-        return plan_of<T>(c).template strided<DIR>(base, nfields, stride, axis, c->st);
+        return plan_of<T>(c).template strided<DIR>(base, nfields, stride, axis, c->st, pr);
     };
     if (c->fft_runs == 1) return one(c->cx<T>(slot), nf, c->slot_stride_c);
     for (int k = 0; k < nf; k++) {
@@ -288,32 +312,61 @@ cudaError_t strided_dispatch(spm_ctx *c, int slot, int nf, int axis) {
     return cudaSuccess;
 }
 
-// Strided (Y/X) FFT pass, bracketed by CUDA events when profiling is on.
+// Pruning of the step's strided passes to the retained 2/3 box (PassPrune):
+// inverse passes read modes outside it as zero, forward passes only produce
+// the column tiles (and on the X pass the ky lines) the box needs.
+PassPrune prune_inverse(const Grid &g, int axis) {
+    return axis == 0 ? PassPrune{g.trn[2], g.trn[1], g.trn[0], g.trn[2]}
+                     : PassPrune{g.trn[2], 0, g.trn[1], g.trn[2]};
+}
+PassPrune prune_forward(const Grid &g, int axis) {
+    return axis == 0 ? PassPrune{g.trn[2], g.trn[1], 0, g.hnz} : PassPrune{g.trn[2], 0, 0, g.hnz};
+}
+
+// Complex elements a strided pass transforms (lines x columns x fields).
+template <typename T>
+double pass_elems(spm_ctx *c, int nf, int axis, const PassPrune &pr) {
+    const Grid &g     = c->g;
+    const int   n     = axis == 1 ? g.ny : g.nx;
+    const int   outer = axis == 1 ? g.nx : g.ny;
+    const int   wk    = (c->use_tma && n <= 256) ? FFTPlan<T>::W_T : FFTPlan<T>::W;
+    const int   cols  = std::min(g.hnz, (std::min(pr.kz_cols, g.hnz) + wk - 1) / wk * wk);
+    return (double)nf * c->fft_runs * outer_count(outer, pr.outer_trn) * (double)n * cols;
+}
+
+// Strided (Y/X) FFT pass, bracketed by CUDA events when profiling is on (the
+// algorithmic bytes of a pass: one read and one write of every element it
+// transforms).
 template <typename T, int DIR>
-int fft_strided_pass(spm_ctx *c, int slot, int nf, int axis) {
+int fft_strided_pass(spm_ctx *c, int slot, int nf, int axis, PassPrune pr) {
     if (c->prof_on) {
         cudaEvent_t a, b;
         SPM_CUDA_CHECK(cudaEventCreate(&a));
         SPM_CUDA_CHECK(cudaEventCreate(&b));
         SPM_CUDA_CHECK(cudaEventRecord(a, c->st));
-        SPM_CUDA_CHECK((strided_dispatch<T, DIR>(c, slot, nf, axis)));
+        SPM_CUDA_CHECK((strided_dispatch<T, DIR>(c, slot, nf, axis, pr)));
         SPM_CUDA_CHECK(cudaEventRecord(b, c->st));
         c->prof_ev.push_back(a);
         c->prof_ev.push_back(b);
-        c->prof_bytes += 2.0 * nf * c->fft_runs * (double)c->g.nx * c->g.ny * c->g.hnz * sizeof(cplx<T>);
+        c->prof_bytes += 2.0 * pass_elems<T>(c, nf, axis, pr) * sizeof(cplx<T>);
     } else {
-        SPM_CUDA_CHECK((strided_dispatch<T, DIR>(c, slot, nf, axis)));
+        SPM_CUDA_CHECK((strided_dispatch<T, DIR>(c, slot, nf, axis, pr)));
     }
     c->launches++;
     return SPM_OK;
 }
+template <typename T, int DIR>
+int fft_strided_pass(spm_ctx *c, int slot, int nf, int axis) {
+    return fft_strided_pass<T, DIR>(c, slot, nf, axis, PassPrune::full(c->g.hnz));
+}
 // z passes over `nf` slots (one launch per slot when batching runs)
 template <typename T>
-int z_pass(spm_ctx *c, int slot, int nf, bool forward) {
+int z_pass(spm_ctx *c, int slot, int nf, bool forward, int kz_keep = 1 << 30) {
     const T scale = (T)(1.0 / ((double)c->g.nx * c->g.ny * c->g.nz));
     auto    one   = [&](int s, int nfields, size_t stride) {
         return forward ? plan_of<T>(c).z_r2c(c->real<T>(s), c->cx<T>(s), nfields, 2 * stride, stride, c->st)
-                       : plan_of<T>(c).z_c2r(c->cx<T>(s), c->real<T>(s), nfields, stride, 2 * stride, scale, c->st);
+                       : plan_of<T>(c).z_c2r(c->cx<T>(s), c->real<T>(s), nfields, stride, 2 * stride, scale, c->st,
+                                             kz_keep);
     };
     if (c->fft_runs == 1) {
         SPM_CUDA_CHECK(one(slot, nf, c->slot_stride_c));
@@ -351,11 +404,21 @@ __global__ void k_zero3(double *uk_dc) {
 // run, FFT stages to L, which is either the run itself or a pool lead whose
 // FFT launches cover the same slots of every run of the pool.
 // ---------------------------------------------------------------------------
+// u (real space) from zeta.  truncate = 1 is the step's Zeta_k2u (2/3 rule
+// applied, pruned passes); truncate = 0 keeps every mode (state getters).
 template <typename T>
 int zeta_to_velocity(spm_ctx *L, int truncate) {
-    LAUNCH(L, k_zeta_to_u<T>, L->pw_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
-           L->cx<T>(U1), L->cx<T>(U2), truncate, L->fstride_c);
-    return fft_inv<T>(L, U0, 3);
+    if (!truncate) {
+        LAUNCH(L, k_zeta_to_u<T>, L->pw_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
+               L->cx<T>(U1), L->cx<T>(U2), 0, L->fstride_c, 0);
+        return fft_inv<T>(L, U0, 3);
+    }
+    int rc;
+    LAUNCH(L, k_zeta_to_u<T>, L->box_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
+           L->cx<T>(U1), L->cx<T>(U2), 1, L->fstride_c, 1);
+    if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 0, prune_inverse(L->g, 0))) != SPM_OK) return rc;
+    if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 1, prune_inverse(L->g, 1))) != SPM_OK) return rc;
+    return z_pass<T>(L, U0, 3, false, L->g.trn[2]);
 }
 
 // NS_solver_slavedEuler (fluid_solver.cxx:348-374).
@@ -363,17 +426,18 @@ template <typename T>
 int ns_solver(spm_ctx *L) {
     int rc;
     // zeta -> u_hat (truncated) -> inverse x, y passes
-    LAUNCH(L, k_zeta_to_u<T>, L->pw_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
-           L->cx<T>(U1), L->cx<T>(U2), 1, L->fstride_c);
-    if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 0)) != SPM_OK) return rc;
-    if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 1)) != SPM_OK) return rc;
+    LAUNCH(L, k_zeta_to_u<T>, L->box_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
+           L->cx<T>(U1), L->cx<T>(U2), 1, L->fstride_c, 1);
+    if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 0, prune_inverse(L->g, 0))) != SPM_OK) return rc;
+    if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 1, prune_inverse(L->g, 1))) != SPM_OK) return rc;
     // inverse z + products + forward z in one pass, then forward y, x passes
-    SPM_CUDA_CHECK(plan_of<T>(L).z_products(L->cx<T>(U0), L->slot_stride_c, L->fft_runs, L->fstride_c, L->st));
+    SPM_CUDA_CHECK(plan_of<T>(L).z_products(L->cx<T>(U0), L->slot_stride_c, L->fft_runs, L->fstride_c, L->st,
+                                            L->g.trn[2], L->g.kz_span()));
     L->launches++;
-    if ((rc = fft_strided_pass<T, -1>(L, U0, 5, 1)) != SPM_OK) return rc;
-    if ((rc = fft_strided_pass<T, -1>(L, U0, 5, 0)) != SPM_OK) return rc;
-    LAUNCH(L, k_ns_update<T>, L->pw_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->cx<T>(U0), L->cx<T>(U1),
-           L->cx<T>(U2), L->cx<T>(A0), L->cx<T>(A1), L->ph.nu, L->ph.dt, L->fstride_c);
+    if ((rc = fft_strided_pass<T, -1>(L, U0, 5, 1, prune_forward(L->g, 1))) != SPM_OK) return rc;
+    if ((rc = fft_strided_pass<T, -1>(L, U0, 5, 0, prune_forward(L->g, 0))) != SPM_OK) return rc;
+    LAUNCH(L, k_ns_update<T>, L->box_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->cx<T>(U0), L->cx<T>(U1),
+           L->cx<T>(U2), L->cx<T>(A0), L->cx<T>(A1), L->ph.nu, L->ph.dt, L->fstride_c, 1, L->zl<T>(0), L->zl<T>(1));
     return SPM_OK;
 }
 
@@ -416,16 +480,28 @@ template <typename T>
 int rigidity_projection(spm_ctx *L) {
     int rc;
     SPM_CUDA_CHECK(plan_of<T>(L).z_makef(L->real<T>(UP0), L->real<T>(U0), L->real<T>(PHIS), L->slot_stride_c,
-                                         L->fft_runs, L->fstride_c, L->st));
+                                         L->fft_runs, L->fstride_c, L->st, L->g.kz_span()));
     L->launches++;
-    if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 1)) != SPM_OK) return rc;
-    if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 0)) != SPM_OK) return rc;
-    LAUNCH(L, k_project_add_curl<T>, L->pw_grid(), 256, 0, L->g, L->cx<T>(UP0), L->cx<T>(UP1), L->cx<T>(UP2),
-           L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->fstride_c);
+    if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 1, prune_forward(L->g, 1))) != SPM_OK) return rc;
+    if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 0, prune_forward(L->g, 0))) != SPM_OK) return rc;
+    LAUNCH(L, k_project_add_curl<T>, L->box_grid(), 256, 0, L->g, L->cx<T>(UP0), L->cx<T>(UP1), L->cx<T>(UP2),
+           L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->fstride_c, 1, L->zl<T>(0), L->zl<T>(1));
     return SPM_OK;
 }
 
 int particle_blocks(spm_ctx *c) { return (c->ph.np + 127) / 128; }
+
+// Zeta uploaded by the host: truncate it once (the reference truncates zeta in
+// place at the start of NS_solver_slavedEuler; the step's retained-box
+// kernels leave the other modes as they are).
+template <typename T>
+int truncate_if_dirty(spm_ctx *c) {
+    if (!c->zeta_dirty) return SPM_OK;
+    LAUNCH(c, k_truncate2<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(Z0), c->cx<T>(Z1));
+    if (c->compensated()) LAUNCH(c, k_truncate2<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(ZL0), c->cx<T>(ZL1));
+    c->zeta_dirty = false;
+    return SPM_OK;
+}
 
 // Time_evolution_hydro (sp_3d_ns.cxx:41-194), Navier_Stokes with free
 // spheres.  L batches the grid stages of runs R[0..nr), which are L's runs in
@@ -434,6 +510,8 @@ int particle_blocks(spm_ctx *c) { return (c->ph.np + 127) / 128; }
 template <typename T>
 int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
     int rc;
+    for (int r = 0; r < nr; r++)
+        if ((rc = truncate_if_dirty<T>(R[r])) != SPM_OK) return rc;
     if ((rc = ns_solver<T>(L)) != SPM_OK) return rc;
     LAUNCH(L, k_fix_cell, (nr + 127) / 128, 128, 0, L->rw, nr);
     if ((rc = zeta_to_velocity<T>(L, 1)) != SPM_OK) return rc;
@@ -467,7 +545,7 @@ int step_ns(spm_ctx *c) {
 template <typename T>
 int initialize_impl(spm_ctx *c) {
     int rc;
-    for (int sl = 0; sl < NSLOT; sl++) SPM_CUDA_CHECK(cudaMemsetAsync(c->real<T>(sl), 0, c->field_bytes(), c->st));
+    for (int sl = 0; sl < c->nslots; sl++) SPM_CUDA_CHECK(cudaMemsetAsync(c->real<T>(sl), 0, c->field_bytes(), c->st));
     SPM_CUDA_CHECK(cudaMemsetAsync(c->ts_dev, 0, sizeof(int), c->st));
     LAUNCH(c, k_zero3, 1, 32, 0, c->uk_dc);
     if ((rc = phi_sum_scatter<T>(c)) != SPM_OK) return rc;
@@ -522,6 +600,39 @@ int download_field(spm_ctx *c, int slot, double *h) {
     const size_t rows = (size_t)c->g.nx * c->g.ny;
     for (size_t r = 0; r < rows; r++)
         for (int k = 0; k < 2 * c->g.hnz; k++) h[r * 2 * c->g.hnz + k] = (double)tmp[r * 2 * c->g.hnzp + k];
+    return SPM_OK;
+}
+
+// Compensated zeta of an FP32-mixed run: upload x as hi = (float)x and
+// lo = (float)(x - hi); download hi + lo.
+int upload_field_split(spm_ctx *c, int slot_hi, int slot_lo, const double *h) {
+    std::vector<float> hi(c->fstride_c * 2, 0.0f), lo(c->fstride_c * 2, 0.0f);
+    const size_t rows = (size_t)c->g.nx * c->g.ny;
+    for (size_t r = 0; r < rows; r++)
+        for (int k = 0; k < 2 * c->g.hnz; k++) {
+            const double x = h[r * 2 * c->g.hnz + k];
+            const float  a = (float)x;
+            hi[r * 2 * c->g.hnzp + k] = a;
+            lo[r * 2 * c->g.hnzp + k] = (float)(x - (double)a);
+        }
+    SPM_CUDA_CHECK(cudaMemcpyAsync(c->real<float>(slot_hi), hi.data(), hi.size() * sizeof(float),
+                                   cudaMemcpyHostToDevice, c->st));
+    SPM_CUDA_CHECK(cudaMemcpyAsync(c->real<float>(slot_lo), lo.data(), lo.size() * sizeof(float),
+                                   cudaMemcpyHostToDevice, c->st));
+    SPM_CUDA_CHECK(cudaStreamSynchronize(c->st));
+    return SPM_OK;
+}
+int download_field_sum(spm_ctx *c, int slot_hi, int slot_lo, double *h) {
+    std::vector<float> hi(c->fstride_c * 2), lo(c->fstride_c * 2);
+    SPM_CUDA_CHECK(cudaMemcpyAsync(hi.data(), c->real<float>(slot_hi), hi.size() * sizeof(float),
+                                   cudaMemcpyDeviceToHost, c->st));
+    SPM_CUDA_CHECK(cudaMemcpyAsync(lo.data(), c->real<float>(slot_lo), lo.size() * sizeof(float),
+                                   cudaMemcpyDeviceToHost, c->st));
+    SPM_CUDA_CHECK(cudaStreamSynchronize(c->st));
+    const size_t rows = (size_t)c->g.nx * c->g.ny;
+    for (size_t r = 0; r < rows; r++)
+        for (int k = 0; k < 2 * c->g.hnz; k++)
+            h[r * 2 * c->g.hnz + k] = (double)hi[r * 2 * c->g.hnzp + k] + (double)lo[r * 2 * c->g.hnzp + k];
     return SPM_OK;
 }
 
@@ -630,7 +741,8 @@ int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *
         c->own_stream = true;
     }
     c->fstride_c    = (size_t)c->g.nx * c->g.ny * c->g.hnzp;
-    const int nslot = (p.equation == SPM_EQ_LEES_EDWARDS) ? NSLOT + LE_EXTRA_SLOTS : NSLOT;
+    const int nslot = slots_for(p);
+    c->nslots       = nslot;
     {
         const char *nt = getenv("SPM_NO_TMA");
         c->use_tma     = !(nt && nt[0] == '1');
@@ -785,7 +897,7 @@ int spm_device_bytes(const spm_params *p, size_t *bytes) {
     if (rc != SPM_OK) return rc;
     const size_t es  = p->precision == SPM_PREC_FP64 ? 8 : 4;
     const size_t fld = (size_t)g.nx * g.ny * g.hnzp * 2 * es;
-    const size_t nslot = (p->equation == SPM_EQ_LEES_EDWARDS) ? (size_t)NSLOT + LE_EXTRA_SLOTS : (size_t)NSLOT;
+    const size_t nslot = (size_t)slots_for(*p);
     *bytes = nslot * fld + (size_t)std::max(p->n_particles, 1) * kPWords * 8 + 64 * 1024;
     return SPM_OK;
 }
@@ -844,8 +956,13 @@ int spm_get_zeta(spm_ctx *c, double *z0, double *z1, double uk_dc[3]) {
     if (!c || !z0 || !z1 || !uk_dc) return fail(SPM_ERR_ARG, "bad argument");
     int rc;
     if ((rc = spm_synchronize(c)) != SPM_OK) return rc;
-    if ((rc = download_field(c, Z0, z0)) != SPM_OK) return rc;
-    if ((rc = download_field(c, Z1, z1)) != SPM_OK) return rc;
+    if (c->compensated()) {
+        if ((rc = download_field_sum(c, Z0, ZL0, z0)) != SPM_OK) return rc;
+        if ((rc = download_field_sum(c, Z1, ZL1, z1)) != SPM_OK) return rc;
+    } else {
+        if ((rc = download_field(c, Z0, z0)) != SPM_OK) return rc;
+        if ((rc = download_field(c, Z1, z1)) != SPM_OK) return rc;
+    }
     SPM_CUDA_CHECK(cudaMemcpy(uk_dc, c->uk_dc, 3 * sizeof(double), cudaMemcpyDeviceToHost));
     return SPM_OK;
 }
@@ -853,8 +970,14 @@ int spm_get_zeta(spm_ctx *c, double *z0, double *z1, double uk_dc[3]) {
 int spm_set_zeta(spm_ctx *c, const double *z0, const double *z1, const double uk_dc[3]) {
     if (!c || !z0 || !z1 || !uk_dc) return fail(SPM_ERR_ARG, "bad argument");
     int rc;
-    if ((rc = upload_field(c, Z0, z0)) != SPM_OK) return rc;
-    if ((rc = upload_field(c, Z1, z1)) != SPM_OK) return rc;
+    if (c->compensated()) {
+        if ((rc = upload_field_split(c, Z0, ZL0, z0)) != SPM_OK) return rc;
+        if ((rc = upload_field_split(c, Z1, ZL1, z1)) != SPM_OK) return rc;
+    } else {
+        if ((rc = upload_field(c, Z0, z0)) != SPM_OK) return rc;
+        if ((rc = upload_field(c, Z1, z1)) != SPM_OK) return rc;
+    }
+    c->zeta_dirty = !c->le.enabled;
     SPM_CUDA_CHECK(cudaMemcpyAsync(c->uk_dc, uk_dc, 3 * sizeof(double), cudaMemcpyHostToDevice, c->st));
     SPM_CUDA_CHECK(cudaStreamSynchronize(c->st));
     return SPM_OK;

@@ -56,6 +56,30 @@ struct Grid {
     double wave[3];
     double dx;
     __host__ __device__ size_t field_elems_c() const { return (size_t)nx * ny * hnzp; }  // complex elements
+
+    // The retained 2/3 box |KX| < TRN_X, |KY| < TRN_Y, KZ < TRN_Z: the only
+    // modes the step's k-space updates read or write.  box_index maps a
+    // dense box index (kz fastest) to the field's complex element index.
+    __host__ __device__ size_t box_elems() const {
+        return (size_t)(2 * trn[0] - 1) * (size_t)(2 * trn[1] - 1) * (size_t)trn[2];
+    }
+    __host__ __device__ size_t box_index(size_t b) const {
+        const int    kz = (int)(b % (size_t)trn[2]);
+        const size_t r  = b / (size_t)trn[2];
+        const int    ny_box = 2 * trn[1] - 1;
+        const int    iy = (int)(r % (size_t)ny_box);
+        const int    ix = (int)(r / (size_t)ny_box);
+        const int    i  = ix < trn[0] ? ix : ix + nx - (2 * trn[0] - 1);
+        const int    j  = iy < trn[1] ? iy : iy + ny - ny_box;
+        return ((size_t)i * ny + j) * hnzp + kz;
+    }
+    // Complex values per z row that a pruned forward z pass must produce so
+    // that every strided column tile covering KZ < TRN_Z reads written data
+    // (tiles are 8, 16 or 32 columns wide).
+    __host__ __device__ int kz_span() const {
+        const int r = (trn[2] + 31) / 32 * 32;
+        return r < hnz ? r : hnz;
+    }
 };
 
 // Device-side error word: kernels that detect a violated precondition (a

@@ -27,14 +27,42 @@
 namespace spm {
 
 // ---------------------------------------------------------------------------
+// Pruning of a strided pass to the 2/3-retained modes.  The step's k-space
+// updates only read and write |KX| < TRN_X, |KY| < TRN_Y, KZ < TRN_Z, so
+//   * a pass only visits column tiles that cover kz < kz_cols,
+//   * the X pass only visits outer lines (ky) with |KY| < outer_trn,
+//   * an inverse pass reads input lines with |K| >= line_trn and columns
+//     kz >= col_keep as zero (those modes are never written upstream).
+// Every retained output is computed by exactly the same arithmetic as in the
+// full pass.  PassPrune::full(hnz) is the unpruned pass.
+// ---------------------------------------------------------------------------
+struct PassPrune {
+    int kz_cols;    // columns [0, kz_cols) are needed
+    int outer_trn;  // > 0: only outer lines o with |K(o)| < outer_trn
+    int line_trn;   // > 0: input lines with |K(n)| >= line_trn read as zero
+    int col_keep;   // input columns kz >= col_keep read as zero
+    static PassPrune full(int hnz) { return PassPrune{hnz, 0, 0, hnz}; }
+};
+
+__host__ __device__ __forceinline__ int signed_mode(int n, int len) { return n > len / 2 ? n - len : n; }
+__host__ __device__ __forceinline__ int outer_count(int n_outer, int outer_trn) {
+    return outer_trn > 0 ? 2 * outer_trn - 1 : n_outer;
+}
+// index oi of the visited outer lines -> outer line o
+__host__ __device__ __forceinline__ int outer_line(int oi, int n_outer, int outer_trn) {
+    return (outer_trn > 0 && oi >= outer_trn) ? oi + n_outer - (2 * outer_trn - 1) : oi;
+}
+
+// ---------------------------------------------------------------------------
 // Strided complex pass (Y or X axis).
-// Element n of column c of tile b lives at
-//   base + (b / col_tiles) * outer_stride + (b % col_tiles) * W + c + n * axis_stride
+// Block b visits column tile ct = b % ct_used of outer line
+// o = outer_line(b / ct_used); element n of column c lives at
+//   base + o * outer_stride + ct * W + c + n * axis_stride
 // ---------------------------------------------------------------------------
 template <typename T, int N, int W, int DIR>
 __global__ void __launch_bounds__(W *Split<N>::N1)
-    fft_strided_kernel(cplx<T> *__restrict__ data, size_t field_stride, int ncols, int col_tiles,
-                       size_t outer_stride, size_t axis_stride, const cplx<T> *__restrict__ twN) {
+    fft_strided_kernel(cplx<T> *__restrict__ data, size_t field_stride, int ncols, int ct_used, int n_outer,
+                       size_t outer_stride, size_t axis_stride, const cplx<T> *__restrict__ twN, PassPrune pr) {
     constexpr int N1 = Split<N>::N1;
     constexpr int N2 = Split<N>::N2;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -43,16 +71,20 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
     const int c   = threadIdx.x % W;
     const int g   = threadIdx.x / W;  // n1 in step 1, k1 base in step 2
     const int b   = blockIdx.x;
-    const int col = (b % col_tiles) * W + c;
+    const int col = (b % ct_used) * W + c;
+    const int o   = outer_line(b / ct_used, n_outer, pr.outer_trn);
     const bool ok = col < ncols;
-    cplx<T> *base = data + (size_t)blockIdx.y * field_stride + (size_t)(b / col_tiles) * outer_stride + col;
+    const bool col_in = ok && col < pr.col_keep;
+    cplx<T> *base = data + (size_t)blockIdx.y * field_stride + (size_t)o * outer_stride + col;
 
     // Step 1: N2-point DFTs over n2 for fixed n1 = g, input index n1 + N1*n2.
     cplx<T> v[N2];
 #pragma unroll
     for (int m = 0; m < N2; m++) {
-        if (ok) {
-            v[m] = base[(size_t)(g + N1 * m) * axis_stride];
+        const int n = g + N1 * m;
+        const bool in = col_in && (pr.line_trn == 0 || abs(signed_mode(n, N)) < pr.line_trn);
+        if (in) {
+            v[m] = base[(size_t)n * axis_stride];
         } else {
             v[m] = cplx<T>{0, 0};
         }
@@ -95,8 +127,8 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
 // ---------------------------------------------------------------------------
 template <typename T, int N, int W, int DIR, int S>
 __global__ void __launch_bounds__(W *Split<N>::N1)
-    fft_strided_tma_kernel(const __grid_constant__ CUtensorMap map, int axis, int n_outer, int col_tiles,
-                           int ntiles, const cplx<T> *__restrict__ twN, unsigned int *err) {
+    fft_strided_tma_kernel(const __grid_constant__ CUtensorMap map, int axis, int n_outer, int ct_used,
+                           int ntiles, const cplx<T> *__restrict__ twN, unsigned int *err, PassPrune pr) {
     constexpr int      N1         = Split<N>::N1;
     constexpr int      N2         = Split<N>::N2;
     constexpr unsigned tile_bytes = N * W * sizeof(cplx<T>);
@@ -107,9 +139,10 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
     const int tid = threadIdx.x;
     const int c   = tid % W;
     const int g   = tid / W;
+    const int n_used = outer_count(n_outer, pr.outer_trn);
     auto coords = [&](int t, int &c0, int &c1, int &c2, int &c3) {
-        const int ct = t % col_tiles, rest = t / col_tiles;
-        const int o = rest % n_outer, f = rest / n_outer;
+        const int ct = t % ct_used, rest = t / ct_used;
+        const int o = outer_line(rest % n_used, n_outer, pr.outer_trn), f = rest / n_used;
         c0 = 2 * ct * W;
         c3 = f;
         if (axis == 1) {
@@ -142,10 +175,16 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
         cplx<T>  *B  = buf + (size_t)b * N * W;
         const bool w = mbar_wait(&full[b], (unsigned)((it / S) & 1), err);
         if (!__syncthreads_and(w)) break;
-        // step 1: N2-point DFTs over n2 for n1 = g, in place
+        // step 1: N2-point DFTs over n2 for n1 = g, in place (pruned inputs
+        // read as zero)
+        const bool col_in = (t % ct_used) * W + c < pr.col_keep;
         cplx<T> v[N2];
 #pragma unroll
-        for (int m = 0; m < N2; m++) v[m] = B[(g + N1 * m) * W + c];
+        for (int m = 0; m < N2; m++) {
+            const int n = g + N1 * m;
+            v[m] = (col_in && (pr.line_trn == 0 || abs(signed_mode(n, N)) < pr.line_trn)) ? B[n * W + c]
+                                                                                           : cplx<T>{0, 0};
+        }
         dft_reg<T, N2, DIR>(v);
 #pragma unroll
         for (int k1 = 1; k1 < N2; k1++) {
@@ -259,10 +298,23 @@ __device__ __forceinline__ void c2r_row(int t, Ld ld, cplx<T> *s, const cplx<T> 
     constexpr int M1 = Split<M>::N1;
     constexpr int M2 = Split<M>::N2;
     constexpr int P  = M1;
-    for (int k = t; k <= M; k += P) {
-        cplx<T> x = ld(k);
-        if (k == 0 || k == M) x.im = 0;
-        s[k] = x;
+    // all loads of the row first (independent, in flight together), then
+    // the stores to the workspace
+    constexpr int KL = M / P + 1;
+    cplx<T>       xl[KL];
+#pragma unroll
+    for (int i = 0; i < KL; i++) {
+        const int k = t + P * i;
+        xl[i]       = k <= M ? ld(k) : cplx<T>{0, 0};
+    }
+#pragma unroll
+    for (int i = 0; i < KL; i++) {
+        const int k = t + P * i;
+        if (k <= M) {
+            cplx<T> x = xl[i];
+            if (k == 0 || k == M) x.im = 0;
+            s[k] = x;
+        }
     }
     __syncthreads();
     // Z'[k] = E' + i O',  E' = c (X[k] + conj X[M-k]),
@@ -356,11 +408,13 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
 
 // ---------------------------------------------------------------------------
 // Z pass, inverse: complex rows -> real rows, output scaled by `scale`.
+// Inputs kz >= kz_keep are read as zero (pruned transforms; hnz: none).
 // ---------------------------------------------------------------------------
 template <typename T, int M, int R>
 __global__ void __launch_bounds__(R *Split<M>::N1)
     fft_z_c2r_kernel(const cplx<T> *in, T *out, size_t field_stride_c, size_t field_stride_real, int nrows,
-                     int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale) {
+                     int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale,
+                     int kz_keep) {
     constexpr int P = Split<M>::N1;
     __shared__ __align__(16) cplx<T> s[R][M + 1];
     const int r   = threadIdx.x / P;
@@ -370,7 +424,7 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
     const cplx<T> *rin = in + (size_t)blockIdx.y * field_stride_c + (size_t)(ok ? row : 0) * hnzp;
     T *rout            = out + (size_t)blockIdx.y * field_stride_real + (size_t)(ok ? row : 0) * 2 * hnzp;
     c2r_row<T, M>(
-        t, [&](int k) { return ok ? rin[k] : cplx<T>{0, 0}; }, s[r], twM, twN, scale,
+        t, [&](int k) { return (ok && k < kz_keep) ? rin[k] : cplx<T>{0, 0}; }, s[r], twM, twN, scale,
         [&](int n, cplx<T> z) {
             if (ok) store_pair<T>(rout, n, z);
         });
@@ -384,28 +438,50 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
 // products in registers/shared memory, forward z transform of the products.
 // io[0..2] hold u_hat (z-complex rows) on input; io[0..4] receive the
 // z-transformed products u2u3, u3u1, u1u2, (u2-u3)(u2+u3), (u3-u1)(u3+u1).
+// Inputs kz >= kz_keep are read as zero; outputs are written for kz <
+// kz_span only (the pruned passes downstream read no further).
 // ---------------------------------------------------------------------------
 template <typename T, int M, int R>
 __global__ void __launch_bounds__(R *Split<M>::N1)
     fft_z_products_kernel(cplx<T> *io, size_t field_stride_c, size_t run_stride_c, int nrows, int hnzp,
-                          const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale) {
-    constexpr int P = Split<M>::N1;
+                          const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale, int kz_keep,
+                          int kz_span) {
+    constexpr int P     = Split<M>::N1;
+    constexpr int PITCH = 2 * (M + 2);  // reals per staged row (>= 2 * hnzp)
     io += (size_t)blockIdx.y * run_stride_c;  // run of a batched pool
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    T       *U  = reinterpret_cast<T *>(smem_raw);                   // [3][R][2M]
-    cplx<T> *ws = reinterpret_cast<cplx<T> *>(U + 3 * R * 2 * M);     // [R][M+1]
+    T       *U  = reinterpret_cast<T *>(smem_raw);                 // [3][R][PITCH]
+    cplx<T> *ws = reinterpret_cast<cplx<T> *>(U + 3 * R * PITCH);   // [R][M+1]
     const int r   = threadIdx.x / P;
     const int t   = threadIdx.x % P;
     const int row = blockIdx.x * R + r;
     const bool ok = row < nrows;
     const size_t roff = (size_t)(ok ? row : 0) * hnzp;
-    T *Ur[3] = {U + (0 * R + r) * 2 * M, U + (1 * R + r) * 2 * M, U + (2 * R + r) * 2 * M};
+    T *Ur[3] = {U + (0 * R + r) * PITCH, U + (1 * R + r) * PITCH, U + (2 * R + r) * PITCH};
+    // Stage the CTA's rows of the three velocity fields (kz < kz_keep only)
+    // with 16-byte asynchronous copies, all in flight together; each complex
+    // row is then transformed in place into its real row.
+    {
+        const int keep   = kz_keep < M + 1 ? kz_keep : M + 1;
+        const int nchunk = (int)((keep * sizeof(cplx<T>) + 15) / 16);
+        for (int q = threadIdx.x; q < 3 * R * nchunk; q += blockDim.x) {
+            const int ch = q % nchunk, rr = (q / nchunk) % R, d = q / (nchunk * R);
+            const int grow = blockIdx.x * R + rr;
+            if (grow < nrows)
+                cp_async16(reinterpret_cast<char *>(U + (d * R + rr) * PITCH) + 16 * ch,
+                           reinterpret_cast<const char *>(io + d * field_stride_c + (size_t)grow * hnzp) + 16 * ch);
+        }
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+    }
 #pragma unroll 1
     for (int d = 0; d < 3; d++) {
-        const cplx<T> *rin = io + d * field_stride_c + roff;
+        const cplx<T> *rin = reinterpret_cast<const cplx<T> *>(Ur[d]);
         T             *ur  = Ur[d];
         c2r_row<T, M>(
-            t, [&](int k) { return ok ? rin[k] : cplx<T>{0, 0}; }, ws + r * (M + 1), twM, twN, scale,
+            t, [&](int k) { return (ok && k < kz_keep) ? rin[k] : cplx<T>{0, 0}; }, ws + r * (M + 1), twM, twN,
+            scale,
             [&](int n, cplx<T> z) {
                 ur[2 * n]     = z.re;
                 ur[2 * n + 1] = z.im;
@@ -428,9 +504,9 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
             },
             ws + r * (M + 1), twM, twN,
             [&](int k, cplx<T> X) {
-                if (ok) rout[k] = X;
+                if (ok && k < kz_span) rout[k] = X;
             });
-        if (ok)
+        if (ok && kz_span > M)
             for (int k = M + 1 + t; k < hnzp; k += P) rout[k] = cplx<T>{0, 0};
     }
 }
@@ -438,13 +514,14 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
 // ---------------------------------------------------------------------------
 // Fused Z pass of the rigidity force (Make_f_particle_dt_nonsole,
 // f_particle.h:35-54): f = up - min(phi_sum, 1) u formed on the fly and
-// transformed forward.  up[0..2] (real rows) are overwritten by f_hat rows.
+// transformed forward.  up[0..2] (real rows) are overwritten by f_hat rows
+// for kz < kz_span.
 // ---------------------------------------------------------------------------
 template <typename T, int M, int R>
 __global__ void __launch_bounds__(R *Split<M>::N1)
     fft_z_makef_kernel(T *up, const T *__restrict__ u, const T *__restrict__ phi_sum, size_t field_stride_c,
                        size_t run_stride_c, int nrows, int hnzp, const cplx<T> *__restrict__ twM,
-                       const cplx<T> *__restrict__ twN) {
+                       const cplx<T> *__restrict__ twN, int kz_span) {
     constexpr int P = Split<M>::N1;
     up += (size_t)blockIdx.y * 2 * run_stride_c;  // run of a batched pool
     u += (size_t)blockIdx.y * 2 * run_stride_c;
@@ -471,9 +548,9 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
             },
             s[r], twM, twN,
             [&](int k, cplx<T> X) {
-                if (ok) out[k] = X;
+                if (ok && k < kz_span) out[k] = X;
             });
-        if (ok)
+        if (ok && kz_span > M)
             for (int k = M + 1 + t; k < hnzp; k += P) out[k] = cplx<T>{0, 0};
     }
 }

@@ -24,19 +24,20 @@ struct FFTPlan {
         return (int)(32768 / (m * sizeof(cplx<T>))) >= 16 ? 16 : (int)(32768 / (m * sizeof(cplx<T>)));
     }
 
-    // rows per CTA of the fused products kernel (three real rows + workspace
-    // per row, kept within 64 KB of dynamic shared memory)
+    // rows per CTA of the fused products kernel (three staged rows + workspace
+    // per row, kept within about 66 KB of dynamic shared memory)
     static constexpr int prows(int m) {
         return (int)(65536 / (8 * m * sizeof(T))) >= 16 ? 16 : (int)(65536 / (8 * m * sizeof(T)));
     }
     static constexpr size_t psmem(int m) {
-        return (size_t)prows(m) * (3 * 2 * m * sizeof(T) + (m + 1) * sizeof(cplx<T>));
+        return (size_t)prows(m) * (3 * 2 * (m + 2) * sizeof(T) + (m + 1) * sizeof(cplx<T>));
     }
 
     static bool size_ok(int n) { return n >= 8 && n <= 512 && (n & (n - 1)) == 0; }
 
     // Fused inverse-z / advection products / forward-z pass over five slots.
-    cudaError_t z_products(cplx<T> *io, size_t fs_c, int nruns, size_t run_stride_c, cudaStream_t st) const {
+    cudaError_t z_products(cplx<T> *io, size_t fs_c, int nruns, size_t run_stride_c, cudaStream_t st, int kz_keep,
+                           int kz_span) const {
         const int nrows = g.nx * g.ny;
         const T   scale = (T)(1.0 / ((double)g.nx * g.ny * g.nz));
         switch (g.nz / 2) {
@@ -45,7 +46,7 @@ struct FFTPlan {
         constexpr int RR = prows(MM);                                                               \
         fft_z_products_kernel<T, MM, RR>                                                            \
             <<<dim3((nrows + RR - 1) / RR, nruns), RR * Split<MM>::N1, psmem(MM), st>>>(            \
-                io, fs_c, run_stride_c, nrows, g.hnzp, tw_zm, tw_zn, scale);                        \
+                io, fs_c, run_stride_c, nrows, g.hnzp, tw_zm, tw_zn, scale, kz_keep, kz_span);      \
     } break;
             SPM_ZP(4) SPM_ZP(8) SPM_ZP(16) SPM_ZP(32) SPM_ZP(64) SPM_ZP(128) SPM_ZP(256)
 #undef SPM_ZP
@@ -55,14 +56,14 @@ struct FFTPlan {
     }
     // Fused f = up - min(phi_sum,1) u and forward z pass (three fields).
     cudaError_t z_makef(T *up, const T *u, const T *phis, size_t fs_c, int nruns, size_t run_stride_c,
-                        cudaStream_t st) const {
+                        cudaStream_t st, int kz_span) const {
         const int nrows = g.nx * g.ny;
         switch (g.nz / 2) {
 #define SPM_ZF(MM)                                                                                         \
     case MM: {                                                                                             \
         constexpr int RR = zrows(MM);                                                                      \
         fft_z_makef_kernel<T, MM, RR><<<dim3((nrows + RR - 1) / RR, nruns), RR * Split<MM>::N1, 0, st>>>( \
-            up, u, phis, fs_c, run_stride_c, nrows, g.hnzp, tw_zm, tw_zn);                                 \
+            up, u, phis, fs_c, run_stride_c, nrows, g.hnzp, tw_zm, tw_zn, kz_span);                        \
     } break;
             SPM_ZF(4) SPM_ZF(8) SPM_ZF(16) SPM_ZF(32) SPM_ZF(64) SPM_ZF(128) SPM_ZF(256)
 #undef SPM_ZF
@@ -121,14 +122,14 @@ struct FFTPlan {
         return cudaGetLastError();
     }
     cudaError_t z_c2r(const cplx<T> *in, T *out, int nfields, size_t fs_c, size_t fs_real, T scale,
-                      cudaStream_t st) const {
+                      cudaStream_t st, int kz_keep = 1 << 30) const {
         const int nrows = g.nx * g.ny;
         switch (g.nz / 2) {
 #define SPM_ZC2R(MM)                                                                                   \
     case MM: {                                                                                         \
         constexpr int RR = zrows(MM);                                                                  \
         fft_z_c2r_kernel<T, MM, RR><<<dim3((nrows + RR - 1) / RR, nfields), RR * Split<MM>::N1, 0, st>>>( \
-            in, out, fs_c, fs_real, nrows, g.hnzp, tw_zm, tw_zn, scale);                               \
+            in, out, fs_c, fs_real, nrows, g.hnzp, tw_zm, tw_zn, scale, kz_keep);                      \
     } break;
             SPM_ZC2R(4) SPM_ZC2R(8) SPM_ZC2R(16) SPM_ZC2R(32) SPM_ZC2R(64) SPM_ZC2R(128) SPM_ZC2R(256)
 #undef SPM_ZC2R
@@ -146,12 +147,14 @@ struct FFTPlan {
     int           sm_count    = 148;
 
     template <int DIR>
-    cudaError_t strided_tma(cplx<T> *data, int nfields, size_t fs_c, int axis, cudaStream_t st) const {
+    cudaError_t strided_tma(cplx<T> *data, int nfields, size_t fs_c, int axis, cudaStream_t st,
+                            PassPrune pr) const {
         const int n = axis == 1 ? g.ny : g.nx;
         if (n > 256 || !encode_tiled_fn()) return cudaErrorNotSupported;
-        const int outer     = axis == 1 ? g.nx : g.ny;
-        const int col_tiles = (g.hnz + W_T - 1) / W_T;
-        const int ntiles    = nfields * outer * col_tiles;
+        const int outer   = axis == 1 ? g.nx : g.ny;
+        const int ct_used = (std::min(pr.kz_cols, g.hnz) + W_T - 1) / W_T;
+        const int ntiles  = nfields * outer_count(outer, pr.outer_trn) * ct_used;
+        if (ntiles == 0) return cudaSuccess;
         CUtensorMap   map;
         const uint64_t dims[4] = {(uint64_t)2 * g.hnz, (uint64_t)g.ny, (uint64_t)g.nx, (uint64_t)nfields};
         const uint64_t strides[3] = {(uint64_t)2 * g.hnzp * sizeof(T), (uint64_t)g.ny * 2 * g.hnzp * sizeof(T),
@@ -165,9 +168,8 @@ struct FFTPlan {
 #define SPM_TMA(NN)                                                                                            \
     case NN:                                                                                                   \
         fft_strided_tma_kernel<T, NN, W_T, DIR, S_T>                                                           \
-            <<<grid, W_T * Split<NN>::N1, (size_t)S_T * NN * W_T * sizeof(cplx<T>), st>>>(map, axis, outer,    \
-                                                                                          col_tiles, ntiles, tw, \
-                                                                                          err);                \
+            <<<grid, W_T * Split<NN>::N1, (size_t)S_T * NN * W_T * sizeof(cplx<T>), st>>>(                     \
+                map, axis, outer, ct_used, ntiles, tw, err, pr);                                               \
         break;
             SPM_TMA(8) SPM_TMA(16) SPM_TMA(32) SPM_TMA(64) SPM_TMA(128) SPM_TMA(256)
 #undef SPM_TMA
@@ -175,28 +177,38 @@ struct FFTPlan {
         }
         return cudaGetLastError();
     }
+    template <int DIR>
+    cudaError_t strided_tma(cplx<T> *data, int nfields, size_t fs_c, int axis, cudaStream_t st) const {
+        return strided_tma<DIR>(data, nfields, fs_c, axis, st, PassPrune::full(g.hnz));
+    }
 
     // axis 1 = Y, axis 0 = X
     template <int DIR>
-    cudaError_t strided(cplx<T> *data, int nfields, size_t fs_c, int axis, cudaStream_t st) const {
+    cudaError_t strided(cplx<T> *data, int nfields, size_t fs_c, int axis, cudaStream_t st, PassPrune pr) const {
         const int    n            = axis == 1 ? g.ny : g.nx;
         const int    outer        = axis == 1 ? g.nx : g.ny;
         const size_t outer_stride = axis == 1 ? (size_t)g.ny * g.hnzp : (size_t)g.hnzp;
         const size_t axis_stride  = axis == 1 ? (size_t)g.hnzp : (size_t)g.ny * g.hnzp;
         const cplx<T> *tw         = axis == 1 ? tw_y : tw_x;
-        const int    col_tiles    = (g.hnz + W - 1) / W;
-        const dim3   grid(outer * col_tiles, nfields);
+        const int    ct_used      = (std::min(pr.kz_cols, g.hnz) + W - 1) / W;
+        const int    nblocks      = outer_count(outer, pr.outer_trn) * ct_used;
+        if (nblocks == 0 || nfields == 0) return cudaSuccess;
+        const dim3   grid(nblocks, nfields);
         switch (n) {
 #define SPM_STR(NN)                                                                                              \
     case NN:                                                                                                     \
         fft_strided_kernel<T, NN, W, DIR><<<grid, W * Split<NN>::N1, (size_t)NN * W * sizeof(cplx<T>), st>>>( \
-            data, fs_c, g.hnz, col_tiles, outer_stride, axis_stride, tw);                                       \
+            data, fs_c, g.hnz, ct_used, outer, outer_stride, axis_stride, tw, pr);                              \
         break;
             SPM_STR(8) SPM_STR(16) SPM_STR(32) SPM_STR(64) SPM_STR(128) SPM_STR(256) SPM_STR(512)
 #undef SPM_STR
             default: return cudaErrorInvalidValue;
         }
         return cudaGetLastError();
+    }
+    template <int DIR>
+    cudaError_t strided(cplx<T> *data, int nfields, size_t fs_c, int axis, cudaStream_t st) const {
+        return strided<DIR>(data, nfields, fs_c, axis, st, PassPrune::full(g.hnz));
     }
 
     // Sets the shared-memory limits of every FFT kernel (process-wide

@@ -118,20 +118,41 @@ __device__ __forceinline__ void i_cross(T kx, T ky, T kz, const cplx<T> a[3], cp
     out[2] = cplx<T>{-(kx * a[1].im - ky * a[0].im), kx * a[1].re - ky * a[0].re};
 }
 
+// Compensated accumulation (hi, lo) += d by TwoSum (Knuth): hi + lo carries
+// the value to about twice the working precision, so the rounding of many
+// small FP32 increments does not accumulate in the state.
+template <typename T>
+__device__ __forceinline__ void comp_add(T &hi, T &lo, T d) {
+    const T t  = d + lo;
+    const T s  = hi + t;
+    const T bp = s - hi;
+    lo         = (hi - (s - bp)) + (t - bp);
+    hi         = s;
+}
+template <typename T>
+__device__ __forceinline__ void comp_add(cplx<T> &hi, cplx<T> &lo, cplx<T> d) {
+    comp_add<T>(hi.re, lo.re, d.re);
+    comp_add<T>(hi.im, lo.im, d.im);
+}
+
 // ---------------------------------------------------------------------------
 // zeta (2/3-truncated on the fly) -> u_hat (3 fields).  Zeta_k2u_k with the
 // preceding Truncate_two_third_rule (fft_wrapper.cxx:591-688,
 // fft_wrapper.h:754-796).  uk_dc is inserted into the real part of k = 0.
+// With `box` only the retained 2/3 box is visited (the pruned inverse passes
+// read everything outside it as zero); k_ns_update and k_project_add_curl
+// take the same flag and then leave modes outside the box untouched (zero).
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_zeta_to_u(Grid g, const cplx<T> *__restrict__ z0p, const cplx<T> *__restrict__ z1p,
                             const double *__restrict__ uk_dc, cplx<T> *__restrict__ u0, cplx<T> *__restrict__ u1,
-                            cplx<T> *__restrict__ u2, int truncate, size_t run_stride_c) {
+                            cplx<T> *__restrict__ u2, int truncate, size_t run_stride_c, int box) {
     const size_t ro = blockIdx.y * run_stride_c;
     z0p += ro, z1p += ro, u0 += ro, u1 += ro, u2 += ro;
     uk_dc += blockIdx.y * kRunWordStride;
-    const size_t n = g.field_elems_c();
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+    const size_t n = box ? g.box_elems() : g.field_elems_c();
+    for (size_t bi = blockIdx.x * (size_t)blockDim.x + threadIdx.x; bi < n; bi += (size_t)gridDim.x * blockDim.x) {
+        const size_t idx = box ? g.box_index(bi) : bi;
         KPoint p;
         size_t row;
         if (!k_point(g, idx, p, row)) {
@@ -189,16 +210,20 @@ template <typename T>
 __global__ void k_ns_update(Grid g, cplx<T> *__restrict__ z0p, cplx<T> *__restrict__ z1p,
                             const cplx<T> *__restrict__ p_u2u3, const cplx<T> *__restrict__ p_u3u1,
                             const cplx<T> *__restrict__ p_u1u2, const cplx<T> *__restrict__ p_a0,
-                            const cplx<T> *__restrict__ p_a1, double nu, double dt, size_t run_stride_c) {
+                            const cplx<T> *__restrict__ p_a1, double nu, double dt, size_t run_stride_c,
+                            int box, cplx<T> *__restrict__ zl0, cplx<T> *__restrict__ zl1) {
     const size_t ro = blockIdx.y * run_stride_c;
     z0p += ro, z1p += ro, p_u2u3 += ro, p_u3u1 += ro, p_u1u2 += ro, p_a0 += ro, p_a1 += ro;
-    const size_t n = g.field_elems_c();
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+    if (zl0) zl0 += ro, zl1 += ro;
+    const size_t n = box ? g.box_elems() : g.field_elems_c();
+    for (size_t bi = blockIdx.x * (size_t)blockDim.x + threadIdx.x; bi < n; bi += (size_t)gridDim.x * blockDim.x) {
+        const size_t idx = box ? g.box_index(bi) : bi;
         KPoint p;
         size_t row;
         if (!k_point(g, idx, p, row)) continue;
         if (!p.keep) {
             z0p[idx] = z1p[idx] = cplx<T>{0, 0};
+            if (zl0) zl0[idx] = zl1[idx] = cplx<T>{0, 0};
             continue;
         }
         const T k1 = (T)p.kx, k2 = (T)p.ky, k3 = (T)p.kz;
@@ -225,12 +250,39 @@ __global__ void k_ns_update(Grid g, cplx<T> *__restrict__ z0p, cplx<T> *__restri
         }
         c = (T)((1.0 / nu) * (k2sum > 0.0 ? 1.0 / k2sum : 0.0));
         cplx<T> z0 = z0p[idx], z1 = z1p[idx];
-        z0.re += dmy * (z0.re - c * f0.re);
-        z0.im += dmy * (z0.im - c * f0.im);
-        z1.re += dmy * (z1.re - c * f1.re);
-        z1.im += dmy * (z1.im - c * f1.im);
+        if (zl0) {
+            // compensated state: increment from (hi - c f) + lo, added by TwoSum
+            cplx<T> l0 = zl0[idx], l1 = zl1[idx];
+            const cplx<T> d0 = {dmy * ((z0.re - c * f0.re) + l0.re), dmy * ((z0.im - c * f0.im) + l0.im)};
+            const cplx<T> d1 = {dmy * ((z1.re - c * f1.re) + l1.re), dmy * ((z1.im - c * f1.im) + l1.im)};
+            comp_add<T>(z0, l0, d0);
+            comp_add<T>(z1, l1, d1);
+            zl0[idx] = l0;
+            zl1[idx] = l1;
+        } else {
+            z0.re += dmy * (z0.re - c * f0.re);
+            z0.im += dmy * (z0.im - c * f0.im);
+            z1.re += dmy * (z1.re - c * f1.re);
+            z1.im += dmy * (z1.im - c * f1.im);
+        }
         z0p[idx] = z0;
         z1p[idx] = z1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Truncate_two_third_rule (fft_wrapper.h:754-796) of the two zeta fields, in
+// place over the whole grid: zeta uploaded by the host may carry modes the
+// step's retained-box kernels never visit.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_truncate2(Grid g, cplx<T> *__restrict__ z0, cplx<T> *__restrict__ z1) {
+    const size_t n = g.field_elems_c();
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        KPoint p;
+        size_t row;
+        if (k_point(g, idx, p, row) && p.keep) continue;
+        z0[idx] = z1[idx] = cplx<T>{0, 0};
     }
 }
 
@@ -313,23 +365,25 @@ __global__ void k_u_to_zeta(Grid g, const cplx<T> *__restrict__ u0, const cplx<T
 template <typename T>
 __global__ void k_project_add_curl(Grid g, const cplx<T> *__restrict__ f0p, const cplx<T> *__restrict__ f1p,
                                    const cplx<T> *__restrict__ f2p, cplx<T> *__restrict__ z0p,
-                                   cplx<T> *__restrict__ z1p, double *__restrict__ uk_dc, size_t run_stride_c) {
+                                   cplx<T> *__restrict__ z1p, double *__restrict__ uk_dc, size_t run_stride_c,
+                                   int box, cplx<T> *__restrict__ zl0, cplx<T> *__restrict__ zl1) {
     const size_t ro = blockIdx.y * run_stride_c;
     f0p += ro, f1p += ro, f2p += ro, z0p += ro, z1p += ro;
+    if (zl0) zl0 += ro, zl1 += ro;
     uk_dc += blockIdx.y * kRunWordStride;
-    const size_t n = g.field_elems_c();
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+    const size_t n = box ? g.box_elems() : g.field_elems_c();
+    for (size_t bi = blockIdx.x * (size_t)blockDim.x + threadIdx.x; bi < n; bi += (size_t)gridDim.x * blockDim.x) {
+        const size_t idx = box ? g.box_index(bi) : bi;
         KPoint p;
         size_t row;
-        if (!k_point(g, idx, p, row) || !p.keep) {
+        if (!k_point(g, idx, p, row) || !p.keep || idx == 0) {
+            if (idx == 0) {
+                uk_dc[0] += (double)f0p[0].re;
+                uk_dc[1] += (double)f1p[0].re;
+                uk_dc[2] += (double)f2p[0].re;
+            }
             z0p[idx] = z1p[idx] = cplx<T>{0, 0};
-            continue;
-        }
-        if (idx == 0) {
-            uk_dc[0] += (double)f0p[0].re;
-            uk_dc[1] += (double)f1p[0].re;
-            uk_dc[2] += (double)f2p[0].re;
-            z0p[0] = z1p[0] = cplx<T>{0, 0};
+            if (zl0) zl0[idx] = zl1[idx] = cplx<T>{0, 0};
             continue;
         }
         const T kx = (T)p.kx, ky = (T)p.ky, kz = (T)p.kz, ik2 = ik2_of<T>(p);
@@ -343,6 +397,22 @@ __global__ void k_project_add_curl(Grid g, const cplx<T> *__restrict__ f0p, cons
         f[2].re -= dr * kz;
         f[2].im -= di * kz;
         cplx<T> om[3], u[3];
+        if (zl0) {
+            // compensated state: curl(i k x omega(zeta) / k^2) = omega exactly
+            // for a solenoidal omega, so zeta_new = zeta + zeta(i k x P f);
+            // only that increment is formed and added by TwoSum
+            i_cross<T>(kx, ky, kz, f, om);
+            cplx<T> a, b;
+            omega_to_zeta<T>(p, om, a, b);
+            cplx<T> z0 = z0p[idx], z1 = z1p[idx], l0 = zl0[idx], l1 = zl1[idx];
+            comp_add<T>(z0, l0, a);
+            comp_add<T>(z1, l1, b);
+            z0p[idx] = z0;
+            z1p[idx] = z1;
+            zl0[idx] = l0;
+            zl1[idx] = l1;
+            continue;
+        }
         zeta_to_omega<T>(p, z0p[idx], z1p[idx], om);
         i_cross<T>(kx * ik2, ky * ik2, kz * ik2, om, u);
 #pragma unroll
