@@ -246,6 +246,18 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
 //          are discarded); st(n, z) receives z = (x[2n], x[2n+1]) * scale-
 //          normalised output.
 // ---------------------------------------------------------------------------
+// Workspace index of a z-row transform: one complex of padding after every
+// N1 values, so the step-2 reads of the four-step FFT (stride N1) hit
+// distinct shared-memory banks.  ws_len<M> complex per row.
+template <int M>
+__device__ __forceinline__ int wsi(int i) {
+    return i + i / Split<M>::N1;
+}
+template <int M>
+constexpr int ws_len() {
+    return M + 2 + (M + 1) / Split<M>::N1;
+}
+
 template <typename T, int M, class Ld, class St>
 __device__ __forceinline__ void r2c_row(int t, Ld ld, cplx<T> *s, const cplx<T> *__restrict__ twM,
                                         const cplx<T> *__restrict__ twN, St st) {
@@ -259,14 +271,14 @@ __device__ __forceinline__ void r2c_row(int t, Ld ld, cplx<T> *s, const cplx<T> 
 #pragma unroll
     for (int k1 = 1; k1 < M2; k1++) v[k1] = cmul(v[k1], twM[(t * k1) & (M - 1)]);
 #pragma unroll
-    for (int k1 = 0; k1 < M2; k1++) s[t + M1 * k1] = v[k1];
+    for (int k1 = 0; k1 < M2; k1++) s[wsi<M>(t + M1 * k1)] = v[k1];
     __syncthreads();
     cplx<T> z[M2 / M1][M1];
 #pragma unroll
     for (int i = 0; i < M2 / M1; i++) {
         const int k1 = t + M1 * i;
 #pragma unroll
-        for (int n1 = 0; n1 < M1; n1++) z[i][n1] = s[n1 + M1 * k1];
+        for (int n1 = 0; n1 < M1; n1++) z[i][n1] = s[wsi<M>(n1 + M1 * k1)];
         dft_reg<T, M1, -1>(z[i]);
     }
     __syncthreads();
@@ -274,14 +286,14 @@ __device__ __forceinline__ void r2c_row(int t, Ld ld, cplx<T> *s, const cplx<T> 
     for (int i = 0; i < M2 / M1; i++) {
         const int k1 = t + M1 * i;
 #pragma unroll
-        for (int k2 = 0; k2 < M1; k2++) s[k1 + M2 * k2] = z[i][k2];
+        for (int k2 = 0; k2 < M1; k2++) s[wsi<M>(k1 + M2 * k2)] = z[i][k2];
     }
     __syncthreads();
     // X[k] = E[k] + W_N^k O[k],  E = (Z[k] + conj Z[M-k]) / 2,
     // O = -i (Z[k] - conj Z[M-k]) / 2,  k = 0..M.
     for (int k = t; k <= M; k += P) {
-        const cplx<T> zk  = s[k & (M - 1)];
-        const cplx<T> zmk = s[(M - k) & (M - 1)];
+        const cplx<T> zk  = s[wsi<M>(k & (M - 1))];
+        const cplx<T> zmk = s[wsi<M>((M - k) & (M - 1))];
         const T       er  = (T)0.5 * (zk.re + zmk.re);
         const T       ei  = (T)0.5 * (zk.im - zmk.im);
         const T       orr = (T)0.5 * (zk.im + zmk.im);
@@ -313,7 +325,7 @@ __device__ __forceinline__ void c2r_row(int t, Ld ld, cplx<T> *s, const cplx<T> 
         if (k <= M) {
             cplx<T> x = xl[i];
             if (k == 0 || k == M) x.im = 0;
-            s[k] = x;
+            s[wsi<M>(k)] = x;
         }
     }
     __syncthreads();
@@ -324,8 +336,8 @@ __device__ __forceinline__ void c2r_row(int t, Ld ld, cplx<T> *s, const cplx<T> 
 #pragma unroll
     for (int i = 0; i < KPT; i++) {
         const int     k   = t + P * i;
-        const cplx<T> xk  = s[k];
-        const cplx<T> xmk = s[M - k];
+        const cplx<T> xk  = s[wsi<M>(k)];
+        const cplx<T> xmk = s[wsi<M>(M - k)];
         const T       er  = scale * (xk.re + xmk.re);
         const T       ei  = scale * (xk.im - xmk.im);
         const T       dr  = scale * (xk.re - xmk.re);
@@ -337,11 +349,11 @@ __device__ __forceinline__ void c2r_row(int t, Ld ld, cplx<T> *s, const cplx<T> 
     }
     __syncthreads();
 #pragma unroll
-    for (int i = 0; i < KPT; i++) s[t + P * i] = zz[i];
+    for (int i = 0; i < KPT; i++) s[wsi<M>(t + P * i)] = zz[i];
     __syncthreads();
     cplx<T> v[M2];
 #pragma unroll
-    for (int m = 0; m < M2; m++) v[m] = s[t + M1 * m];
+    for (int m = 0; m < M2; m++) v[m] = s[wsi<M>(t + M1 * m)];
     dft_reg<T, M2, +1>(v);
 #pragma unroll
     for (int k1 = 1; k1 < M2; k1++) {
@@ -350,14 +362,14 @@ __device__ __forceinline__ void c2r_row(int t, Ld ld, cplx<T> *s, const cplx<T> 
         v[k1]     = cmul(v[k1], w);
     }
 #pragma unroll
-    for (int k1 = 0; k1 < M2; k1++) s[t + M1 * k1] = v[k1];
+    for (int k1 = 0; k1 < M2; k1++) s[wsi<M>(t + M1 * k1)] = v[k1];
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < M2 / M1; i++) {
         const int k1 = t + M1 * i;
         cplx<T>   u[M1];
 #pragma unroll
-        for (int n1 = 0; n1 < M1; n1++) u[n1] = s[n1 + M1 * k1];
+        for (int n1 = 0; n1 < M1; n1++) u[n1] = s[wsi<M>(n1 + M1 * k1)];
         dft_reg<T, M1, +1>(u);
 #pragma unroll
         for (int k2 = 0; k2 < M1; k2++) st(k1 + M2 * k2, u[k2]);
@@ -390,7 +402,7 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
     fft_z_r2c_kernel(const T *in, cplx<T> *out, size_t field_stride_real, size_t field_stride_c, int nrows,
                      int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN) {
     constexpr int P = Split<M>::N1;
-    __shared__ __align__(16) cplx<T> s[R][M];
+    __shared__ __align__(16) cplx<T> s[R][ws_len<M>()];
     const int r   = threadIdx.x / P;
     const int t   = threadIdx.x % P;
     const int row = blockIdx.x * R + r;
@@ -416,7 +428,7 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
                      int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale,
                      int kz_keep) {
     constexpr int P = Split<M>::N1;
-    __shared__ __align__(16) cplx<T> s[R][M + 1];
+    __shared__ __align__(16) cplx<T> s[R][ws_len<M>()];
     const int r   = threadIdx.x / P;
     const int t   = threadIdx.x % P;
     const int row = blockIdx.x * R + r;
@@ -451,7 +463,7 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
     io += (size_t)blockIdx.y * run_stride_c;  // run of a batched pool
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T       *U  = reinterpret_cast<T *>(smem_raw);                 // [3][R][PITCH]
-    cplx<T> *ws = reinterpret_cast<cplx<T> *>(U + 3 * R * PITCH);   // [R][M+1]
+    cplx<T> *ws = reinterpret_cast<cplx<T> *>(U + 3 * R * PITCH);   // [R][ws_len<M>]
     const int r   = threadIdx.x / P;
     const int t   = threadIdx.x % P;
     const int row = blockIdx.x * R + r;
@@ -480,7 +492,7 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
         const cplx<T> *rin = reinterpret_cast<const cplx<T> *>(Ur[d]);
         T             *ur  = Ur[d];
         c2r_row<T, M>(
-            t, [&](int k) { return (ok && k < kz_keep) ? rin[k] : cplx<T>{0, 0}; }, ws + r * (M + 1), twM, twN,
+            t, [&](int k) { return (ok && k < kz_keep) ? rin[k] : cplx<T>{0, 0}; }, ws + r * ws_len<M>(), twM, twN,
             scale,
             [&](int n, cplx<T> z) {
                 ur[2 * n]     = z.re;
@@ -502,7 +514,7 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
                 }
                 return cplx<T>{o[0], o[1]};
             },
-            ws + r * (M + 1), twM, twN,
+            ws + r * ws_len<M>(), twM, twN,
             [&](int k, cplx<T> X) {
                 if (ok && k < kz_span) rout[k] = X;
             });
@@ -526,7 +538,7 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
     up += (size_t)blockIdx.y * 2 * run_stride_c;  // run of a batched pool
     u += (size_t)blockIdx.y * 2 * run_stride_c;
     phi_sum += (size_t)blockIdx.y * 2 * run_stride_c;
-    __shared__ __align__(16) cplx<T> s[R][M];
+    __shared__ __align__(16) cplx<T> s[R][ws_len<M>()];
     const int r   = threadIdx.x / P;
     const int t   = threadIdx.x % P;
     const int row = blockIdx.x * R + r;

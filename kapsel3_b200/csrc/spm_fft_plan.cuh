@@ -18,11 +18,12 @@ struct FFTPlan {
     cplx<T> *tw_zn = nullptr;  // e^{-2 pi i k/NZ}, k <= NZ/2
 
     static constexpr int W = sizeof(T) == 8 ? 16 : 32;  // kz columns per strided tile
-    // rows per Z-pass CTA: 16, fewer for long rows so a CTA's row buffer
-    // stays within 33 KB of static shared memory
+    // rows per Z-pass CTA: 16, fewer (a power of two) for long rows so a
+    // CTA's row workspaces stay within 46 KB of static shared memory
     static constexpr int zrows(int m) {
-        return (int)(32768 / (m * sizeof(cplx<T>))) >= 16 ? 16 : (int)(32768 / (m * sizeof(cplx<T>)));
+        return pow2_floor_16((int)(47104 / ((size_t)ws_len_of(m) * sizeof(cplx<T>))));
     }
+    static constexpr int pow2_floor_16(int r) { return r >= 16 ? 16 : r >= 8 ? 8 : r >= 4 ? 4 : r >= 2 ? 2 : 1; }
 
     // rows per CTA of the fused products kernel (three staged rows + workspace
     // per row, kept within about 66 KB of dynamic shared memory)
@@ -30,10 +31,15 @@ struct FFTPlan {
         return (int)(65536 / (8 * m * sizeof(T))) >= 16 ? 16 : (int)(65536 / (8 * m * sizeof(T)));
     }
     static constexpr size_t psmem(int m) {
-        return (size_t)prows(m) * (3 * 2 * (m + 2) * sizeof(T) + (m + 1) * sizeof(cplx<T>));
+        return (size_t)prows(m) * (3 * 2 * (m + 2) * sizeof(T) + (size_t)ws_len_of(m) * sizeof(cplx<T>));
     }
 
     static bool size_ok(int n) { return n >= 8 && n <= 512 && (n & (n - 1)) == 0; }
+    // ws_len<M>() for a runtime M (Split<M>::N1 of spm_dft.cuh)
+    static constexpr int ws_len_of(int m) {
+        const int n1 = m <= 8 ? 2 : m <= 32 ? 4 : m <= 128 ? 8 : 16;
+        return m + 2 + (m + 1) / n1;
+    }
 
     // Fused inverse-z / advection products / forward-z pass over five slots.
     cudaError_t z_products(cplx<T> *io, size_t fs_c, int nruns, size_t run_stride_c, cudaStream_t st, int kz_keep,
