@@ -80,6 +80,12 @@ struct spm_ctx {
     Phys         ph{};
     cudaStream_t st         = nullptr;
     bool         own_stream = false;
+    // second stream of the step: the particle work that only needs the
+    // previous step's state (position update, phi scatter, Lennard-Jones
+    // forces, clearing the scatter slots) runs on it beside the fluid solver
+    cudaStream_t side     = nullptr;
+    cudaEvent_t  ev_fork  = nullptr;
+    cudaEvent_t  ev_join  = nullptr;
     void *       arena      = nullptr;  // slot 0 of this run's fields
     size_t       fstride_c  = 0;        // complex elements per field
     size_t       slot_stride_c = 0;     // complex elements between two slots of this run
@@ -512,19 +518,44 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
     int rc;
     for (int r = 0; r < nr; r++)
         if ((rc = truncate_if_dirty<T>(R[r])) != SPM_OK) return rc;
+    // fork: position update (Euler/AB2 from the previous velocities), phi
+    // scatter and Lennard-Jones forces need nothing from this step's fluid
+    // solve; they run on the side stream while the main stream advances zeta.
+    // The scatter slots are free here (the previous step consumed them).
+    SPM_CUDA_CHECK(cudaEventRecord(L->ev_fork, L->st));
+    SPM_CUDA_CHECK(cudaStreamWaitEvent(L->side, L->ev_fork, 0));
+    {
+        const cudaStream_t main_st = L->st;
+        L->st                      = L->side;
+        for (int r = 0; r < nr; r++) R[r]->st = L->side;
+        rc = clear_scatter_slots<T>(L);
+        for (int r = 0; r < nr && rc == SPM_OK; r++) {
+            spm_ctx *c = R[r];
+            if (c->ph.np == 0) continue;
+            auto side_work = [&]() -> int {
+                LAUNCH(c, p_position, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev, 1);
+                int e = phi_sum_scatter<T>(c, false);
+                if (e != SPM_OK) return e;
+                LAUNCH(c, p_forces, (c->ph.np + 3) / 4, 128, 0, c->ph, c->ps, 0, 0.0);
+                return SPM_OK;
+            };
+            rc = side_work();
+        }
+        L->st = main_st;
+        for (int r = 0; r < nr; r++) R[r]->st = main_st;
+        if (rc != SPM_OK) return rc;
+    }
+    SPM_CUDA_CHECK(cudaEventRecord(L->ev_join, L->side));
     if ((rc = ns_solver<T>(L)) != SPM_OK) return rc;
     LAUNCH(L, k_fix_cell, (nr + 127) / 128, 128, 0, L->rw, nr);
     if ((rc = zeta_to_velocity<T>(L, 1)) != SPM_OK) return rc;
-    if ((rc = clear_scatter_slots<T>(L)) != SPM_OK) return rc;
+    SPM_CUDA_CHECK(cudaStreamWaitEvent(L->st, L->ev_join, 0));  // join
     for (int r = 0; r < nr; r++) {
         spm_ctx *c = R[r];
         if (c->ph.np == 0) continue;
-        LAUNCH(c, p_position, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev, 1);
-        if ((rc = phi_sum_scatter<T>(c, false)) != SPM_OK) return rc;
         LAUNCH(c, s_hydro_force<T>, c->ph.np, 256, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
                c->ncells, c->real<T>(PHIS), c->real<T>(U0), c->real<T>(U1), c->real<T>(U2), c->ps.f_hydro,
                c->ps.torque_hydro);
-        LAUNCH(c, p_forces, (c->ph.np + 3) / 4, 128, 0, c->ph, c->ps, 0, 0.0);
         LAUNCH(c, p_velocity, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev);
         if (c->P.kbt > 0.0) LAUNCH(c, p_thermostat_serial, 1, 32, 0, c->ph, c->ps, c->mt);
         if ((rc = up_scatter<T>(c, false)) != SPM_OK) return rc;
@@ -705,6 +736,9 @@ void destroy_ctx(spm_ctx *c) {
     dev_free(c->le.dev);
     dev_free(c->le.ppart);
     dev_free(c->le.partial);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->own_stream && c->st) cudaStreamDestroy(c->st);
     delete c;
 }
@@ -739,6 +773,12 @@ int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *
             return fail(SPM_ERR_CUDA, "stream creation failed");
         }
         c->own_stream = true;
+    }
+    if (!lead && (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+                  cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+                  cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess)) {
+        destroy_ctx(c);
+        return fail(SPM_ERR_CUDA, "side stream / events");
     }
     c->fstride_c    = (size_t)c->g.nx * c->g.ny * c->g.hnzp;
     const int nslot = slots_for(p);

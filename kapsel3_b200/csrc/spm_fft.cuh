@@ -253,9 +253,21 @@ template <int M>
 __device__ __forceinline__ int wsi(int i) {
     return i + i / Split<M>::N1;
 }
-template <int M>
+// Row strides of the per-row shared buffers, in complex (pair) units: at
+// least `need`, and congruent to the P = N1 threads of a row modulo the pairs
+// per 128 bytes, so the rows that one shared-memory wavefront serves (a
+// half-warp of 8-byte or a quarter-warp of 16-byte accesses) fall on
+// disjoint banks.
+template <typename T, int M>
+constexpr int row_stride(int need) {
+    constexpr int mod = 128 / (int)sizeof(cplx<T>);
+    constexpr int p   = Split<M>::N1 % mod;
+    const int     r   = need % mod;
+    return need + ((p - r + mod) % mod);
+}
+template <typename T, int M>
 constexpr int ws_len() {
-    return M + 2 + (M + 1) / Split<M>::N1;
+    return row_stride<T, M>(M + 2 + (M + 1) / Split<M>::N1);
 }
 
 template <typename T, int M, class Ld, class St>
@@ -402,7 +414,7 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
     fft_z_r2c_kernel(const T *in, cplx<T> *out, size_t field_stride_real, size_t field_stride_c, int nrows,
                      int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN) {
     constexpr int P = Split<M>::N1;
-    __shared__ __align__(16) cplx<T> s[R][ws_len<M>()];
+    __shared__ __align__(16) cplx<T> s[R][ws_len<T, M>()];
     const int r   = threadIdx.x / P;
     const int t   = threadIdx.x % P;
     const int row = blockIdx.x * R + r;
@@ -428,7 +440,7 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
                      int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale,
                      int kz_keep) {
     constexpr int P = Split<M>::N1;
-    __shared__ __align__(16) cplx<T> s[R][ws_len<M>()];
+    __shared__ __align__(16) cplx<T> s[R][ws_len<T, M>()];
     const int r   = threadIdx.x / P;
     const int t   = threadIdx.x % P;
     const int row = blockIdx.x * R + r;
@@ -459,7 +471,7 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
                           const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale, int kz_keep,
                           int kz_span) {
     constexpr int P     = Split<M>::N1;
-    constexpr int PITCH = 2 * (M + 2);  // reals per staged row (>= 2 * hnzp)
+    constexpr int PITCH = 2 * row_stride<T, M>(M + 2);  // reals per staged row (>= 2 * hnzp)
     io += (size_t)blockIdx.y * run_stride_c;  // run of a batched pool
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T       *U  = reinterpret_cast<T *>(smem_raw);                 // [3][R][PITCH]
@@ -492,12 +504,9 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
         const cplx<T> *rin = reinterpret_cast<const cplx<T> *>(Ur[d]);
         T             *ur  = Ur[d];
         c2r_row<T, M>(
-            t, [&](int k) { return (ok && k < kz_keep) ? rin[k] : cplx<T>{0, 0}; }, ws + r * ws_len<M>(), twM, twN,
+            t, [&](int k) { return (ok && k < kz_keep) ? rin[k] : cplx<T>{0, 0}; }, ws + r * ws_len<T, M>(), twM, twN,
             scale,
-            [&](int n, cplx<T> z) {
-                ur[2 * n]     = z.re;
-                ur[2 * n + 1] = z.im;
-            });
+            [&](int n, cplx<T> z) { store_pair<T>(ur, n, z); });
     }
 #pragma unroll 1
     for (int p = 0; p < 5; p++) {
@@ -505,16 +514,18 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
         r2c_row<T, M>(
             t,
             [&](int n) {
-                T o[2];
+                const cplx<T> a = load_pair<T>(Ur[0], n), b = load_pair<T>(Ur[1], n), c = load_pair<T>(Ur[2], n);
+                const T       xs[2] = {a.re, a.im}, ys[2] = {b.re, b.im}, zs[2] = {c.re, c.im};
+                T             o[2];
 #pragma unroll
                 for (int e = 0; e < 2; e++) {
-                    const T x = Ur[0][2 * n + e], y = Ur[1][2 * n + e], z = Ur[2][2 * n + e];
+                    const T x = xs[e], y = ys[e], z = zs[e];
                     o[e] = p == 0 ? y * z : p == 1 ? z * x : p == 2 ? x * y : p == 3 ? (y - z) * (y + z)
                                                                                      : (z - x) * (z + x);
                 }
                 return cplx<T>{o[0], o[1]};
             },
-            ws + r * ws_len<M>(), twM, twN,
+            ws + r * ws_len<T, M>(), twM, twN,
             [&](int k, cplx<T> X) {
                 if (ok && k < kz_span) rout[k] = X;
             });
@@ -538,7 +549,7 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
     up += (size_t)blockIdx.y * 2 * run_stride_c;  // run of a batched pool
     u += (size_t)blockIdx.y * 2 * run_stride_c;
     phi_sum += (size_t)blockIdx.y * 2 * run_stride_c;
-    __shared__ __align__(16) cplx<T> s[R][ws_len<M>()];
+    __shared__ __align__(16) cplx<T> s[R][ws_len<T, M>()];
     const int r   = threadIdx.x / P;
     const int t   = threadIdx.x % P;
     const int row = blockIdx.x * R + r;

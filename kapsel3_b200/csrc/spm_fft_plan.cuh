@@ -31,14 +31,21 @@ struct FFTPlan {
         return (int)(65536 / (8 * m * sizeof(T))) >= 16 ? 16 : (int)(65536 / (8 * m * sizeof(T)));
     }
     static constexpr size_t psmem(int m) {
-        return (size_t)prows(m) * (3 * 2 * (m + 2) * sizeof(T) + (size_t)ws_len_of(m) * sizeof(cplx<T>));
+        return (size_t)prows(m) * (3 * 2 * stride_of(m, m + 2) * sizeof(T) + (size_t)ws_len_of(m) * sizeof(cplx<T>));
     }
 
     static bool size_ok(int n) { return n >= 8 && n <= 512 && (n & (n - 1)) == 0; }
     // ws_len<M>() for a runtime M (Split<M>::N1 of spm_dft.cuh)
     static constexpr int ws_len_of(int m) {
         const int n1 = m <= 8 ? 2 : m <= 32 ? 4 : m <= 128 ? 8 : 16;
-        return m + 2 + (m + 1) / n1;
+        return stride_of(m, m + 2 + (m + 1) / n1);
+    }
+    // row_stride<T, M>(need) of spm_fft.cuh for a runtime M
+    static constexpr int stride_of(int m, int need) {
+        const int n1  = m <= 8 ? 2 : m <= 32 ? 4 : m <= 128 ? 8 : 16;
+        const int mod = 128 / (int)sizeof(cplx<T>);
+        const int p = n1 % mod, r = need % mod;
+        return need + ((p - r + mod) % mod);
     }
 
     // Fused inverse-z / advection products / forward-z pass over five slots.
