@@ -305,7 +305,8 @@ def main():
     peaks = read_peaks()
     prof = results["prof"]
     roof = {"bound": "hbm", "kernel": prof["kernel"], "achieved": prof["gbs"], "peak": peaks["hbm_gbs"],
-            "unit": "GB/s", "frac": prof["gbs"] / peaks["hbm_gbs"], "traffic": None,
+            "unit": "GB/s", "frac": prof["gbs"] / peaks["hbm_gbs"], "traffic": read_traffic(),
+            "traffic_source": TRAFFIC_FILE,
             "peak_source": peaks["source"], "bytes_per_launch": prof["bytes"], "avg_launch_us": prof["us"],
             "note": "algorithmic bytes = one read + one write of every complex element the pass transforms"}
     line = {
@@ -420,6 +421,22 @@ def step_bytes(cfg, w):
     nx, ny, nz = cfg.shape
     S = nx * ny * (nz + 2) * w
     return 52 * S + cfg.n_particles * 1935 * 13 * 8
+
+
+TRAFFIC_FILE = "profiles/spm_step_fp32_256cubed_dram_traffic.md"
+
+
+def read_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    capture (dram__bytes_read.sum + dram__bytes_write.sum, averaged over the
+    step's strided passes); None if the summary is missing."""
+    try:
+        for line in open(os.path.join(ROOT, TRAFFIC_FILE)):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
 
 
 def read_peaks():

@@ -100,6 +100,8 @@ struct spm_ctx {
     FFTPlan<float>  *pp32 = &plan32;
     spm_pool        *pool = nullptr;  // pool this run belongs to (null for a lone run)
     int *        cells   = nullptr;
+    int *        sc_idx  = nullptr;  // stencil cache of the NS step: grid index per (particle, cell)
+    double *     sc_w    = nullptr;  // ... and its profile weight
     int          ncells  = 0;
     double *     uk_dc   = nullptr;  // rw->uk_dc
     double *     pbuf    = nullptr;  // particle state arrays
@@ -116,6 +118,7 @@ struct spm_ctx {
     std::vector<cudaEvent_t> prof_ev;
     double                   prof_bytes = 0.0;
     bool                     use_tma    = true;  // SPM_NO_TMA=1 selects the direct-load passes
+    bool                     overlap    = true;  // SPM_NO_OVERLAP=1 keeps the particle work on the main stream
     bool                     zeta_dirty = false;  // zeta set by the host since the last NS step
     int                      nslots     = NSLOT;  // field slots of this run (slots_for)
 
@@ -415,13 +418,13 @@ __global__ void k_zero3(double *uk_dc) {
 template <typename T>
 int zeta_to_velocity(spm_ctx *L, int truncate) {
     if (!truncate) {
-        LAUNCH(L, k_zeta_to_u<T>, L->pw_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
-               L->cx<T>(U1), L->cx<T>(U2), 0, L->fstride_c, 0);
+        LAUNCH(L, (k_zeta_to_u<T, 0>), L->pw_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
+               L->cx<T>(U1), L->cx<T>(U2), 0, L->fstride_c);
         return fft_inv<T>(L, U0, 3);
     }
     int rc;
-    LAUNCH(L, k_zeta_to_u<T>, L->box_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
-           L->cx<T>(U1), L->cx<T>(U2), 1, L->fstride_c, 1);
+    LAUNCH(L, (k_zeta_to_u<T, 1>), L->box_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
+           L->cx<T>(U1), L->cx<T>(U2), 1, L->fstride_c);
     if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 0, prune_inverse(L->g, 0))) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 1, prune_inverse(L->g, 1))) != SPM_OK) return rc;
     return z_pass<T>(L, U0, 3, false, L->g.trn[2]);
@@ -432,8 +435,8 @@ template <typename T>
 int ns_solver(spm_ctx *L) {
     int rc;
     // zeta -> u_hat (truncated) -> inverse x, y passes
-    LAUNCH(L, k_zeta_to_u<T>, L->box_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
-           L->cx<T>(U1), L->cx<T>(U2), 1, L->fstride_c, 1);
+    LAUNCH(L, (k_zeta_to_u<T, 1>), L->box_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
+           L->cx<T>(U1), L->cx<T>(U2), 1, L->fstride_c);
     if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 0, prune_inverse(L->g, 0))) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 1, prune_inverse(L->g, 1))) != SPM_OK) return rc;
     // inverse z + products + forward z in one pass, then forward y, x passes
@@ -442,8 +445,8 @@ int ns_solver(spm_ctx *L) {
     L->launches++;
     if ((rc = fft_strided_pass<T, -1>(L, U0, 5, 1, prune_forward(L->g, 1))) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, -1>(L, U0, 5, 0, prune_forward(L->g, 0))) != SPM_OK) return rc;
-    LAUNCH(L, k_ns_update<T>, L->box_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->cx<T>(U0), L->cx<T>(U1),
-           L->cx<T>(U2), L->cx<T>(A0), L->cx<T>(A1), L->ph.nu, L->ph.dt, L->fstride_c, 1, L->zl<T>(0), L->zl<T>(1));
+    LAUNCH(L, (k_ns_update<T, 2>), L->box_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->cx<T>(U0), L->cx<T>(U1),
+           L->cx<T>(U2), L->cx<T>(A0), L->cx<T>(A1), L->ph.nu, L->ph.dt, L->fstride_c, L->zl<T>(0), L->zl<T>(1));
     return SPM_OK;
 }
 
@@ -490,8 +493,8 @@ int rigidity_projection(spm_ctx *L) {
     L->launches++;
     if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 1, prune_forward(L->g, 1))) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 0, prune_forward(L->g, 0))) != SPM_OK) return rc;
-    LAUNCH(L, k_project_add_curl<T>, L->box_grid(), 256, 0, L->g, L->cx<T>(UP0), L->cx<T>(UP1), L->cx<T>(UP2),
-           L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->fstride_c, 1, L->zl<T>(0), L->zl<T>(1));
+    LAUNCH(L, (k_project_add_curl<T, 2>), L->box_grid(), 256, 0, L->g, L->cx<T>(UP0), L->cx<T>(UP1), L->cx<T>(UP2),
+           L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->fstride_c, L->zl<T>(0), L->zl<T>(1));
     return SPM_OK;
 }
 
@@ -522,20 +525,24 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
     // scatter and Lennard-Jones forces need nothing from this step's fluid
     // solve; they run on the side stream while the main stream advances zeta.
     // The scatter slots are free here (the previous step consumed them).
-    SPM_CUDA_CHECK(cudaEventRecord(L->ev_fork, L->st));
-    SPM_CUDA_CHECK(cudaStreamWaitEvent(L->side, L->ev_fork, 0));
+    const cudaStream_t side = L->overlap ? L->side : L->st;
+    if (L->overlap) {
+        SPM_CUDA_CHECK(cudaEventRecord(L->ev_fork, L->st));
+        SPM_CUDA_CHECK(cudaStreamWaitEvent(side, L->ev_fork, 0));
+    }
     {
         const cudaStream_t main_st = L->st;
-        L->st                      = L->side;
-        for (int r = 0; r < nr; r++) R[r]->st = L->side;
+        L->st                      = side;
+        for (int r = 0; r < nr; r++) R[r]->st = side;
         rc = clear_scatter_slots<T>(L);
         for (int r = 0; r < nr && rc == SPM_OK; r++) {
             spm_ctx *c = R[r];
             if (c->ph.np == 0) continue;
             auto side_work = [&]() -> int {
                 LAUNCH(c, p_position, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev, 1);
-                int e = phi_sum_scatter<T>(c, false);
-                if (e != SPM_OK) return e;
+                const dim3 sgrid((c->ncells + 127) / 128, c->ph.np);
+                LAUNCH(c, s_phi_scatter_cache<T>, sgrid, 128, 0, c->g, c->ph, c->ps.x, c->cells, c->ncells,
+                       c->real<T>(PHIS), c->err, c->sc_idx, c->sc_w);
                 LAUNCH(c, p_forces, (c->ph.np + 3) / 4, 128, 0, c->ph, c->ps, 0, 0.0);
                 return SPM_OK;
             };
@@ -545,20 +552,25 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
         for (int r = 0; r < nr; r++) R[r]->st = main_st;
         if (rc != SPM_OK) return rc;
     }
-    SPM_CUDA_CHECK(cudaEventRecord(L->ev_join, L->side));
+    if (L->overlap) SPM_CUDA_CHECK(cudaEventRecord(L->ev_join, side));
     if ((rc = ns_solver<T>(L)) != SPM_OK) return rc;
     LAUNCH(L, k_fix_cell, (nr + 127) / 128, 128, 0, L->rw, nr);
     if ((rc = zeta_to_velocity<T>(L, 1)) != SPM_OK) return rc;
-    SPM_CUDA_CHECK(cudaStreamWaitEvent(L->st, L->ev_join, 0));  // join
+    if (L->overlap) SPM_CUDA_CHECK(cudaStreamWaitEvent(L->st, L->ev_join, 0));  // join
     for (int r = 0; r < nr; r++) {
         spm_ctx *c = R[r];
         if (c->ph.np == 0) continue;
-        LAUNCH(c, s_hydro_force<T>, c->ph.np, 256, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
-               c->ncells, c->real<T>(PHIS), c->real<T>(U0), c->real<T>(U1), c->real<T>(U2), c->ps.f_hydro,
-               c->ps.torque_hydro);
+        LAUNCH(c, s_hydro_force_cached<T>, c->ph.np, 256, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
+               c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS), c->real<T>(U0), c->real<T>(U1), c->real<T>(U2),
+               c->ps.f_hydro, c->ps.torque_hydro);
         LAUNCH(c, p_velocity, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev);
         if (c->P.kbt > 0.0) LAUNCH(c, p_thermostat_serial, 1, 32, 0, c->ph, c->ps, c->mt);
-        if ((rc = up_scatter<T>(c, false)) != SPM_OK) return rc;
+        {
+            const dim3 sgrid((c->ncells + 127) / 128, c->ph.np);
+            LAUNCH(c, s_up_scatter_cached<T>, sgrid, 128, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
+                   c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS), c->real<T>(UP0), c->real<T>(UP1),
+                   c->real<T>(UP2));
+        }
     }
     if ((rc = rigidity_projection<T>(L)) != SPM_OK) return rc;
     LAUNCH(L, k_ts_advance, (nr + 127) / 128, 128, 0, L->rw, nr);
@@ -731,6 +743,8 @@ void destroy_ctx(spm_ctx *c) {
     if (c->owns_arena) dev_free(c->arena);
     if (c->owns_rw) dev_free(c->rw);
     dev_free(c->cells);
+    dev_free(c->sc_idx);
+    dev_free(c->sc_w);
     dev_free(c->pbuf);
     dev_free(c->mt);
     dev_free(c->le.dev);
@@ -786,6 +800,8 @@ int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *
     {
         const char *nt = getenv("SPM_NO_TMA");
         c->use_tma     = !(nt && nt[0] == '1');
+        const char *no = getenv("SPM_NO_OVERLAP");
+        c->overlap     = !(no && no[0] == '1');
     }
     cudaError_t e = cudaSuccess;
     if (lead) {
@@ -841,6 +857,14 @@ int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *
         dev_alloc((void **)&c->mt, 625 * sizeof(unsigned int)) != cudaSuccess) {
         destroy_ctx(c);
         return fail(SPM_ERR_NOMEM, "small device buffers");
+    }
+    if (p.equation == SPM_EQ_NAVIER_STOKES && p.n_particles > 0) {
+        const size_t nsc = (size_t)p.n_particles * cells.size();
+        if (dev_alloc((void **)&c->sc_idx, nsc * sizeof(int)) != cudaSuccess ||
+            dev_alloc((void **)&c->sc_w, nsc * sizeof(double)) != cudaSuccess) {
+            destroy_ctx(c);
+            return fail(SPM_ERR_NOMEM, "stencil cache");
+        }
     }
     cudaMemcpy(c->cells, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemset(c->pbuf, 0, (size_t)np * kPWords * sizeof(double));
@@ -938,7 +962,8 @@ int spm_device_bytes(const spm_params *p, size_t *bytes) {
     const size_t es  = p->precision == SPM_PREC_FP64 ? 8 : 4;
     const size_t fld = (size_t)g.nx * g.ny * g.hnzp * 2 * es;
     const size_t nslot = (size_t)slots_for(*p);
-    *bytes = nslot * fld + (size_t)std::max(p->n_particles, 1) * kPWords * 8 + 64 * 1024;
+    const size_t sc = p->equation == SPM_EQ_NAVIER_STOKES ? (size_t)p->n_particles * sekibun(*p).size() * 12 : 0;
+    *bytes = nslot * fld + (size_t)std::max(p->n_particles, 1) * kPWords * 8 + sc + 64 * 1024;
     return SPM_OK;
 }
 

@@ -51,12 +51,7 @@ struct KPoint {
     bool   keep;  // inside the 2/3-rule retained box
 };
 
-__device__ __forceinline__ bool k_point(const Grid &g, size_t idx, KPoint &p, size_t &row) {
-    const int kz = (int)(idx % (size_t)g.hnzp);
-    row          = idx / (size_t)g.hnzp;
-    const int j  = (int)(row % (size_t)g.ny);
-    const int i  = (int)(row / (size_t)g.ny);
-    if (kz >= g.hnz) return false;
+__device__ __forceinline__ void k_point_ijk(const Grid &g, int i, int j, int kz, KPoint &p) {
     p.KX   = i > g.nx / 2 ? i - g.nx : i;  // Calc_KX_Ooura (fft_wrapper.h:719)
     p.KY   = j > g.ny / 2 ? j - g.ny : j;
     p.KZ   = kz;
@@ -64,7 +59,67 @@ __device__ __forceinline__ bool k_point(const Grid &g, size_t idx, KPoint &p, si
     p.ky   = g.wave[1] * (double)p.KY;
     p.kz   = g.wave[2] * (double)p.KZ;
     p.keep = (abs(p.KX) < g.trn[0]) && (abs(p.KY) < g.trn[1]) && (p.KZ < g.trn[2]);
+}
+
+__device__ __forceinline__ bool k_point(const Grid &g, size_t idx, KPoint &p, size_t &row) {
+    const int kz = (int)(idx % (size_t)g.hnzp);
+    row          = idx / (size_t)g.hnzp;
+    const int j  = (int)(row % (size_t)g.ny);
+    const int i  = (int)(row / (size_t)g.ny);
+    if (kz >= g.hnz) return false;
+    k_point_ijk(g, i, j, kz, p);
     return true;
+}
+
+// Calls f(idx, p, valid) for the modes a k-space kernel visits.  BOX == 1:
+// only the retained 2/3 box; a warp walks one (kx, ky) row at a time with its
+// lanes on consecutive kz, so there is no per-element index division.
+// BOX == 2: the retained box, one mode per thread.
+// BOX == 0: every element of the field (valid = false on row padding).
+template <int BOX, class F>
+__device__ __forceinline__ void for_modes(const Grid &g, F f) {
+    if constexpr (BOX == 2) {
+        // retained box, one element per thread (heavier per-mode work: more
+        // independent modes in flight than the row walk)
+        const int    nyb = 2 * g.trn[1] - 1;
+        const size_t n   = g.box_elems();
+        for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < n; b += (size_t)gridDim.x * blockDim.x) {
+            const int kz = (int)(b % (size_t)g.trn[2]);
+            const int rr = (int)(b / (size_t)g.trn[2]);
+            const int iy = rr % nyb, ix = rr / nyb;
+            const int i  = ix < g.trn[0] ? ix : ix + g.nx - (2 * g.trn[0] - 1);
+            const int j  = iy < g.trn[1] ? iy : iy + g.ny - nyb;
+            KPoint    p;
+            k_point_ijk(g, i, j, kz, p);
+            f(((size_t)i * g.ny + j) * g.hnzp + kz, p, true);
+        }
+    } else if constexpr (BOX == 1) {
+        const int nyb    = 2 * g.trn[1] - 1;
+        const int nrows  = (2 * g.trn[0] - 1) * nyb;
+        const int lane   = threadIdx.x & 31;
+        const int warp   = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+        const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+        for (int rr = warp; rr < nrows; rr += nwarps) {
+            const int    iy   = rr % nyb, ix = rr / nyb;
+            const int    i    = ix < g.trn[0] ? ix : ix + g.nx - (2 * g.trn[0] - 1);
+            const int    j    = iy < g.trn[1] ? iy : iy + g.ny - nyb;
+            const size_t base = ((size_t)i * g.ny + j) * g.hnzp;
+            for (int kz = lane; kz < g.trn[2]; kz += 32) {
+                KPoint p;
+                k_point_ijk(g, i, j, kz, p);
+                f(base + kz, p, true);
+            }
+        }
+    } else {
+        const size_t n = g.field_elems_c();
+        for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n;
+             idx += (size_t)gridDim.x * blockDim.x) {
+            KPoint p;
+            size_t row;
+            const bool v = k_point(g, idx, p, row);
+            f(idx, p, v);
+        }
+    }
 }
 
 template <typename T>
@@ -143,21 +198,17 @@ __device__ __forceinline__ void comp_add(cplx<T> &hi, cplx<T> &lo, cplx<T> d) {
 // read everything outside it as zero); k_ns_update and k_project_add_curl
 // take the same flag and then leave modes outside the box untouched (zero).
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, int BOX>
 __global__ void k_zeta_to_u(Grid g, const cplx<T> *__restrict__ z0p, const cplx<T> *__restrict__ z1p,
                             const double *__restrict__ uk_dc, cplx<T> *__restrict__ u0, cplx<T> *__restrict__ u1,
-                            cplx<T> *__restrict__ u2, int truncate, size_t run_stride_c, int box) {
+                            cplx<T> *__restrict__ u2, int truncate, size_t run_stride_c) {
     const size_t ro = blockIdx.y * run_stride_c;
     z0p += ro, z1p += ro, u0 += ro, u1 += ro, u2 += ro;
     uk_dc += blockIdx.y * kRunWordStride;
-    const size_t n = box ? g.box_elems() : g.field_elems_c();
-    for (size_t bi = blockIdx.x * (size_t)blockDim.x + threadIdx.x; bi < n; bi += (size_t)gridDim.x * blockDim.x) {
-        const size_t idx = box ? g.box_index(bi) : bi;
-        KPoint p;
-        size_t row;
-        if (!k_point(g, idx, p, row)) {
+    for_modes<BOX>(g, [&](size_t idx, const KPoint &p, bool valid) {
+        if (!valid) {
             u0[idx] = u1[idx] = u2[idx] = cplx<T>{0, 0};
-            continue;
+            return;
         }
         cplx<T> u[3] = {{0, 0}, {0, 0}, {0, 0}};
         if (p.keep || !truncate) {
@@ -174,7 +225,7 @@ __global__ void k_zeta_to_u(Grid g, const cplx<T> *__restrict__ z0p, const cplx<
         u0[idx] = u[0];
         u1[idx] = u[1];
         u2[idx] = u[2];
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -206,25 +257,21 @@ __global__ void r_advection_products(Grid g, T *__restrict__ u0, T *__restrict__
 // retained box are written as zero (the reference truncates zeta in place at
 // the start of Zeta_k2advection_k and never updates those modes).
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, int BOX>
 __global__ void k_ns_update(Grid g, cplx<T> *__restrict__ z0p, cplx<T> *__restrict__ z1p,
                             const cplx<T> *__restrict__ p_u2u3, const cplx<T> *__restrict__ p_u3u1,
                             const cplx<T> *__restrict__ p_u1u2, const cplx<T> *__restrict__ p_a0,
                             const cplx<T> *__restrict__ p_a1, double nu, double dt, size_t run_stride_c,
-                            int box, cplx<T> *__restrict__ zl0, cplx<T> *__restrict__ zl1) {
+                            cplx<T> *__restrict__ zl0, cplx<T> *__restrict__ zl1) {
     const size_t ro = blockIdx.y * run_stride_c;
     z0p += ro, z1p += ro, p_u2u3 += ro, p_u3u1 += ro, p_u1u2 += ro, p_a0 += ro, p_a1 += ro;
     if (zl0) zl0 += ro, zl1 += ro;
-    const size_t n = box ? g.box_elems() : g.field_elems_c();
-    for (size_t bi = blockIdx.x * (size_t)blockDim.x + threadIdx.x; bi < n; bi += (size_t)gridDim.x * blockDim.x) {
-        const size_t idx = box ? g.box_index(bi) : bi;
-        KPoint p;
-        size_t row;
-        if (!k_point(g, idx, p, row)) continue;
+    for_modes<BOX>(g, [&](size_t idx, const KPoint &p, bool valid) {
+        if (!valid) return;
         if (!p.keep) {
             z0p[idx] = z1p[idx] = cplx<T>{0, 0};
             if (zl0) zl0[idx] = zl1[idx] = cplx<T>{0, 0};
-            continue;
+            return;
         }
         const T k1 = (T)p.kx, k2 = (T)p.ky, k3 = (T)p.kz;
         const T k1k2 = k1 * k2, k2k3 = k2 * k3, k3k1 = k3 * k1;
@@ -267,7 +314,7 @@ __global__ void k_ns_update(Grid g, cplx<T> *__restrict__ z0p, cplx<T> *__restri
         }
         z0p[idx] = z0;
         z1p[idx] = z1;
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -362,21 +409,17 @@ __global__ void k_u_to_zeta(Grid g, const cplx<T> *__restrict__ u0, const cplx<T
 // Modes outside the 2/3 box come out exactly zero (the reference leaves
 // round-off there, which its next step truncates before use).
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, int BOX>
 __global__ void k_project_add_curl(Grid g, const cplx<T> *__restrict__ f0p, const cplx<T> *__restrict__ f1p,
                                    const cplx<T> *__restrict__ f2p, cplx<T> *__restrict__ z0p,
                                    cplx<T> *__restrict__ z1p, double *__restrict__ uk_dc, size_t run_stride_c,
-                                   int box, cplx<T> *__restrict__ zl0, cplx<T> *__restrict__ zl1) {
+                                   cplx<T> *__restrict__ zl0, cplx<T> *__restrict__ zl1) {
     const size_t ro = blockIdx.y * run_stride_c;
     f0p += ro, f1p += ro, f2p += ro, z0p += ro, z1p += ro;
     if (zl0) zl0 += ro, zl1 += ro;
     uk_dc += blockIdx.y * kRunWordStride;
-    const size_t n = box ? g.box_elems() : g.field_elems_c();
-    for (size_t bi = blockIdx.x * (size_t)blockDim.x + threadIdx.x; bi < n; bi += (size_t)gridDim.x * blockDim.x) {
-        const size_t idx = box ? g.box_index(bi) : bi;
-        KPoint p;
-        size_t row;
-        if (!k_point(g, idx, p, row) || !p.keep || idx == 0) {
+    for_modes<BOX>(g, [&](size_t idx, const KPoint &p, bool valid) {
+        if (!valid || !p.keep || idx == 0) {
             if (idx == 0) {
                 uk_dc[0] += (double)f0p[0].re;
                 uk_dc[1] += (double)f1p[0].re;
@@ -384,7 +427,7 @@ __global__ void k_project_add_curl(Grid g, const cplx<T> *__restrict__ f0p, cons
             }
             z0p[idx] = z1p[idx] = cplx<T>{0, 0};
             if (zl0) zl0[idx] = zl1[idx] = cplx<T>{0, 0};
-            continue;
+            return;
         }
         const T kx = (T)p.kx, ky = (T)p.ky, kz = (T)p.kz, ik2 = ik2_of<T>(p);
         cplx<T> f[3] = {f0p[idx], f1p[idx], f2p[idx]};
@@ -411,7 +454,7 @@ __global__ void k_project_add_curl(Grid g, const cplx<T> *__restrict__ f0p, cons
             z1p[idx] = z1;
             zl0[idx] = l0;
             zl1[idx] = l1;
-            continue;
+            return;
         }
         zeta_to_omega<T>(p, z0p[idx], z1p[idx], om);
         i_cross<T>(kx * ik2, ky * ik2, kz * ik2, om, u);
@@ -422,7 +465,7 @@ __global__ void k_project_add_curl(Grid g, const cplx<T> *__restrict__ f0p, cons
         omega_to_zeta<T>(p, om, a, b);
         z0p[idx] = a;
         z1p[idx] = b;
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -566,6 +609,8 @@ __global__ void s_up_scatter(Grid g, Phys ph, const double *__restrict__ x, cons
     atomicAdd(&up2[s.idx], (T)(vs[2] * wgt));
 }
 
+
+
 // Block-wide sum of 6 doubles (blockDim.x a multiple of 32, <= 1024).
 __device__ __forceinline__ void block_sum6(double v[6]) {
     __shared__ double red[32][6];
@@ -639,6 +684,132 @@ __global__ void s_hydro_force(Grid g, Phys ph, const double *__restrict__ x, con
         if (ph.rotation)
             for (int d = 0; d < 3; d++) torque_hydro[3 * p + d] = dmy * acc[3 + d];
     }
+}
+
+// ---------------------------------------------------------------------------
+// Stencil cache of the step.  The phi scatter evaluates, for every (particle,
+// Sekibun cell), the grid index and the profile weight Phi; the hydrodynamic
+// force and the phi*v_p scatter of the same step (same positions) read them
+// back instead of recomputing the minimum-image distance and the profile.
+// sc_idx[p * ncells + m] = -1 where Phi is zero (or the particle is outside
+// the box).  Offsets r = cell * dx - residue are rebuilt from the cell.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void particle_residue(const Grid &g, const double xp[3], double res[3]) {
+    const double idx = 1.0 / g.dx;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double dmy = xp[d] * idx;
+        res[d]           = (dmy - (double)(int)dmy) * g.dx;
+    }
+}
+__device__ __forceinline__ void cell_offset(const Grid &g, int cell_packed, const double res[3], double r[3]) {
+    const int c[3] = {(int)(int8_t)(cell_packed & 0xff), (int)(int8_t)((cell_packed >> 8) & 0xff),
+                      (int)(int8_t)((cell_packed >> 16) & 0xff)};
+#pragma unroll
+    for (int d = 0; d < 3; d++) r[d] = (double)c[d] * g.dx - res[d];
+}
+
+template <typename T>
+__global__ void s_phi_scatter_cache(Grid g, Phys ph, const double *__restrict__ x, const int *__restrict__ cells,
+                                    int ncells, T *__restrict__ phi_sum, unsigned int *err, int *__restrict__ sc_idx,
+                                    double *__restrict__ sc_w) {
+    const int p = blockIdx.y;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ph.np || m >= ncells) return;
+    const size_t o     = (size_t)p * ncells + m;
+    const double xp[3] = {x[3 * p], x[3 * p + 1], x[3 * p + 2]};
+    if (!particle_in_box(ph, xp)) {
+        if (m == 0) atomicOr(err, (unsigned)SPM_DEVERR_PARTICLE_OUT_OF_BOX);
+        sc_idx[o] = -1;
+        return;
+    }
+    StencilPoint s;
+    stencil_point(g, ph, xp, cells[m], s);
+    const double v = phi_prof(s.dist, ph.radius, ph.hxi, g.dx);
+    sc_idx[o]      = v != 0.0 ? (int)s.idx : -1;
+    sc_w[o]        = v;
+    if (v != 0.0) atomicAdd(&phi_sum[s.idx], (T)v);
+}
+
+// Calc_f_hydro_correct_precision from the stencil cache (same sums as
+// s_hydro_force).
+template <typename T>
+__global__ void s_hydro_force_cached(Grid g, Phys ph, const double *__restrict__ x, const double *__restrict__ v,
+                                     const double *__restrict__ w, const int *__restrict__ cells, int ncells,
+                                     const int *__restrict__ sc_idx, const double *__restrict__ sc_w,
+                                     const T *__restrict__ phi_sum, const T *__restrict__ u0,
+                                     const T *__restrict__ u1, const T *__restrict__ u2, double *__restrict__ f_hydro,
+                                     double *__restrict__ torque_hydro) {
+    const int p = blockIdx.x;
+    if (p >= ph.np) return;
+    const double xp[3] = {x[3 * p], x[3 * p + 1], x[3 * p + 2]};
+    const double vp[3] = {v[3 * p], v[3 * p + 1], v[3 * p + 2]};
+    const double op[3] = {w[3 * p], w[3 * p + 1], w[3 * p + 2]};
+    double       res[3];
+    particle_residue(g, xp, res);
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int m = threadIdx.x; m < ncells; m += blockDim.x) {
+        const size_t o  = (size_t)p * ncells + m;
+        const int    id = sc_idx[o];
+        if (id < 0) continue;
+        double r[3];
+        cell_offset(g, cells[m], res, r);
+        const double ps  = (double)phi_sum[id];
+        const double wgt = sc_w[o] / (ps > 1.0 ? ps : 1.0);
+        double       vs[3] = {vp[0], vp[1], vp[2]};
+        if (ph.rotation) {
+            vs[0] += op[1] * r[2] - op[2] * r[1];
+            vs[1] += op[2] * r[0] - op[0] * r[2];
+            vs[2] += op[0] * r[1] - op[1] * r[0];
+        }
+        const double fp0 = (vs[0] - (double)u0[id]) * wgt;
+        const double fp1 = (vs[1] - (double)u1[id]) * wgt;
+        const double fp2 = (vs[2] - (double)u2[id]) * wgt;
+        acc[0] += fp0;
+        acc[1] += fp1;
+        acc[2] += fp2;
+        acc[3] += r[1] * fp2 - r[2] * fp1;
+        acc[4] += r[2] * fp0 - r[0] * fp2;
+        acc[5] += r[0] * fp1 - r[1] * fp0;
+    }
+    block_sum6(acc);
+    if (threadIdx.x == 0) {
+        const double dmy = -ph.dx3 * ph.rho / ph.dt;
+        for (int d = 0; d < 3; d++) f_hydro[3 * p + d] = dmy * acc[d];
+        if (ph.rotation)
+            for (int d = 0; d < 3; d++) torque_hydro[3 * p + d] = dmy * acc[3 + d];
+    }
+}
+
+// Make_u_particle_sum from the stencil cache (same terms as s_up_scatter).
+template <typename T>
+__global__ void s_up_scatter_cached(Grid g, Phys ph, const double *__restrict__ x, const double *__restrict__ v,
+                                    const double *__restrict__ w, const int *__restrict__ cells, int ncells,
+                                    const int *__restrict__ sc_idx, const double *__restrict__ sc_w,
+                                    const T *__restrict__ phi_sum, T *__restrict__ up0, T *__restrict__ up1,
+                                    T *__restrict__ up2) {
+    const int p = blockIdx.y;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ph.np || m >= ncells) return;
+    const size_t o  = (size_t)p * ncells + m;
+    const int    id = sc_idx[o];
+    if (id < 0) return;
+    const double xp[3] = {x[3 * p], x[3 * p + 1], x[3 * p + 2]};
+    double       res[3], r[3];
+    particle_residue(g, xp, res);
+    cell_offset(g, cells[m], res, r);
+    const double ps  = (double)phi_sum[id];
+    const double wgt = sc_w[o] / (ps > 1.0 ? ps : 1.0);
+    double       vs[3] = {v[3 * p], v[3 * p + 1], v[3 * p + 2]};
+    if (ph.rotation) {
+        const double *om = w + 3 * p;
+        vs[0] += om[1] * r[2] - om[2] * r[1];
+        vs[1] += om[2] * r[0] - om[0] * r[2];
+        vs[2] += om[0] * r[1] - om[1] * r[0];
+    }
+    atomicAdd(&up0[id], (T)(vs[0] * wgt));
+    atomicAdd(&up1[id], (T)(vs[1] * wgt));
+    atomicAdd(&up2[id], (T)(vs[2] * wgt));
 }
 
 // ---------------------------------------------------------------------------
