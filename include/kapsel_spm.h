@@ -122,6 +122,15 @@ int spm_get_time(spm_ctx *ctx, int *ts, double *time);
  * apparent}.  For a Lees-Edwards run spm_get_velocity returns the oblique
  * (contravariant) velocity on the sheared grid. */
 int spm_get_shear_state(spm_ctx *ctx, double *degree_oblique, double stress[8]);
+/* Checkpoint / restart (the reference's restart files, resume.cxx:10-74,
+ * 381-588): writes, or reads back into a context created with the same
+ * parameters, every piece of device state the next steps read (zeta with its
+ * FP32 compensation words, uk_dc, the step counter, the particle buffer, the
+ * MT19937 state, Lees-Edwards scalars) plus ts, time and degree_oblique, so
+ * a restored run continues as the saved one would have.  The file format is
+ * this library's own (binary, host byte order). */
+int spm_save_state(spm_ctx *ctx, const char *path);
+int spm_load_state(spm_ctx *ctx, const char *path);
 
 /* ---- reference solver boundaries (host arrays, reference layout) -------- */
 /* NS_solver_slavedEuler (fluid_solver.h:77-82, fluid_solver.cxx:348-374):
@@ -230,6 +239,10 @@ int spm_pool_stats(spm_pool *pool, long long *graph_kernels, int *captures);
 /* Host-side fault injection: the next `count` device allocations of contexts
  * and pools fail with SPM_ERR_NOMEM (0 switches it off). */
 int spm_debug_fail_allocations(int count);
+/* Device blocks of up to 64 MB that destroyed contexts and pools freed are
+ * kept for reuse (at most 2 GB per process), because cudaFree waits for the
+ * whole device.  This returns them all to the driver; bytes = what was held. */
+int spm_release_cached_memory(size_t *bytes);
 
 /* ---- serving loop (no reference counterpart) -----------------------------
  * A persistent worker thread admits submitted Navier_Stokes runs by device-
@@ -253,6 +266,7 @@ typedef struct spm_server_config {
     int    steps_per_launch;    /* steps enqueued per pool launch (1: per-step latency) */
     int    poll_us;             /* worker sleep when nothing progressed */
     int    device;              /* CUDA device index */
+    double pool_idle_s;         /* an empty pool keeps its arena this long, unless a request waits */
 } spm_server_config;
 typedef struct spm_server_stats {
     long long submitted, rejected, admitted, completed, failed, cancelled, queued;

@@ -51,6 +51,7 @@ class SpmServerConfig(C.Structure):
         ("steps_per_launch", C.c_int),
         ("poll_us", C.c_int),
         ("device", C.c_int),
+        ("pool_idle_s", C.c_double),
     ]
 
 
@@ -101,6 +102,8 @@ _SIGS = {
     "spm_get_phi": (C.c_int, [_P, _D]),
     "spm_get_time": (C.c_int, [_P, C.POINTER(C.c_int), _D]),
     "spm_get_shear_state": (C.c_int, [_P, _D, _D]),
+    "spm_save_state": (C.c_int, [_P, C.c_char_p]),
+    "spm_load_state": (C.c_int, [_P, C.c_char_p]),
     "spm_ns_solver_slaved_euler_host": (C.c_int, [_P, _D, _D, _D]),
     "spm_solenoidal_uk_host": (C.c_int, [_P, _D, _D, _D]),
     "spm_zeta_k2u_k_host": (C.c_int, [_P, _D, _D, _D, _D, _D, _D]),
@@ -134,6 +137,7 @@ _SIGS = {
     "spm_pool_synchronize": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_uint)]),
     "spm_pool_stats": (C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
     "spm_debug_fail_allocations": (C.c_int, [C.c_int]),
+    "spm_release_cached_memory": (C.c_int, [C.POINTER(C.c_size_t)]),
     "spm_server_config_default": (C.c_int, [C.POINTER(SpmServerConfig)]),
     "spm_server_create": (C.c_int, [C.POINTER(SpmServerConfig), C.POINTER(_P)]),
     "spm_server_destroy": (C.c_int, [_P]),

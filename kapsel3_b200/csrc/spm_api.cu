@@ -2,6 +2,8 @@
 // device-resident state, and the reference-boundary entry points.
 #include <atomic>
 #include <cstdlib>
+#include <mutex>
+#include <unordered_map>
 #include <cstring>
 #include <fstream>
 #include <map>
@@ -32,16 +34,78 @@ namespace {
 // told to fail the next n calls (host-side fault injection for the serving
 // tests; spm_debug_fail_allocations).
 std::atomic<int> g_fail_allocs{0};
-cudaError_t      dev_alloc(void **p, size_t bytes) {
+
+// Small device blocks freed by contexts are kept for reuse instead of being
+// returned with cudaFree, which waits for the whole device: a serving loop
+// that retires and admits runs continuously would otherwise stall every
+// pool in flight at each retirement.  Blocks up to kCacheBlock bytes (sizes
+// rounded up to an eighth of their octave) are kept per device, at most
+// kCacheTotal bytes in all; a block is only cached after its owner's stream
+// was synchronised (destroy_ctx, pool release), so no work still uses it.
+constexpr size_t kCacheBlock = (size_t)64 << 20;
+constexpr size_t kCacheTotal = (size_t)2 << 30;
+struct BlockCache {
+    std::mutex                                           mu;
+    std::unordered_map<void *, std::pair<size_t, int>>   live;  // block -> (bytes, device)
+    std::multimap<std::pair<int, size_t>, void *>        idle;  // (device, bytes) -> block
+    size_t                                               idle_bytes = 0;
+};
+BlockCache &block_cache() {
+    static BlockCache c;
+    return c;
+}
+size_t round_block(size_t b) {
+    if (b <= 4096) return 4096;
+    int lg = 63 - __builtin_clzll((unsigned long long)b);
+    const size_t granule = (size_t)1 << (lg - 3);
+    return (b + granule - 1) / granule * granule;
+}
+
+cudaError_t dev_alloc(void **p, size_t bytes) {
     for (int n = g_fail_allocs.load(); n > 0; n = g_fail_allocs.load())
         if (g_fail_allocs.compare_exchange_weak(n, n - 1)) {
             *p = nullptr;
             return cudaErrorMemoryAllocation;
         }
-    return cudaMalloc(p, bytes);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t rb = bytes <= kCacheBlock ? round_block(bytes) : bytes;
+    BlockCache  &bc = block_cache();
+    {
+        std::lock_guard<std::mutex> lk(bc.mu);
+        auto it = bc.idle.find({dev, rb});
+        if (it != bc.idle.end()) {
+            *p = it->second;
+            bc.idle.erase(it);
+            bc.idle_bytes -= rb;
+            bc.live[*p] = {rb, dev};
+            return cudaSuccess;
+        }
+    }
+    cudaError_t e = cudaMalloc(p, rb);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(bc.mu);
+    bc.live[*p] = {rb, dev};
+    return cudaSuccess;
 }
 void dev_free(void *p) {
-    if (p) cudaFree(p);
+    if (!p) return;
+    BlockCache &bc = block_cache();
+    {
+        std::lock_guard<std::mutex> lk(bc.mu);
+        auto it = bc.live.find(p);
+        if (it != bc.live.end()) {
+            const size_t b = it->second.first;
+            const int    d = it->second.second;
+            bc.live.erase(it);
+            if (b <= kCacheBlock && bc.idle_bytes + b <= kCacheTotal) {
+                bc.idle.insert({{d, b}, p});
+                bc.idle_bytes += b;
+                return;
+            }
+        }
+    }
+    cudaFree(p);
 }
 }  // namespace
 
@@ -1160,3 +1224,4 @@ int spm_kernel_launches(spm_ctx *c, long long *count, int reset) {
 
 #include "spm_api_boundary.inc"
 #include "spm_pool.inc"
+#include "spm_checkpoint.inc"

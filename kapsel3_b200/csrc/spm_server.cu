@@ -63,6 +63,7 @@ struct PoolEntry {
     bool                   inflight = false;
     int                    steps_inflight = 0;
     double                 t_launch = 0.0;
+    double                 t_empty  = 0.0;  // when the pool last became empty (0: has members)
 };
 
 bool same_key(const spm_params &a, const spm_params &b) {
@@ -345,10 +346,21 @@ void spm_server::loop() {
                 if (q->cancel) retire(pe.get(), q, SPM_REQ_CANCELLED, SPM_OK, "cancelled");
         }
         if (admit_some()) progressed = true;
-        // drop empty pools (frees their arenas for other grid sizes)
+        // Drop pools that stayed empty for pool_idle_s, or at once when a
+        // queued request is waiting: freeing an arena waits for the whole
+        // device, so a pool that empties and refills within a moment keeps it.
+        bool waiting = false;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            waiting = !queue.empty();
+        }
+        const double tnow = now_s();
         for (size_t i = 0; i < pools.size();) {
             PoolEntry *pe = pools[i].get();
-            if (pe->members.empty() && !pe->inflight) {
+            if (!pe->members.empty()) pe->t_empty = 0.0;
+            if (pe->members.empty() && !pe->inflight && pe->t_empty == 0.0) pe->t_empty = tnow;
+            const bool idle_long = pe->t_empty > 0.0 && tnow - pe->t_empty >= cfg.pool_idle_s;
+            if (pe->members.empty() && !pe->inflight && (idle_long || waiting || stop)) {
                 long long k = 0;
                 int       cnt = 0;
                 spm_pool_stats(pe->pool, &k, &cnt);
@@ -395,6 +407,7 @@ int spm_server_config_default(spm_server_config *c) {
     c->use_graph             = 1;
     c->steps_per_launch      = 1;
     c->poll_us               = 20;
+    c->pool_idle_s           = 2.0;
     c->device                = 0;
     return SPM_OK;
 }

@@ -194,6 +194,14 @@ class SPMRun:
         N.check(self.L.spm_get_shear_state(self.h, C.byref(deg), N.dptr(st)), "spm_get_shear_state")
         return deg.value, st
 
+    def save_state(self, path: str):
+        """Checkpoint of the device state (spm_save_state)."""
+        N.check(self.L.spm_save_state(self.h, path.encode()), "spm_save_state")
+
+    def load_state(self, path: str):
+        """Restores a checkpoint written by a run with the same parameters."""
+        N.check(self.L.spm_load_state(self.h, path.encode()), "spm_load_state")
+
     def kernel_launches(self, reset: bool = False) -> int:
         n = C.c_longlong()
         N.check(self.L.spm_kernel_launches(self.h, C.byref(n), 1 if reset else 0), "spm_kernel_launches")

@@ -1,0 +1,86 @@
+"""Checkpoint / restart of device state (spm_save_state / spm_load_state).
+
+A run saved after n1 steps and restored into a fresh context continues like
+the original: after n2 more steps the particle state and zeta agree within
+1e-12 relative (the shared-profile scatters use float atomics, whose order
+may differ where three or more profiles overlap a cell).  Covered: FP64
+Navier_Stokes with the thermostat (MT19937 state), FP32-mixed (compensated
+zeta words) and Lees-Edwards (degree_oblique and its device scalars).  A
+checkpoint is refused by a context with other parameters, and a truncated
+file is refused."""
+import os
+
+import numpy as np
+import pytest
+
+from kapsel3_b200 import _native as N
+from kapsel3_b200.spm import SPMRun
+from kapsel3_b200.udf import EQ_LE, SPMConfig, make_particles
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+CASES = {
+    "ns_fp64_thermostat": (SPMConfig(npx=5, npy=5, npz=5, n_particles=4, a=4.0, a_xi=2.0, dt=0.05, kbt=1e-4),
+                           N.SPM_PREC_FP64),
+    "ns_fp32_mixed": (SPMConfig(npx=5, npy=5, npz=5, n_particles=3, a=4.0, a_xi=2.0, dt=0.05,
+                                body_force=(1e-3, 0.0, 0.0)), N.SPM_PREC_FP32_MIXED),
+    "lees_edwards_fp64": (SPMConfig(npx=5, npy=5, npz=5, n_particles=3, a=3.5, a_xi=2.0, dt=0.05, equation=EQ_LE,
+                                    shear_rate=0.3, kbt=1e-5), N.SPM_PREC_FP64),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_restored_run_continues_like_the_original(gpu, name, tmp_path):
+    cfg, prec = CASES[name]
+    parts = make_particles(cfg, seed=31, v_sd=1e-3, random_orientation=True)
+    path = os.path.join(tmp_path, "run.ck")
+    with SPMRun(cfg, precision=prec) as a:
+        a.initialize(parts)
+        a.step(7)
+        a.save_state(path)
+        a.step(6)
+        pa, (za, dca), ta = a.particles(), a.zeta(), a.time()
+        sa = a.shear_state() if cfg.equation == EQ_LE else None
+    with SPMRun(cfg, precision=prec) as b:
+        b.load_state(path)
+        assert b.time()[0] == 7
+        b.step(6)
+        pb, (zb, dcb), tb = b.particles(), b.zeta(), b.time()
+        sb = b.shear_state() if cfg.equation == EQ_LE else None
+    assert ta == tb
+    for k in ("x", "v", "omega", "q", "f_hydro_previous"):
+        assert rel(pb[k], pa[k]) <= TOL, (name, k)
+    assert rel(zb, za) <= TOL and rel(dcb, dca) <= TOL
+    if sa is not None:
+        assert sb[0] == sa[0]
+        assert rel(sb[1], sa[1]) <= TOL
+
+
+def test_checkpoint_is_refused_by_another_run(gpu, tmp_path):
+    cfg, prec = CASES["ns_fp64_thermostat"]
+    parts = make_particles(cfg, seed=3)
+    path = os.path.join(tmp_path, "run.ck")
+    with SPMRun(cfg, precision=prec) as a:
+        a.initialize(parts)
+        a.step(2)
+        a.save_state(path)
+    other = SPMConfig(npx=5, npy=5, npz=5, n_particles=4, a=4.0, a_xi=2.0, dt=0.04, kbt=1e-4)
+    with SPMRun(other, precision=prec) as b:
+        with pytest.raises(N.SpmError):
+            b.load_state(path)
+    with SPMRun(cfg, precision=N.SPM_PREC_FP32_MIXED) as b:
+        with pytest.raises(N.SpmError):
+            b.load_state(path)
+    data = open(path, "rb").read()
+    short = os.path.join(tmp_path, "short.ck")
+    open(short, "wb").write(data[: len(data) // 2])
+    with SPMRun(cfg, precision=prec) as b:
+        with pytest.raises(N.SpmError, match="truncated"):
+            b.load_state(short)
