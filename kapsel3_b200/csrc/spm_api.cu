@@ -546,15 +546,14 @@ int clear_scatter_slots(spm_ctx *L) {
     return SPM_OK;
 }
 
-// Rigidity projection of the step: f = up - phi u formed inside the forward z
-// pass, forward y, x passes, then the projection and the update of zeta and
-// uk_dc closed in k space (k_project_add_curl).
+// Rigidity projection of the step: the forward transform of f (scattered by
+// s_f_scatter_cached, or up itself when u = 0 at initialisation), then the
+// projection and the update of zeta and uk_dc closed in k space
+// (k_project_add_curl).
 template <typename T>
 int rigidity_projection(spm_ctx *L) {
     int rc;
-    SPM_CUDA_CHECK(plan_of<T>(L).z_makef(L->real<T>(UP0), L->real<T>(U0), L->real<T>(PHIS), L->slot_stride_c,
-                                         L->fft_runs, L->fstride_c, L->st, L->g.kz_span()));
-    L->launches++;
+    if ((rc = z_pass<T>(L, UP0, 3, true)) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 1, prune_forward(L->g, 1))) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 0, prune_forward(L->g, 0))) != SPM_OK) return rc;
     LAUNCH(L, (k_project_add_curl<T, 2>), L->box_grid(), 256, 0, L->g, L->cx<T>(UP0), L->cx<T>(UP1), L->cx<T>(UP2),
@@ -631,9 +630,9 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
         if (c->P.kbt > 0.0) LAUNCH(c, p_thermostat_serial, 1, 32, 0, c->ph, c->ps, c->mt);
         {
             const dim3 sgrid((c->ncells + 127) / 128, c->ph.np);
-            LAUNCH(c, s_up_scatter_cached<T>, sgrid, 128, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
-                   c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS), c->real<T>(UP0), c->real<T>(UP1),
-                   c->real<T>(UP2));
+            LAUNCH(c, s_f_scatter_cached<T>, sgrid, 128, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
+                   c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS), c->real<T>(U0), c->real<T>(U1),
+                   c->real<T>(U2), c->real<T>(UP0), c->real<T>(UP1), c->real<T>(UP2));
         }
     }
     if ((rc = rigidity_projection<T>(L)) != SPM_OK) return rc;

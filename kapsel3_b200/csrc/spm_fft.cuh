@@ -534,48 +534,4 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
     }
 }
 
-// ---------------------------------------------------------------------------
-// Fused Z pass of the rigidity force (Make_f_particle_dt_nonsole,
-// f_particle.h:35-54): f = up - min(phi_sum, 1) u formed on the fly and
-// transformed forward.  up[0..2] (real rows) are overwritten by f_hat rows
-// for kz < kz_span.
-// ---------------------------------------------------------------------------
-template <typename T, int M, int R>
-__global__ void __launch_bounds__(R *Split<M>::N1)
-    fft_z_makef_kernel(T *up, const T *__restrict__ u, const T *__restrict__ phi_sum, size_t field_stride_c,
-                       size_t run_stride_c, int nrows, int hnzp, const cplx<T> *__restrict__ twM,
-                       const cplx<T> *__restrict__ twN, int kz_span) {
-    constexpr int P = Split<M>::N1;
-    up += (size_t)blockIdx.y * 2 * run_stride_c;  // run of a batched pool
-    u += (size_t)blockIdx.y * 2 * run_stride_c;
-    phi_sum += (size_t)blockIdx.y * 2 * run_stride_c;
-    __shared__ __align__(16) cplx<T> s[R][ws_len<T, M>()];
-    const int r   = threadIdx.x / P;
-    const int t   = threadIdx.x % P;
-    const int row = blockIdx.x * R + r;
-    const bool ok = row < nrows;
-    const size_t roff = (size_t)(ok ? row : 0) * 2 * hnzp;
-    const T *ph = phi_sum + roff;
-#pragma unroll 1
-    for (int d = 0; d < 3; d++) {
-        T       *upr = up + 2 * d * field_stride_c + roff;
-        const T *ur  = u + 2 * d * field_stride_c + roff;
-        cplx<T> *out = reinterpret_cast<cplx<T> *>(upr);
-        r2c_row<T, M>(
-            t,
-            [&](int n) {
-                if (!ok) return cplx<T>{0, 0};
-                const cplx<T> a = load_pair<T>(upr, n), b = load_pair<T>(ur, n), f = load_pair<T>(ph, n);
-                const T       f0 = f.re < (T)1 ? f.re : (T)1, f1 = f.im < (T)1 ? f.im : (T)1;
-                return cplx<T>{a.re - f0 * b.re, a.im - f1 * b.im};
-            },
-            s[r], twM, twN,
-            [&](int k, cplx<T> X) {
-                if (ok && k < kz_span) out[k] = X;
-            });
-        if (ok && kz_span > M)
-            for (int k = M + 1 + t; k < hnzp; k += P) out[k] = cplx<T>{0, 0};
-    }
-}
-
 }  // namespace spm

@@ -67,23 +67,6 @@ struct FFTPlan {
         }
         return cudaGetLastError();
     }
-    // Fused f = up - min(phi_sum,1) u and forward z pass (three fields).
-    cudaError_t z_makef(T *up, const T *u, const T *phis, size_t fs_c, int nruns, size_t run_stride_c,
-                        cudaStream_t st, int kz_span) const {
-        const int nrows = g.nx * g.ny;
-        switch (g.nz / 2) {
-#define SPM_ZF(MM)                                                                                         \
-    case MM: {                                                                                             \
-        constexpr int RR = zrows(MM);                                                                      \
-        fft_z_makef_kernel<T, MM, RR><<<dim3((nrows + RR - 1) / RR, nruns), RR * Split<MM>::N1, 0, st>>>( \
-            up, u, phis, fs_c, run_stride_c, nrows, g.hnzp, tw_zm, tw_zn, kz_span);                        \
-    } break;
-            SPM_ZF(4) SPM_ZF(8) SPM_ZF(16) SPM_ZF(32) SPM_ZF(64) SPM_ZF(128) SPM_ZF(256)
-#undef SPM_ZF
-            default: return cudaErrorInvalidValue;
-        }
-        return cudaGetLastError();
-    }
 
     cudaError_t create(const Grid &grid) {
         g = grid;

@@ -781,13 +781,20 @@ __global__ void s_hydro_force_cached(Grid g, Phys ph, const double *__restrict__
     }
 }
 
-// Make_u_particle_sum from the stencil cache (same terms as s_up_scatter).
+// The rigidity force f = up - min(phi_sum, 1) u (Make_f_particle_dt_nonsole,
+// f_particle.h:35-54) scattered directly from the stencil cache.  With w_p =
+// Phi_p / max(phi_sum, 1): up = sum_p w_p (v_p + omega_p x r) and
+// min(phi_sum, 1) = sum_p w_p, so f = sum_p w_p (v_p + omega_p x r - u), the
+// integrand of the hydrodynamic force.  f is zero wherever no profile
+// reaches, so the forward z pass of f reads three fields instead of the
+// seven (up, u, phi) of forming f on the fly.
 template <typename T>
-__global__ void s_up_scatter_cached(Grid g, Phys ph, const double *__restrict__ x, const double *__restrict__ v,
-                                    const double *__restrict__ w, const int *__restrict__ cells, int ncells,
-                                    const int *__restrict__ sc_idx, const double *__restrict__ sc_w,
-                                    const T *__restrict__ phi_sum, T *__restrict__ up0, T *__restrict__ up1,
-                                    T *__restrict__ up2) {
+__global__ void s_f_scatter_cached(Grid g, Phys ph, const double *__restrict__ x, const double *__restrict__ v,
+                                   const double *__restrict__ w, const int *__restrict__ cells, int ncells,
+                                   const int *__restrict__ sc_idx, const double *__restrict__ sc_w,
+                                   const T *__restrict__ phi_sum, const T *__restrict__ u0, const T *__restrict__ u1,
+                                   const T *__restrict__ u2, T *__restrict__ f0, T *__restrict__ f1,
+                                   T *__restrict__ f2) {
     const int p = blockIdx.y;
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= ph.np || m >= ncells) return;
@@ -807,9 +814,9 @@ __global__ void s_up_scatter_cached(Grid g, Phys ph, const double *__restrict__ 
         vs[1] += om[2] * r[0] - om[0] * r[2];
         vs[2] += om[0] * r[1] - om[1] * r[0];
     }
-    atomicAdd(&up0[id], (T)(vs[0] * wgt));
-    atomicAdd(&up1[id], (T)(vs[1] * wgt));
-    atomicAdd(&up2[id], (T)(vs[2] * wgt));
+    atomicAdd(&f0[id], (T)((vs[0] - (double)u0[id]) * wgt));
+    atomicAdd(&f1[id], (T)((vs[1] - (double)u1[id]) * wgt));
+    atomicAdd(&f2[id], (T)((vs[2] - (double)u2[id]) * wgt));
 }
 
 // ---------------------------------------------------------------------------
