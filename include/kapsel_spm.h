@@ -87,6 +87,18 @@ int spm_params_default(spm_params *p);
  * Gourmet_file_io) into p; particle initial state goes to the optional
  * host record array (n_particles records, may be NULL). */
 int spm_params_from_udf_keys(const char *path, spm_params *p, double *particles_out, int max_particles);
+/* Reads a UDF input file in the OCTA UDF format the reference reads
+ * through UDFManager (Gourmet_file_io, input.cxx:677-2556): the schema from
+ * its \begin{def}/\begin{global_def} blocks and \include'd files (the
+ * reference's define.udf), the values from its \begin{data} block.  Same
+ * parameters, particle records and errors as spm_params_from_udf_keys. */
+int spm_params_from_udf(const char *path, spm_params *p, double *particles_out, int max_particles);
+/* The \begin{data} values of a UDF file flattened to "<udf.path>=<value>\n"
+ * lines (paths as the reference's Location strings name them, e.g.
+ * "object_type.spherical_particle.Particle_spec[0].Particle_number").
+ * *needed receives the text size including the terminating NUL; out is
+ * filled only when capacity >= *needed (out may be NULL to query). */
+int spm_udf_read_keys(const char *path, char *out, size_t capacity, size_t *needed);
 /* Allocates all device state for one run on the current device.
  * `stream` is a cudaStream_t (NULL: a new non-blocking stream). */
 int spm_create(const spm_params *p, void *stream, spm_ctx **out);

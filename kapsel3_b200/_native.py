@@ -88,6 +88,8 @@ _SIGS = {
     "spm_device_count": (C.c_int, [C.POINTER(C.c_int)]),
     "spm_params_default": (C.c_int, [C.POINTER(SpmParams)]),
     "spm_params_from_udf_keys": (C.c_int, [C.c_char_p, C.POINTER(SpmParams), _D, C.c_int]),
+    "spm_params_from_udf": (C.c_int, [C.c_char_p, C.POINTER(SpmParams), _D, C.c_int]),
+    "spm_udf_read_keys": (C.c_int, [C.c_char_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "spm_create": (C.c_int, [C.POINTER(SpmParams), _P, C.POINTER(_P)]),
     "spm_destroy": (C.c_int, [_P]),
     "spm_device_bytes": (C.c_int, [C.POINTER(SpmParams), C.POINTER(C.c_size_t)]),

@@ -1,12 +1,14 @@
 // C ABI of the B200 SPM step: context management, the whole step on
 // device-resident state, and the reference-boundary entry points.
 #include <atomic>
+#include <cctype>
 #include <cstdlib>
 #include <mutex>
 #include <unordered_map>
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <memory>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -1221,6 +1223,7 @@ int spm_kernel_launches(spm_ctx *c, long long *count, int reset) {
 
 }  // extern "C"
 
+#include "spm_udf.inc"
 #include "spm_api_boundary.inc"
 #include "spm_pool.inc"
 #include "spm_checkpoint.inc"

@@ -14,7 +14,7 @@ Errors raise `SpmError` with the library's message (the reference exits).
 from __future__ import annotations
 
 import ctypes as C
-from typing import Dict, Optional
+from typing import Dict, Optional, Tuple
 
 import numpy as np
 
@@ -74,6 +74,41 @@ def params_from_config(cfg: SPMConfig, precision: int = N.SPM_PREC_FP64,
     p.precision = precision
     p.mt_seed = mt_seed
     return p
+
+
+def read_udf(path: str) -> Dict[str, str]:
+    """The data of a UDF input file (KAPSEL's input.udf format, schema from
+    its \\include'd define.udf) flattened to {udf.path: value}."""
+    L = N.lib()
+    need = C.c_size_t()
+    N.check(L.spm_udf_read_keys(path.encode(), None, 0, C.byref(need)), "spm_udf_read_keys")
+    buf = C.create_string_buffer(need.value)
+    N.check(L.spm_udf_read_keys(path.encode(), buf, need.value, C.byref(need)), "spm_udf_read_keys")
+    return dict(line.split("=", 1) for line in buf.value.decode().splitlines())
+
+
+def config_from_udf(path: str) -> Tuple[SPMConfig, Dict[str, np.ndarray]]:
+    """Run parameters and initial particles of a UDF input file, as
+    Gourmet_file_io and Init_Particle read them (user_specify or
+    uniform_random placement; user_specify, random or space_align
+    orientation)."""
+    L = N.lib()
+    p = N.SpmParams()
+    N.check(L.spm_params_from_udf(path.encode(), C.byref(p), None, 0), "spm_params_from_udf")
+    rec = np.zeros((max(p.n_particles, 1), N.SPM_PARTICLE_WORDS))
+    N.check(L.spm_params_from_udf(path.encode(), C.byref(p), N.dptr(rec), p.n_particles), "spm_params_from_udf")
+    kv = read_udf(path)
+    cfg = SPMConfig(
+        npx=p.npx, npy=p.npy, npz=p.npz, dx=p.dx, rho=p.rho, eta=p.eta, kbt=p.kbt,
+        alpha_v=p.alpha_v, alpha_o=p.alpha_o,
+        equation=EQ_LE if p.equation == N.SPM_EQ_LEES_EDWARDS else "Navier_Stokes",
+        shear_rate=p.shear_rate, n_particles=p.n_particles, mass_ratio=p.mass_ratio, a=p.a, a_xi=p.a_xi,
+        epsilon=p.epsilon, lj_powers=("12:6", "24:12", "36:18")[p.lj_powers],
+        lj_truncate={1: "ON", 0: "OFF", -1: "NONE"}[p.lj_truncate], rotation=bool(p.rotation),
+        fix_cell=tuple(bool(p.fix_cell[d]) for d in range(3)), dt=p.dt,
+        gts=int(kv.get("output.GTS", 1)), num_snap=int(kv.get("output.Num_snap", 1)),
+        body_force=tuple(float(p.body_force[d]) for d in range(3)))
+    return cfg, unpack_particles(rec[:p.n_particles])
 
 
 class SPMRun:

@@ -19,6 +19,8 @@ from __future__ import annotations
 
 import dataclasses
 import math
+import os
+import re
 from typing import Dict, Optional
 
 import numpy as np
@@ -228,3 +230,105 @@ def read_udf_keys(path: str) -> Dict[str, str]:
             kk, vv = line.split("=", 1)
             out[kk.strip()] = vv.strip()
     return out
+
+
+# ---------------------------------------------------------------------------
+# UDF files in the OCTA format (the format KAPSEL's input.udf uses)
+# ---------------------------------------------------------------------------
+_INT = re.compile(r"[+-]?\d+$")
+
+
+def _leaf_type(v: str) -> str:
+    if _INT.match(v):
+        return "int"
+    try:
+        float(v)
+        return "double"
+    except ValueError:
+        return "string"
+
+
+def _udf_tree(keys: Dict[str, str]) -> dict:
+    """Nests flat UDF paths ("a.b[2].c") into dicts (structs) and lists
+    (arrays), keeping the order in which fields first appear."""
+    root: dict = {}
+    for path, val in keys.items():
+        segs = path.split(".")
+        node = root
+        for n, seg in enumerate(segs):
+            name, *idx = seg.replace("]", "").split("[")
+            last = n == len(segs) - 1
+            if not idx:
+                if last:
+                    node[name] = val
+                else:
+                    node = node.setdefault(name, {})
+                continue
+            arr = node.setdefault(name, [])
+            for m, i in enumerate(int(i) for i in idx):
+                while len(arr) <= i:
+                    arr.append(None)
+                if m < len(idx) - 1:
+                    arr[i] = arr[i] if arr[i] is not None else []
+                    arr = arr[i]
+                elif last:
+                    arr[i] = val
+                else:
+                    arr[i] = arr[i] if arr[i] is not None else {}
+                    node = arr[i]
+    return root
+
+
+def _udf_type(node) -> tuple:
+    """(array depth, type text) of a tree node; arrays take their element
+    type from element 0."""
+    depth = 0
+    while isinstance(node, list):
+        depth += 1
+        node = next((e for e in node if e is not None), "")
+    if isinstance(node, dict):
+        body = " ".join(f"{k}{'[]' * d}: {t}" for k, (d, t) in ((k, _udf_type(v)) for k, v in node.items()))
+        return depth, "{" + body + "}"
+    return depth, _leaf_type(node)
+
+
+def _udf_value(node) -> str:
+    if isinstance(node, list):
+        return "[" + ", ".join(_udf_value(e) for e in node) + "]"
+    if isinstance(node, dict):
+        return "{" + ", ".join(_udf_value(v) for v in node.values()) + "}"
+    return node if _leaf_type(node) != "string" else '"' + node + '"'
+
+
+def udf_text(keys: Dict[str, str]) -> tuple:
+    """(schema, data) text of a self-describing UDF file holding `keys`:
+    a \\begin{def} block declaring every top-level field and a
+    \\begin{data} block with the values in schema order."""
+    tree = _udf_tree(keys)
+    schema = ["\\begin{def}"]
+    data = ["\\begin{data}"]
+    for name, node in tree.items():
+        d, t = _udf_type(node)
+        schema.append(f"{name}{'[]' * d}: {t}")
+        data.append(f"{name}: {_udf_value(node)}")
+    schema.append("\\end{def}")
+    data.append("\\end{data}")
+    return "\n".join(schema) + "\n", "\n".join(data) + "\n"
+
+
+def write_udf(path: str, cfg: SPMConfig, particles: Dict[str, np.ndarray],
+              out_dir: Optional[str] = None, define_path: Optional[str] = None) -> None:
+    """Writes the run as a UDF input file (the paths of `udf_keys`).  With
+    `define_path` the schema goes to that file and the input file
+    \\include's it, as KAPSEL's input.udf includes define.udf."""
+    schema, data = udf_text(udf_keys(cfg, particles, out_dir or "/tmp/kapsel_avs"))
+    with open(path, "w") as f:
+        f.write("// SPM run written by kapsel3_b200.udf.write_udf\n")
+        if define_path:
+            with open(define_path, "w") as g:
+                g.write(schema)
+            rel = os.path.relpath(define_path, os.path.dirname(os.path.abspath(path)))
+            f.write(f'\\include{{"{rel}"}}\n')
+        else:
+            f.write(schema)
+        f.write(data)
