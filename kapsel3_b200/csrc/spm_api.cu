@@ -1,6 +1,10 @@
 // C ABI of the B200 SPM step: context management, the whole step on
 // device-resident state, and the reference-boundary entry points.
 #include <atomic>
+#include <cerrno>
+#include <condition_variable>
+#include <deque>
+#include <thread>
 #include <cctype>
 #include <cstdlib>
 #include <mutex>
@@ -12,6 +16,8 @@
 #include <sstream>
 #include <string>
 #include <vector>
+
+#include <sys/stat.h>
 
 #include "../../include/kapsel_spm.h"
 #include "spm_fft_plan.cuh"
@@ -139,6 +145,7 @@ int slots_for(const spm_params &p) {
 }
 
 struct spm_pool;
+struct AvsOut;
 
 struct spm_ctx {
     spm_params   P{};
@@ -187,6 +194,7 @@ struct spm_ctx {
     bool                     overlap    = true;  // SPM_NO_OVERLAP=1 keeps the particle work on the main stream
     bool                     zeta_dirty = false;  // zeta set by the host since the last NS step
     int                      nslots     = NSLOT;  // field slots of this run (slots_for)
+    AvsOut                  *avs        = nullptr;  // AVS field/particle output (spm_avs_open)
 
     bool fp64() const { return P.precision == SPM_PREC_FP64; }
     // zeta kept as a compensated FP32 pair (FP32-mixed Navier_Stokes)
@@ -434,12 +442,15 @@ template <typename T, int DIR>
 int fft_strided_pass(spm_ctx *c, int slot, int nf, int axis) {
     return fft_strided_pass<T, DIR>(c, slot, nf, axis, PassPrune::full(c->g.hnz));
 }
-// z passes over `nf` slots (one launch per slot when batching runs)
+// z passes over `nf` slots (one launch per slot when batching runs).
+// kz_keep: inverse inputs kz >= kz_keep read as zero; kz_span: forward
+// outputs kz >= kz_span left unwritten (both: pruned transforms).
 template <typename T>
-int z_pass(spm_ctx *c, int slot, int nf, bool forward, int kz_keep = 1 << 30) {
+int z_pass(spm_ctx *c, int slot, int nf, bool forward, int kz_keep = 1 << 30, int kz_span = 1 << 30) {
     const T scale = (T)(1.0 / ((double)c->g.nx * c->g.ny * c->g.nz));
     auto    one   = [&](int s, int nfields, size_t stride) {
-        return forward ? plan_of<T>(c).z_r2c(c->real<T>(s), c->cx<T>(s), nfields, 2 * stride, stride, c->st)
+        return forward ? plan_of<T>(c).z_r2c(c->real<T>(s), c->cx<T>(s), nfields, 2 * stride, stride, c->st,
+                                             kz_span)
                        : plan_of<T>(c).z_c2r(c->cx<T>(s), c->real<T>(s), nfields, stride, 2 * stride, scale, c->st,
                                              kz_keep);
     };
@@ -555,7 +566,7 @@ int clear_scatter_slots(spm_ctx *L) {
 template <typename T>
 int rigidity_projection(spm_ctx *L) {
     int rc;
-    if ((rc = z_pass<T>(L, UP0, 3, true)) != SPM_OK) return rc;
+    if ((rc = z_pass<T>(L, UP0, 3, true, 1 << 30, L->g.kz_span())) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 1, prune_forward(L->g, 1))) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 0, prune_forward(L->g, 0))) != SPM_OK) return rc;
     LAUNCH(L, (k_project_add_curl<T, 2>), L->box_grid(), 256, 0, L->g, L->cx<T>(UP0), L->cx<T>(UP1), L->cx<T>(UP2),
@@ -800,8 +811,11 @@ int download_particles(spm_ctx *c, double *rec) {
     return SPM_OK;
 }
 
+void avs_release(spm_ctx *c);
+
 void destroy_ctx(spm_ctx *c) {
     if (!c) return;
+    avs_release(c);
     if (c->st) cudaStreamSynchronize(c->st);
     c->plan64.destroy();
     c->plan32.destroy();
@@ -1227,3 +1241,4 @@ int spm_kernel_launches(spm_ctx *c, long long *count, int reset) {
 #include "spm_api_boundary.inc"
 #include "spm_pool.inc"
 #include "spm_checkpoint.inc"
+#include "spm_output.inc"

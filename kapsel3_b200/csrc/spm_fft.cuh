@@ -270,6 +270,28 @@ constexpr int ws_len() {
     return row_stride<T, M>(M + 2 + (M + 1) / Split<M>::N1);
 }
 
+// The even/odd split of a length-2M real transform packed as M complex
+// values: X[k] from Z[k], Z[M-k] (forward) and Z'[k] from X[k], X[M-k]
+// (inverse, scaled by c).  w = e^{-2 pi i k / (2M)}.
+template <typename T>
+__device__ __forceinline__ cplx<T> r2c_split(const cplx<T> &zk, const cplx<T> &zmk, const cplx<T> &w) {
+    const T er  = (T)0.5 * (zk.re + zmk.re);
+    const T ei  = (T)0.5 * (zk.im - zmk.im);
+    const T orr = (T)0.5 * (zk.im + zmk.im);
+    const T oi  = (T)-0.5 * (zk.re - zmk.re);
+    return cplx<T>{er + (w.re * orr - w.im * oi), ei + (w.re * oi + w.im * orr)};
+}
+template <typename T>
+__device__ __forceinline__ cplx<T> c2r_split(const cplx<T> &xk, const cplx<T> &xmk, const cplx<T> &w, T c) {
+    const T er  = c * (xk.re + xmk.re);
+    const T ei  = c * (xk.im - xmk.im);
+    const T dr  = c * (xk.re - xmk.re);
+    const T di  = c * (xk.im + xmk.im);
+    const T orr = dr * w.re + di * w.im;
+    const T oi  = di * w.re - dr * w.im;
+    return cplx<T>{er - oi, ei + orr};
+}
+
 template <typename T, int M, class Ld, class St>
 __device__ __forceinline__ void r2c_row(int t, Ld ld, cplx<T> *s, const cplx<T> *__restrict__ twM,
                                         const cplx<T> *__restrict__ twN, St st) {
@@ -302,16 +324,18 @@ __device__ __forceinline__ void r2c_row(int t, Ld ld, cplx<T> *s, const cplx<T> 
     }
     __syncthreads();
     // X[k] = E[k] + W_N^k O[k],  E = (Z[k] + conj Z[M-k]) / 2,
-    // O = -i (Z[k] - conj Z[M-k]) / 2,  k = 0..M.
-    for (int k = t; k <= M; k += P) {
-        const cplx<T> zk  = s[wsi<M>(k & (M - 1))];
-        const cplx<T> zmk = s[wsi<M>((M - k) & (M - 1))];
-        const T       er  = (T)0.5 * (zk.re + zmk.re);
-        const T       ei  = (T)0.5 * (zk.im - zmk.im);
-        const T       orr = (T)0.5 * (zk.im + zmk.im);
-        const T       oi  = (T)-0.5 * (zk.re - zmk.re);
-        const cplx<T> w   = twN[k];  // e^{-2 pi i k / (2M)}, k = 0..M
-        st(k, cplx<T>{er + (w.re * orr - w.im * oi), ei + (w.re * oi + w.im * orr)});
+    // O = -i (Z[k] - conj Z[M-k]) / 2,  k = 0..M.  A thread reads the pair
+    // Z[k], Z[M-k] (k = t + P i <= M/2) once and forms X[k] and X[M-k].
+    constexpr int H = M / 2;
+#pragma unroll
+    for (int i = 0; i <= H / P; i++) {
+        const int k = t + P * i;
+        if (k <= H) {
+            const cplx<T> zk  = s[wsi<M>(k)];
+            const cplx<T> zmk = s[wsi<M>((M - k) & (M - 1))];
+            st(k, r2c_split<T>(zk, zmk, twN[k]));  // twN: e^{-2 pi i k / (2M)}, k = 0..M
+            if (k != H) st(M - k, r2c_split<T>(zmk, zk, twN[M - k]));
+        }
     }
     __syncthreads();
 }
@@ -322,46 +346,32 @@ __device__ __forceinline__ void c2r_row(int t, Ld ld, cplx<T> *s, const cplx<T> 
     constexpr int M1 = Split<M>::N1;
     constexpr int M2 = Split<M>::N2;
     constexpr int P  = M1;
-    // all loads of the row first (independent, in flight together), then
-    // the stores to the workspace
-    constexpr int KL = M / P + 1;
-    cplx<T>       xl[KL];
+    // Z'[k] = E' + i O',  E' = c (X[k] + conj X[M-k]),
+    // O' = c (X[k] - conj X[M-k]) W_N^{-k},  k = 0..M-1.  A thread loads
+    // the pair X[k], X[M-k] (k = t + P i <= M/2; all loads first, in flight
+    // together) and writes Z'[k] and Z'[M-k]; the imaginary parts of X[0]
+    // and X[M] are discarded.
+    constexpr int H  = M / 2;
+    constexpr int NI = H / P + 1;
+    cplx<T>       xa[NI], xb[NI];
 #pragma unroll
-    for (int i = 0; i < KL; i++) {
+    for (int i = 0; i < NI; i++) {
         const int k = t + P * i;
-        xl[i]       = k <= M ? ld(k) : cplx<T>{0, 0};
-    }
-#pragma unroll
-    for (int i = 0; i < KL; i++) {
-        const int k = t + P * i;
-        if (k <= M) {
-            cplx<T> x = xl[i];
-            if (k == 0 || k == M) x.im = 0;
-            s[wsi<M>(k)] = x;
+        if (k <= H) {
+            xa[i] = ld(k);
+            xb[i] = k == H ? xa[i] : ld(M - k);
         }
     }
-    __syncthreads();
-    // Z'[k] = E' + i O',  E' = c (X[k] + conj X[M-k]),
-    // O' = c (X[k] - conj X[M-k]) W_N^{-k},  k = 0..M-1.
-    constexpr int KPT = M / P;
-    cplx<T>       zz[KPT];
 #pragma unroll
-    for (int i = 0; i < KPT; i++) {
-        const int     k   = t + P * i;
-        const cplx<T> xk  = s[wsi<M>(k)];
-        const cplx<T> xmk = s[wsi<M>(M - k)];
-        const T       er  = scale * (xk.re + xmk.re);
-        const T       ei  = scale * (xk.im - xmk.im);
-        const T       dr  = scale * (xk.re - xmk.re);
-        const T       di  = scale * (xk.im + xmk.im);
-        const cplx<T> w   = twN[k];
-        const T       orr = dr * w.re + di * w.im;
-        const T       oi  = di * w.re - dr * w.im;
-        zz[i]             = cplx<T>{er - oi, ei + orr};
+    for (int i = 0; i < NI; i++) {
+        const int k = t + P * i;
+        if (k <= H) {
+            cplx<T> a = xa[i], b = xb[i];
+            if (k == 0) a.im = b.im = 0;
+            s[wsi<M>(k)] = c2r_split<T>(a, b, twN[k], scale);
+            if (k != 0 && k != H) s[wsi<M>(M - k)] = c2r_split<T>(b, a, twN[M - k], scale);
+        }
     }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < KPT; i++) s[wsi<M>(t + P * i)] = zz[i];
     __syncthreads();
     cplx<T> v[M2];
 #pragma unroll
@@ -407,12 +417,13 @@ __device__ __forceinline__ void store_pair(T *row, int n, cplx<T> z) {
 // ---------------------------------------------------------------------------
 // Z pass, forward: real rows -> complex rows (in and out may alias).
 // in:  real row r at in + r*2*hnzp (2M reals used),   M = NZ/2
-// out: complex row r at out + r*hnzp (M+1 values, padding zeroed)
+// out: complex row r at out + r*hnzp (M+1 values, padding zeroed); outputs
+//      kz >= kz_span are not written (pruned transforms downstream read none)
 // ---------------------------------------------------------------------------
 template <typename T, int M, int R>
 __global__ void __launch_bounds__(R *Split<M>::N1)
     fft_z_r2c_kernel(const T *in, cplx<T> *out, size_t field_stride_real, size_t field_stride_c, int nrows,
-                     int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN) {
+                     int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, int kz_span) {
     constexpr int P = Split<M>::N1;
     __shared__ __align__(16) cplx<T> s[R][ws_len<T, M>()];
     const int r   = threadIdx.x / P;
@@ -424,9 +435,9 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
     r2c_row<T, M>(
         t, [&](int n) { return ok ? load_pair<T>(rin, n) : cplx<T>{0, 0}; }, s[r], twM, twN,
         [&](int k, cplx<T> X) {
-            if (ok) rout[k] = X;
+            if (ok && k < kz_span) rout[k] = X;
         });
-    if (ok)
+    if (ok && kz_span > M)
         for (int k = M + 1 + t; k < hnzp; k += P) rout[k] = cplx<T>{0, 0};
 }
 

@@ -102,14 +102,15 @@ struct FFTPlan {
     }
 
     // Individual passes (exposed for the fused step).
-    cudaError_t z_r2c(const T *in, cplx<T> *out, int nfields, size_t fs_real, size_t fs_c, cudaStream_t st) const {
+    cudaError_t z_r2c(const T *in, cplx<T> *out, int nfields, size_t fs_real, size_t fs_c, cudaStream_t st,
+                      int kz_span = 1 << 30) const {
         const int nrows = g.nx * g.ny;
         switch (g.nz / 2) {
 #define SPM_ZR2C(MM)                                                                                   \
     case MM: {                                                                                         \
         constexpr int RR = zrows(MM);                                                                  \
         fft_z_r2c_kernel<T, MM, RR><<<dim3((nrows + RR - 1) / RR, nfields), RR * Split<MM>::N1, 0, st>>>( \
-            in, out, fs_real, fs_c, nrows, g.hnzp, tw_zm, tw_zn);                                      \
+            in, out, fs_real, fs_c, nrows, g.hnzp, tw_zm, tw_zn, kz_span);                             \
     } break;
             SPM_ZR2C(4) SPM_ZR2C(8) SPM_ZR2C(16) SPM_ZR2C(32) SPM_ZR2C(64) SPM_ZR2C(128) SPM_ZR2C(256)
 #undef SPM_ZR2C

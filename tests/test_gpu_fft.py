@@ -10,7 +10,8 @@ from kapsel3_b200.udf import SPMConfig
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(3, 3, 3), (4, 4, 4), (5, 5, 5), (6, 5, 4), (4, 6, 5), (7, 7, 7), (5, 4, 8), (8, 8, 8), (9, 3, 3)]
+SHAPES = [(3, 3, 3), (4, 4, 4), (5, 5, 5), (6, 5, 4), (4, 6, 5), (7, 7, 7), (5, 4, 8), (8, 8, 8), (9, 3, 3),
+          (3, 3, 6), (4, 3, 9)]
 
 
 @pytest.mark.parametrize("np3", SHAPES)
