@@ -143,6 +143,25 @@ int spm_get_shear_state(spm_ctx *ctx, double *degree_oblique, double stress[8]);
  * this library's own (binary, host byte order). */
 int spm_save_state(spm_ctx *ctx, const char *path);
 int spm_load_state(spm_ctx *ctx, const char *path);
+/* ---- output in the reference's legacy AVS format -----------------------
+ * (output.AVS = ON, FileType = BINARY; Init_avs / Output_avs,
+ * avs_output.cxx:45-143, 261-285; Init_avs_p / Output_avs_p,
+ * avs_output_p.cxx; frame content of Output_field_data, output.cxx:129-191).
+ * spm_avs_open writes <out_dir>/<out_name>.fld, <out_name>.cod and, with
+ * particles, <out_name>p.fld, and creates <out_dir>/avs.  spm_avs_frame
+ * writes the frame of the run's current (ts, time): avs/<out_name>_<ts>.dat
+ * (ux uy uz phi pressure tau_xy tau_yz tau_zx tau_xx tau_yy as float, x
+ * fastest) and avs/<out_name>p_<ts>.cod / .dat, appending the frame's
+ * description to the .fld files.  It returns once the frame is enqueued on
+ * the run's stream: the copy to host memory and the file writes overlap the
+ * following steps.  spm_avs_flush waits until every enqueued frame is on
+ * disk and reports the first write error; spm_avs_close flushes and releases
+ * the staging buffers (spm_destroy does too).  Navier_Stokes runs only (not
+ * Lees-Edwards, not pooled runs). */
+int spm_avs_open(spm_ctx *ctx, const char *out_dir, const char *out_name, int num_snap);
+int spm_avs_frame(spm_ctx *ctx);
+int spm_avs_flush(spm_ctx *ctx);
+int spm_avs_close(spm_ctx *ctx);
 
 /* ---- reference solver boundaries (host arrays, reference layout) -------- */
 /* NS_solver_slavedEuler (fluid_solver.h:77-82, fluid_solver.cxx:348-374):

@@ -106,6 +106,10 @@ _SIGS = {
     "spm_get_shear_state": (C.c_int, [_P, _D, _D]),
     "spm_save_state": (C.c_int, [_P, C.c_char_p]),
     "spm_load_state": (C.c_int, [_P, C.c_char_p]),
+    "spm_avs_open": (C.c_int, [_P, C.c_char_p, C.c_char_p, C.c_int]),
+    "spm_avs_frame": (C.c_int, [_P]),
+    "spm_avs_flush": (C.c_int, [_P]),
+    "spm_avs_close": (C.c_int, [_P]),
     "spm_ns_solver_slaved_euler_host": (C.c_int, [_P, _D, _D, _D]),
     "spm_solenoidal_uk_host": (C.c_int, [_P, _D, _D, _D]),
     "spm_zeta_k2u_k_host": (C.c_int, [_P, _D, _D, _D, _D, _D, _D]),

@@ -237,6 +237,20 @@ class SPMRun:
         """Restores a checkpoint written by a run with the same parameters."""
         N.check(self.L.spm_load_state(self.h, path.encode()), "spm_load_state")
 
+    def avs_open(self, out_dir: str, out_name: str, num_snap: int):
+        """Legacy AVS output of this run (spm_avs_open): headers now, one
+        frame per avs_frame() call."""
+        N.check(self.L.spm_avs_open(self.h, out_dir.encode(), out_name.encode(), int(num_snap)), "spm_avs_open")
+
+    def avs_frame(self):
+        """Enqueues the frame of the current step (spm_avs_frame); the files
+        are written while the run goes on."""
+        N.check(self.L.spm_avs_frame(self.h), "spm_avs_frame")
+
+    def avs_close(self):
+        """Waits for the enqueued frames and closes the output (spm_avs_close)."""
+        N.check(self.L.spm_avs_close(self.h), "spm_avs_close")
+
     def kernel_launches(self, reset: bool = False) -> int:
         n = C.c_longlong()
         N.check(self.L.spm_kernel_launches(self.h, C.byref(n), 1 if reset else 0), "spm_kernel_launches")

@@ -72,6 +72,22 @@ def run_reference(keys_path: str, dump_path: Optional[str] = None, fields_every:
     return r.stderr
 
 
+def run_reference_avs(keys_path: str, timeout: float = 600.0) -> str:
+    """Runs kapsel_ref_avs (the serial reference with its own legacy AVS
+    output) on a key file; the files go to the key file's
+    output.ON.Out_dir."""
+    exe = os.path.join(REF_DIR, "kapsel_ref_avs")
+    if not os.access(exe, os.X_OK):
+        raise FileNotFoundError("oracle/_ref/kapsel_ref_avs is not built (make -C oracle/ref_build)")
+    wd = tempfile.mkdtemp(prefix="kapsel_ref_avs_")
+    open(f"{wd}/def.udf", "w").close()
+    cmd = [exe, f"-I{keys_path}", f"-O{wd}/out.udf", f"-D{wd}/def.udf", f"-R{wd}/res.udf"]
+    r = subprocess.run(cmd, cwd=wd, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference run failed ({r.returncode}):\n{r.stderr[-3000:]}")
+    return r.stderr
+
+
 def read_dump(path: str) -> Dict:
     raw = open(path, "rb").read()
     hdr = np.frombuffer(raw, dtype=np.int32, count=8)
