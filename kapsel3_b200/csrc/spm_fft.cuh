@@ -169,6 +169,13 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
             }
         }
     }
+    // the step-1 twiddles of this thread's n1 = g are the same for every tile
+    cplx<T> tw1[N2];
+#pragma unroll
+    for (int k1 = 1; k1 < N2; k1++) {
+        tw1[k1] = twN[(g * k1) & (N - 1)];
+        if (DIR > 0) tw1[k1].im = -tw1[k1].im;
+    }
     int it = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
         const int b  = it % S;
@@ -187,11 +194,7 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
         }
         dft_reg<T, N2, DIR>(v);
 #pragma unroll
-        for (int k1 = 1; k1 < N2; k1++) {
-            cplx<T> tw = twN[(g * k1) & (N - 1)];
-            if (DIR > 0) tw.im = -tw.im;
-            v[k1] = cmul(v[k1], tw);
-        }
+        for (int k1 = 1; k1 < N2; k1++) v[k1] = cmul(v[k1], tw1[k1]);
 #pragma unroll
         for (int k1 = 0; k1 < N2; k1++) B[(g + N1 * k1) * W + c] = v[k1];
         __syncthreads();
@@ -493,31 +496,16 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
     const bool ok = row < nrows;
     const size_t roff = (size_t)(ok ? row : 0) * hnzp;
     T *Ur[3] = {U + (0 * R + r) * PITCH, U + (1 * R + r) * PITCH, U + (2 * R + r) * PITCH};
-    // Stage the CTA's rows of the three velocity fields (kz < kz_keep only)
-    // with 16-byte asynchronous copies, all in flight together; each complex
-    // row is then transformed in place into its real row.
-    {
-        const int keep   = kz_keep < M + 1 ? kz_keep : M + 1;
-        const int nchunk = (int)((keep * sizeof(cplx<T>) + 15) / 16);
-        for (int q = threadIdx.x; q < 3 * R * nchunk; q += blockDim.x) {
-            const int ch = q % nchunk, rr = (q / nchunk) % R, d = q / (nchunk * R);
-            const int grow = blockIdx.x * R + rr;
-            if (grow < nrows)
-                cp_async16(reinterpret_cast<char *>(U + (d * R + rr) * PITCH) + 16 * ch,
-                           reinterpret_cast<const char *>(io + d * field_stride_c + (size_t)grow * hnzp) + 16 * ch);
-        }
-        cp_async_commit();
-        cp_async_wait_all();
-        __syncthreads();
-    }
+    // Inverse z of the three velocity rows: each thread loads its pairs
+    // X[k], X[M-k] straight from global memory (all in flight together) and
+    // the real row lands in U[d].
 #pragma unroll 1
     for (int d = 0; d < 3; d++) {
-        const cplx<T> *rin = reinterpret_cast<const cplx<T> *>(Ur[d]);
+        const cplx<T> *rin = io + d * field_stride_c + roff;
         T             *ur  = Ur[d];
         c2r_row<T, M>(
             t, [&](int k) { return (ok && k < kz_keep) ? rin[k] : cplx<T>{0, 0}; }, ws + r * ws_len<T, M>(), twM, twN,
-            scale,
-            [&](int n, cplx<T> z) { store_pair<T>(ur, n, z); });
+            scale, [&](int n, cplx<T> z) { store_pair<T>(ur, n, z); });
     }
 #pragma unroll 1
     for (int p = 0; p < 5; p++) {

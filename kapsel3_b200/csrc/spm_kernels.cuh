@@ -1006,10 +1006,9 @@ __global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift) {
 
 // MD_solver_velocity_Euler / _AB2_hydro (particle_solver.cxx:103-142,
 // 239-281) followed by reset_Forces (particle_solver.cxx:11-37).
-__global__ void p_velocity(Phys ph, PState s, const int *__restrict__ ts_dev) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= ph.np) return;
-    const int euler = *ts_dev == 0;
+// Velocity / angular-velocity update of particle n (Euler at step 0, AB2
+// after) and the shift of the current forces to the previous ones.
+__device__ __forceinline__ void velocity_update_one(const Phys &ph, const PState &s, int n, int euler) {
     const double dmy = (euler ? ph.dt : ph.hdt) * ph.imass;
     const double dmr = (euler ? ph.dt : ph.hdt) * ph.imoi;
     for (int d = 0; d < 3; d++) {
@@ -1032,6 +1031,12 @@ __global__ void p_velocity(Phys ph, PState s, const int *__restrict__ ts_dev) {
         s.torque_hydro_previous[i] = s.torque_hydro[i];
         s.torque_hydro[i]          = 0.0;
     }
+}
+
+__global__ void p_velocity(Phys ph, PState s, const int *__restrict__ ts_dev) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ph.np) return;
+    velocity_update_one(ph, s, n, *ts_dev == 0);
 }
 
 // The Lees-Edwards velocity update also records momentum_depend_fr, the LJ
