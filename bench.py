@@ -308,7 +308,9 @@ def main():
             "unit": "GB/s", "frac": prof["gbs"] / peaks["hbm_gbs"], "traffic": read_traffic(),
             "traffic_source": TRAFFIC_FILE,
             "peak_source": peaks["source"], "bytes_per_launch": prof["bytes"], "avg_launch_us": prof["us"],
-            "note": "algorithmic bytes = one read + one write of every complex element the pass transforms"}
+            "note": ("algorithmic bytes = one read of every complex element a pass transforms that can be "
+                     "nonzero (inverse passes: |K| < TRN) + one write of every element that is needed "
+                     "(forward passes: |K| < TRN), over the visited lines and column tiles")}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": fp32["ms"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

@@ -399,27 +399,32 @@ cudaError_t strided_dispatch(spm_ctx *c, int slot, int nf, int axis, PassPrune p
 // inverse passes read modes outside it as zero, forward passes only produce
 // the column tiles (and on the X pass the ky lines) the box needs.
 PassPrune prune_inverse(const Grid &g, int axis) {
-    return axis == 0 ? PassPrune{g.trn[2], g.trn[1], g.trn[0], g.trn[2]}
-                     : PassPrune{g.trn[2], 0, g.trn[1], g.trn[2]};
+    return axis == 0 ? PassPrune{g.trn[2], g.trn[1], g.trn[0], g.trn[2], 0}
+                     : PassPrune{g.trn[2], 0, g.trn[1], g.trn[2], 0};
 }
 PassPrune prune_forward(const Grid &g, int axis) {
-    return axis == 0 ? PassPrune{g.trn[2], g.trn[1], 0, g.hnz} : PassPrune{g.trn[2], 0, 0, g.hnz};
+    return axis == 0 ? PassPrune{g.trn[2], g.trn[1], 0, g.hnz, g.trn[0]} : PassPrune{g.trn[2], 0, 0, g.hnz, g.trn[1]};
 }
 
-// Complex elements a strided pass transforms (lines x columns x fields).
+// Complex elements a strided pass must read plus those it must write: the
+// visited lines x columns x fields, reads limited to the lines that can be
+// nonzero (|K| < line_trn) and writes to the lines that are needed (|K| <
+// out_trn) on pruned passes.
 template <typename T>
-double pass_elems(spm_ctx *c, int nf, int axis, const PassPrune &pr) {
+double pass_elems_rw(spm_ctx *c, int nf, int axis, const PassPrune &pr) {
     const Grid &g     = c->g;
     const int   n     = axis == 1 ? g.ny : g.nx;
     const int   outer = axis == 1 ? g.nx : g.ny;
     const int   wk    = (c->use_tma && n <= 256) ? FFTPlan<T>::W_T : FFTPlan<T>::W;
     const int   cols  = std::min(g.hnz, (std::min(pr.kz_cols, g.hnz) + wk - 1) / wk * wk);
-    return (double)nf * c->fft_runs * outer_count(outer, pr.outer_trn) * (double)n * cols;
+    const int   hl    = pruned_box_lines(n, pr.line_trn);
+    const int   hs    = pruned_box_lines(n, pr.out_trn);
+    const int   lines = (hl == n ? n : 2 * hl) + (hs == n ? n : 2 * hs);
+    return (double)nf * c->fft_runs * outer_count(outer, pr.outer_trn) * (double)lines * cols;
 }
 
 // Strided (Y/X) FFT pass, bracketed by CUDA events when profiling is on (the
-// algorithmic bytes of a pass: one read and one write of every element it
-// transforms).
+// algorithmic bytes of a pass: pass_elems_rw complex elements).
 template <typename T, int DIR>
 int fft_strided_pass(spm_ctx *c, int slot, int nf, int axis, PassPrune pr) {
     if (c->prof_on) {
@@ -431,7 +436,7 @@ int fft_strided_pass(spm_ctx *c, int slot, int nf, int axis, PassPrune pr) {
         SPM_CUDA_CHECK(cudaEventRecord(b, c->st));
         c->prof_ev.push_back(a);
         c->prof_ev.push_back(b);
-        c->prof_bytes += 2.0 * pass_elems<T>(c, nf, axis, pr) * sizeof(cplx<T>);
+        c->prof_bytes += pass_elems_rw<T>(c, nf, axis, pr) * sizeof(cplx<T>);
     } else {
         SPM_CUDA_CHECK((strided_dispatch<T, DIR>(c, slot, nf, axis, pr)));
     }

@@ -41,8 +41,13 @@ struct PassPrune {
     int outer_trn;  // > 0: only outer lines o with |K(o)| < outer_trn
     int line_trn;   // > 0: input lines with |K(n)| >= line_trn read as zero
     int col_keep;   // input columns kz >= col_keep read as zero
-    static PassPrune full(int hnz) { return PassPrune{hnz, 0, 0, hnz}; }
+    int out_trn;    // > 0: only output lines with |K(n)| < out_trn are needed
+    static PassPrune full(int hnz) { return PassPrune{hnz, 0, 0, hnz, 0}; }
 };
+// Lines a TMA box of a pruned pass covers: two boxes of h lines at 0 and
+// N - h hold every line with |K| < trn (h = trn), one box of N lines
+// otherwise.
+__host__ __device__ __forceinline__ int pruned_box_lines(int n, int trn) { return (trn > 0 && 2 * trn < n) ? trn : n; }
 
 __host__ __device__ __forceinline__ int signed_mode(int n, int len) { return n > len / 2 ? n - len : n; }
 __host__ __device__ __forceinline__ int outer_count(int n_outer, int outer_trn) {
@@ -127,11 +132,17 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
 // ---------------------------------------------------------------------------
 template <typename T, int N, int W, int DIR, int S>
 __global__ void __launch_bounds__(W *Split<N>::N1)
-    fft_strided_tma_kernel(const __grid_constant__ CUtensorMap map, int axis, int n_outer, int ct_used,
-                           int ntiles, const cplx<T> *__restrict__ twN, unsigned int *err, PassPrune pr) {
-    constexpr int      N1         = Split<N>::N1;
-    constexpr int      N2         = Split<N>::N2;
-    constexpr unsigned tile_bytes = N * W * sizeof(cplx<T>);
+    fft_strided_tma_kernel(const __grid_constant__ CUtensorMap lmap, const __grid_constant__ CUtensorMap smap,
+                           int axis, int n_outer, int ct_used, int ntiles, const cplx<T> *__restrict__ twN,
+                           unsigned int *err, PassPrune pr) {
+    constexpr int  N1         = Split<N>::N1;
+    constexpr int  N2         = Split<N>::N2;
+    // lines per load / store box (lmap / smap): N, or two boxes of the
+    // pruned line count (inputs outside them are zero, outputs outside them
+    // are not needed)
+    const int      hl         = pruned_box_lines(N, pr.line_trn);
+    const int      hs         = pruned_box_lines(N, pr.out_trn);
+    const unsigned load_bytes = (unsigned)((hl == N ? N : 2 * hl) * W * sizeof(cplx<T>));
     extern __shared__ __align__(128) unsigned char smem_raw[];
     cplx<T>           *buf = reinterpret_cast<cplx<T> *>(smem_raw);
     __shared__ __align__(8) uint64_t full[S];
@@ -158,15 +169,23 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
         fence_mbar_init();
     }
     __syncthreads();
+    // tile t into ring buffer b: lines [0, hl) and, when pruned, [N - hl, N)
+    auto load_tile = [&](int t, int b) {
+        int c0, c1, c2, c3;
+        coords(t, c0, c1, c2, c3);
+        cplx<T> *dst = buf + (size_t)b * N * W;
+        mbar_expect_tx(&full[b], load_bytes);
+        tma_load_4d(dst, &lmap, c0, c1, c2, c3, &full[b]);
+        if (hl < N) {
+            const int sh = N - hl;
+            tma_load_4d(dst + (size_t)sh * W, &lmap, c0, c1 + (axis == 1 ? sh : 0), c2 + (axis == 1 ? 0 : sh), c3,
+                        &full[b]);
+        }
+    };
     if (tid == 0) {
         for (int b = 0; b < S; b++) {
             const int t = blockIdx.x + b * gridDim.x;
-            if (t < ntiles) {
-                int c0, c1, c2, c3;
-                coords(t, c0, c1, c2, c3);
-                mbar_expect_tx(&full[b], tile_bytes);
-                tma_load_4d(buf + (size_t)b * N * W, &map, c0, c1, c2, c3, &full[b]);
-            }
+            if (t < ntiles) load_tile(t, b);
         }
     }
     // the step-1 twiddles of this thread's n1 = g are the same for every tile
@@ -219,18 +238,19 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
         if (tid == 0) {
             int c0, c1, c2, c3;
             coords(t, c0, c1, c2, c3);
-            tma_store_4d(&map, c0, c1, c2, c3, B);
+            tma_store_4d(&smap, c0, c1, c2, c3, B);
+            if (hs < N) {
+                const int sh = N - hs;
+                tma_store_4d(&smap, c0, c1 + (axis == 1 ? sh : 0), c2 + (axis == 1 ? 0 : sh), c3, B + (size_t)sh * W);
+            }
             bulk_commit();
             // refill the buffer of the previous iteration with the tile S
             // iterations after it, once its store has read shared memory
             if (it >= 1) {
                 const int tn = t + (S - 1) * (int)gridDim.x;
                 if (tn < ntiles) {
-                    const int bp = (it - 1) % S;
                     bulk_wait_read<1>();
-                    coords(tn, c0, c1, c2, c3);
-                    mbar_expect_tx(&full[bp], tile_bytes);
-                    tma_load_4d(buf + (size_t)bp * N * W, &map, c0, c1, c2, c3, &full[bp]);
+                    load_tile(tn, (it - 1) % S);
                 }
             }
         }

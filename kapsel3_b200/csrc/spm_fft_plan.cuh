@@ -152,13 +152,19 @@ struct FFTPlan {
         const int ct_used = (std::min(pr.kz_cols, g.hnz) + W_T - 1) / W_T;
         const int ntiles  = nfields * outer_count(outer, pr.outer_trn) * ct_used;
         if (ntiles == 0) return cudaSuccess;
-        CUtensorMap   map;
         const uint64_t dims[4] = {(uint64_t)2 * g.hnz, (uint64_t)g.ny, (uint64_t)g.nx, (uint64_t)nfields};
         const uint64_t strides[3] = {(uint64_t)2 * g.hnzp * sizeof(T), (uint64_t)g.ny * 2 * g.hnzp * sizeof(T),
                                      (uint64_t)fs_c * sizeof(cplx<T>)};
-        const uint32_t box[4] = {(uint32_t)(2 * W_T), axis == 1 ? (uint32_t)n : 1u, axis == 1 ? 1u : (uint32_t)n,
-                                 1u};
-        if (!make_map_4d<T>(&map, data, dims, strides, box)) return cudaErrorNotSupported;
+        // load and store maps: boxes of N lines, or of the pruned line count
+        // (two boxes per tile, pruned_box_lines)
+        CUtensorMap lmap, smap;
+        auto        make = [&](CUtensorMap *m, int lines) {
+            const uint32_t box[4] = {(uint32_t)(2 * W_T), axis == 1 ? (uint32_t)lines : 1u,
+                                     axis == 1 ? 1u : (uint32_t)lines, 1u};
+            return make_map_4d<T>(m, data, dims, strides, box);
+        };
+        if (!make(&lmap, pruned_box_lines(n, pr.line_trn)) || !make(&smap, pruned_box_lines(n, pr.out_trn)))
+            return cudaErrorNotSupported;
         const cplx<T> *tw   = axis == 1 ? tw_y : tw_x;
         const int      grid = std::min(ntiles, sm_count * ctas_per_sm);
         switch (n) {
@@ -166,7 +172,7 @@ struct FFTPlan {
     case NN:                                                                                                   \
         fft_strided_tma_kernel<T, NN, W_T, DIR, S_T>                                                           \
             <<<grid, W_T * Split<NN>::N1, (size_t)S_T * NN * W_T * sizeof(cplx<T>), st>>>(                     \
-                map, axis, outer, ct_used, ntiles, tw, err, pr);                                               \
+                lmap, smap, axis, outer, ct_used, ntiles, tw, err, pr);                                        \
         break;
             SPM_TMA(8) SPM_TMA(16) SPM_TMA(32) SPM_TMA(64) SPM_TMA(128) SPM_TMA(256)
 #undef SPM_TMA
