@@ -195,6 +195,12 @@ struct spm_ctx {
     bool                     zeta_dirty = false;  // zeta set by the host since the last NS step
     int                      nslots     = NSLOT;  // field slots of this run (slots_for)
     AvsOut                  *avs        = nullptr;  // AVS field/particle output (spm_avs_open)
+    // one Navier_Stokes step of a lone run captured as a CUDA graph and
+    // replayed by spm_step (SPM_NO_GRAPH=1 keeps the direct launches)
+    bool                     use_graph    = true;
+    cudaGraph_t              step_graph   = nullptr;
+    cudaGraphExec_t          step_exec    = nullptr;
+    long long                step_kernels = 0;
 
     bool fp64() const { return P.precision == SPM_PREC_FP64; }
     // zeta kept as a compensated FP32 pair (FP32-mixed Navier_Stokes)
@@ -692,6 +698,44 @@ int step_impl(spm_ctx *c) {
     return step_ns<T>(c);
 }
 
+// One Navier_Stokes step from the run's captured graph.  The first call
+// captures step_ns (the side-stream fork and join included) and restores the
+// host counters the capture advanced; every call replays the graph and
+// advances them.  Host-set zeta is truncated before, outside the graph.
+template <typename T>
+int step_graphed(spm_ctx *c) {
+    int rc;
+    if ((rc = truncate_if_dirty<T>(c)) != SPM_OK) return rc;
+    if (!c->step_exec) {
+        const int       ts = c->ts;
+        const double    tm = c->time;
+        const long long ln = c->launches;
+        SPM_CUDA_CHECK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+        rc              = step_ns<T>(c);
+        cudaGraph_t g   = nullptr;
+        cudaError_t e   = cudaStreamEndCapture(c->st, &g);
+        c->step_kernels = c->launches - ln;
+        c->ts           = ts;
+        c->time         = tm;
+        c->launches     = ln;
+        if (rc != SPM_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return rc != SPM_OK ? rc : fail(SPM_ERR_CUDA, std::string("step capture: ") + cudaGetErrorString(e));
+        }
+        if ((e = cudaGraphInstantiate(&c->step_exec, g, 0)) != cudaSuccess) {
+            cudaGraphDestroy(g);
+            return fail(SPM_ERR_CUDA, std::string("step graph instantiate: ") + cudaGetErrorString(e));
+        }
+        c->step_graph = g;
+    }
+    SPM_CUDA_CHECK(cudaGraphLaunch(c->step_exec, c->st));
+    c->launches += c->step_kernels;
+    c->ts++;
+    c->time += c->ph.dt;
+    return SPM_OK;
+}
+
 // host <-> device field transfer with precision conversion
 int upload_field(spm_ctx *c, int slot, const double *h) {
     const size_t nd = (size_t)c->g.nx * c->g.ny * 2 * c->g.hnz;  // reference layout
@@ -820,6 +864,8 @@ void destroy_ctx(spm_ctx *c) {
     if (!c) return;
     avs_release(c);
     if (c->st) cudaStreamSynchronize(c->st);
+    if (c->step_exec) cudaGraphExecDestroy(c->step_exec);
+    if (c->step_graph) cudaGraphDestroy(c->step_graph);
     c->plan64.destroy();
     c->plan32.destroy();
     if (c->owns_arena) dev_free(c->arena);
@@ -884,6 +930,8 @@ int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *
         c->use_tma     = !(nt && nt[0] == '1');
         const char *no = getenv("SPM_NO_OVERLAP");
         c->overlap     = !(no && no[0] == '1');
+        const char *ng = getenv("SPM_NO_GRAPH");
+        c->use_graph   = !(ng && ng[0] == '1');
     }
     cudaError_t e = cudaSuccess;
     if (lead) {
@@ -1074,8 +1122,10 @@ int spm_initialize(spm_ctx *c, const double *particles_host) {
 
 int spm_step(spm_ctx *c, int nsteps) {
     if (!c || nsteps < 0) return fail(SPM_ERR_ARG, "bad argument");
+    const bool graph = c->use_graph && !c->pool && !c->prof_on && c->P.equation == SPM_EQ_NAVIER_STOKES;
     for (int i = 0; i < nsteps; i++) {
-        int rc = c->fp64() ? step_impl<double>(c) : step_impl<float>(c);
+        int rc = graph ? (c->fp64() ? step_graphed<double>(c) : step_graphed<float>(c))
+                       : (c->fp64() ? step_impl<double>(c) : step_impl<float>(c));
         if (rc != SPM_OK) return rc;
     }
     return SPM_OK;
