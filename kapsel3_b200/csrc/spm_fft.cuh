@@ -315,15 +315,18 @@ __device__ __forceinline__ cplx<T> c2r_split(const cplx<T> &xk, const cplx<T> &x
     return cplx<T>{er - oi, ei + orr};
 }
 
-template <typename T, int M, class Ld, class St>
-__device__ __forceinline__ void r2c_row(int t, Ld ld, cplx<T> *s, const cplx<T> *__restrict__ twM,
-                                        const cplx<T> *__restrict__ twN, St st) {
+// r2c_row_m: as r2c_row, with ldm(m) returning the input of element
+// t + M1 m (m = 0..M2-1, a compile-time index after unrolling), so the row
+// may come from registers.
+template <typename T, int M, class LdM, class St>
+__device__ __forceinline__ void r2c_row_m(int t, LdM ldm, cplx<T> *s, const cplx<T> *__restrict__ twM,
+                                          const cplx<T> *__restrict__ twN, St st) {
     constexpr int M1 = Split<M>::N1;
     constexpr int M2 = Split<M>::N2;
     constexpr int P  = M1;
     cplx<T>       v[M2];
 #pragma unroll
-    for (int m = 0; m < M2; m++) v[m] = ld(t + M1 * m);
+    for (int m = 0; m < M2; m++) v[m] = ldm(m);
     dft_reg<T, M2, -1>(v);
 #pragma unroll
     for (int k1 = 1; k1 < M2; k1++) v[k1] = cmul(v[k1], twM[(t * k1) & (M - 1)]);
@@ -364,8 +367,17 @@ __device__ __forceinline__ void r2c_row(int t, Ld ld, cplx<T> *s, const cplx<T> 
 }
 
 template <typename T, int M, class Ld, class St>
-__device__ __forceinline__ void c2r_row(int t, Ld ld, cplx<T> *s, const cplx<T> *__restrict__ twM,
-                                        const cplx<T> *__restrict__ twN, T scale, St st) {
+__device__ __forceinline__ void r2c_row(int t, Ld ld, cplx<T> *s, const cplx<T> *__restrict__ twM,
+                                        const cplx<T> *__restrict__ twN, St st) {
+    r2c_row_m<T, M>(t, [&](int m) { return ld(t + Split<M>::N1 * m); }, s, twM, twN, st);
+}
+
+// c2r_row_m: as c2r_row, with stm(m, z) receiving output element t + M1 m
+// (m = 0..M2-1, compile-time after unrolling), so the row may stay in
+// registers.
+template <typename T, int M, class Ld, class StM>
+__device__ __forceinline__ void c2r_row_m(int t, Ld ld, cplx<T> *s, const cplx<T> *__restrict__ twM,
+                                          const cplx<T> *__restrict__ twN, T scale, StM stm) {
     constexpr int M1 = Split<M>::N1;
     constexpr int M2 = Split<M>::N2;
     constexpr int P  = M1;
@@ -417,9 +429,16 @@ __device__ __forceinline__ void c2r_row(int t, Ld ld, cplx<T> *s, const cplx<T> 
         for (int n1 = 0; n1 < M1; n1++) u[n1] = s[wsi<M>(n1 + M1 * k1)];
         dft_reg<T, M1, +1>(u);
 #pragma unroll
-        for (int k2 = 0; k2 < M1; k2++) st(k1 + M2 * k2, u[k2]);
+        for (int k2 = 0; k2 < M1; k2++) stm(i + (M2 / M1) * k2, u[k2]);  // element k1 + M2 k2 = t + M1 m
     }
     __syncthreads();
+}
+
+template <typename T, int M, class Ld, class St>
+__device__ __forceinline__ void c2r_row(int t, Ld ld, cplx<T> *s, const cplx<T> *__restrict__ twM,
+                                        const cplx<T> *__restrict__ twN, T scale, St st) {
+    c2r_row_m<T, M>(t, ld, s, twM, twN, scale,
+                    [&](int m, const cplx<T> &z) { st(t + Split<M>::N1 * m, z); });
 }
 
 template <typename T>
@@ -545,6 +564,61 @@ __global__ void __launch_bounds__(R *Split<M>::N1)
                 return cplx<T>{o[0], o[1]};
             },
             ws + r * ws_len<T, M>(), twM, twN,
+            [&](int k, cplx<T> X) {
+                if (ok && k < kz_span) rout[k] = X;
+            });
+        if (ok && kz_span > M)
+            for (int k = M + 1 + t; k < hnzp; k += P) rout[k] = cplx<T>{0, 0};
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The same fused Z pass with the three velocity rows kept in registers: the
+// inverse transform leaves element t + M1 m of its row in slot m of thread
+// t, which is the slot the forward transform of a product reads it from, so
+// the products are formed in registers and only the transform workspace is
+// in shared memory (for FP32 rows: 3 x M2 complex values per thread).
+// ---------------------------------------------------------------------------
+template <typename T, int M, int R>
+__global__ void __launch_bounds__(R *Split<M>::N1)
+    fft_z_products_reg_kernel(cplx<T> *io, size_t field_stride_c, size_t run_stride_c, int nrows, int hnzp,
+                              const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale,
+                              int kz_keep, int kz_span) {
+    constexpr int P  = Split<M>::N1;
+    constexpr int M2 = Split<M>::N2;
+    __shared__ __align__(16) cplx<T> ws[R][ws_len<T, M>()];
+    io += (size_t)blockIdx.y * run_stride_c;  // run of a batched pool
+    const int    r    = threadIdx.x / P;
+    const int    t    = threadIdx.x % P;
+    const int    row  = blockIdx.x * R + r;
+    const bool   ok   = row < nrows;
+    const size_t roff = (size_t)(ok ? row : 0) * hnzp;
+    cplx<T>      u[3][M2];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const cplx<T> *rin = io + d * field_stride_c + roff;
+        c2r_row_m<T, M>(
+            t, [&](int k) { return (ok && k < kz_keep) ? rin[k] : cplx<T>{0, 0}; }, ws[r], twM, twN, scale,
+            [&](int m, const cplx<T> &z) { u[d][m] = z; });
+    }
+#pragma unroll 1
+    for (int p = 0; p < 5; p++) {
+        cplx<T> *rout = io + p * field_stride_c + roff;
+        r2c_row_m<T, M>(
+            t,
+            [&](int m) {
+                const T xs[2] = {u[0][m].re, u[0][m].im}, ys[2] = {u[1][m].re, u[1][m].im},
+                        zs[2] = {u[2][m].re, u[2][m].im};
+                T o[2];
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const T x = xs[e], y = ys[e], z = zs[e];
+                    o[e] = p == 0 ? y * z : p == 1 ? z * x : p == 2 ? x * y : p == 3 ? (y - z) * (y + z)
+                                                                                     : (z - x) * (z + x);
+                }
+                return cplx<T>{o[0], o[1]};
+            },
+            ws[r], twM, twN,
             [&](int k, cplx<T> X) {
                 if (ok && k < kz_span) rout[k] = X;
             });

@@ -56,10 +56,17 @@ struct FFTPlan {
         switch (g.nz / 2) {
 #define SPM_ZP(MM)                                                                                  \
     case MM: {                                                                                      \
-        constexpr int RR = prows(MM);                                                               \
-        fft_z_products_kernel<T, MM, RR>                                                            \
-            <<<dim3((nrows + RR - 1) / RR, nruns), RR * Split<MM>::N1, psmem(MM), st>>>(            \
-                io, fs_c, run_stride_c, nrows, g.hnzp, tw_zm, tw_zn, scale, kz_keep, kz_span);      \
+        if (sizeof(T) == 4 && kRegProducts) {                                                       \
+            constexpr int RR = zrows(MM);                                                           \
+            fft_z_products_reg_kernel<T, MM, RR>                                                    \
+                <<<dim3((nrows + RR - 1) / RR, nruns), RR * Split<MM>::N1, 0, st>>>(                \
+                    io, fs_c, run_stride_c, nrows, g.hnzp, tw_zm, tw_zn, scale, kz_keep, kz_span);  \
+        } else {                                                                                    \
+            constexpr int RR = prows(MM);                                                           \
+            fft_z_products_kernel<T, MM, RR>                                                        \
+                <<<dim3((nrows + RR - 1) / RR, nruns), RR * Split<MM>::N1, psmem(MM), st>>>(        \
+                    io, fs_c, run_stride_c, nrows, g.hnzp, tw_zm, tw_zn, scale, kz_keep, kz_span);  \
+        }                                                                                           \
     } break;
             SPM_ZP(4) SPM_ZP(8) SPM_ZP(16) SPM_ZP(32) SPM_ZP(64) SPM_ZP(128) SPM_ZP(256)
 #undef SPM_ZP
@@ -137,10 +144,12 @@ struct FFTPlan {
     // Persistent TMA-pipelined strided pass (N <= 256): tile W_T columns,
     // S_T-deep buffer ring.  Returns cudaErrorNotSupported when it cannot run
     // (size or missing driver entry point); the caller then uses strided().
-    static constexpr int W_T = sizeof(T) == 8 ? 8 : 16;
+    static constexpr int W_T = sizeof(T) == 8 ? 16 : 32;
     static constexpr int S_T = 3;
+    // FP32 advection products with the velocity rows in registers
+    static constexpr bool kRegProducts = true;
     unsigned int *err = nullptr;  // device error word (set by the owner)
-    int           ctas_per_sm = 2;
+    int           ctas_per_sm = 1;
     int           sm_count    = 148;
 
     template <int DIR>
