@@ -651,7 +651,7 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
                c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS), c->real<T>(U0), c->real<T>(U1), c->real<T>(U2),
                c->ps.f_hydro, c->ps.torque_hydro);
         LAUNCH(c, p_velocity, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev);
-        if (c->P.kbt > 0.0) LAUNCH(c, p_thermostat_serial, 1, 32, 0, c->ph, c->ps, c->mt);
+        if (c->P.kbt > 0.0) LAUNCH(c, p_thermostat, 1, kThermoThreads, 0, c->ph, c->ps, c->mt);
         const dim3 sgrid((c->ncells + 127) / 128, c->ph.np);
         LAUNCH(c, s_f_scatter_cached<T>, sgrid, 128, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
                c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS), c->real<T>(U0), c->real<T>(U1), c->real<T>(U2),

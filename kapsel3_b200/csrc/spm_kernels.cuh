@@ -1099,52 +1099,125 @@ __global__ void k_fix_cell(RunWords *rw, int nr) {
 // (Add_random_force_thermostat, fluct.cxx:10-37).
 // State layout: mt[0..623], mt[624] = mti.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned int mt_next(unsigned int *mt) {
-    unsigned int mti = mt[624];
-    if (mti >= 624u) {
-        for (int i = 0; i < 624; i++) {
-            const unsigned int y = (mt[i] & 0x80000000u) | (mt[(i + 1) % 624] & 0x7fffffffu);
-            unsigned int       v = mt[(i + 397) % 624] ^ (y >> 1);
-            if (y & 1u) v ^= 0x9908b0dfu;
-            mt[i] = v;
-        }
-        mti = 0;
-    }
-    unsigned int y = mt[mti++];
-    mt[624]        = mti;
+// The draws are made by one block of 1024 threads, with the generator state
+// in shared memory, and reproduce the serial stream exactly:
+//  - the MT19937 twist runs in four phases [0,227) [227,454) [454,623)
+//    [623], each reading only words the serial loop has already updated or
+//    not yet touched, then the outputs are tempered in parallel;
+//  - Gauss2 consumes uniforms in consecutive pairs (x1, x2) from the
+//    stream, so the pairs are fixed by the stream; each is accepted when
+//    0 < x1^2 + x2^2 < 1, and a block prefix sum over the accept flags
+//    hands accepted pair a to particle a / 3, pair a % 3 (normals 2(a%3),
+//    2(a%3)+1 of that particle: v for normals 0-2, omega for 3-5);
+//  - the state advances by exactly the uniforms the serial loop consumes
+//    (up to the second uniform of the last accepted pair).
+constexpr int kThermoThreads = 1024;
+__device__ __forceinline__ unsigned int mt_temper(unsigned int y) {
     y ^= (y >> 11);
     y ^= (y << 7) & 0x9d2c5680u;
     y ^= (y << 15) & 0xefc60000u;
     y ^= (y >> 18);
     return y;
 }
-__device__ __forceinline__ double mt_real3(unsigned int *mt) {
-    return ((double)mt_next(mt) + 0.5) * (1.0 / 4294967296.0);
+__device__ __forceinline__ unsigned int mt_twist_word(const unsigned int *mt, int i) {
+    const unsigned int y = (mt[i] & 0x80000000u) | (mt[(i + 1) % 624] & 0x7fffffffu);
+    unsigned int       v = mt[(i + 397) % 624] ^ (y >> 1);
+    if (y & 1u) v ^= 0x9908b0dfu;
+    return v;
 }
-__device__ __forceinline__ void gauss2(unsigned int *mt, double &g0, double &g1) {
-    double x1, x2, rsq;
-    do {
-        x1  = 2.0 * mt_real3(mt) - 1.0;
-        x2  = 2.0 * mt_real3(mt) - 1.0;
-        rsq = x1 * x1 + x2 * x2;
-    } while (rsq >= 1.0 || rsq == 0.0);
-    const double factor = sqrt(-2.0 * log(rsq) / rsq);
-    g0                  = factor * x1;
-    g1                  = factor * x2;
+__global__ void __launch_bounds__(kThermoThreads) p_thermostat(Phys ph, PState s, unsigned int *mt_g) {
+    __shared__ unsigned int mt[624];
+    __shared__ double       uni[624 + 1];  // the carried uniform, then this round's outputs
+    __shared__ int          wsum[kThermoThreads / 32];
+    __shared__ int          sh_mti, sh_carry, sh_done, sh_taken, sh_used;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int i = tid; i < 624; i += blockDim.x) mt[i] = mt_g[i];
+    if (tid == 0) {
+        sh_mti   = (int)mt_g[624];
+        sh_carry = 0;
+        sh_done  = 0;
+        sh_taken = 0;
+    }
+    __syncthreads();
+    const int need = 3 * ph.np;  // accepted pairs
+    if (need == 0) return;
+    // a round accepts about 245 pairs; the cap only bounds the loop
+    for (int round = 0; !sh_done && round < need + 64; round++) {
+        if (sh_mti >= 624) {  // twist, in four dependency-ordered phases
+            const int lo[4] = {0, 227, 454, 623}, hi[4] = {227, 454, 623, 624};
+            for (int ph4 = 0; ph4 < 4; ph4++) {
+                const int    i = lo[ph4] + tid;
+                unsigned int v = 0;
+                if (i < hi[ph4]) v = mt_twist_word(mt, i);
+                __syncthreads();
+                if (i < hi[ph4]) mt[i] = v;
+                __syncthreads();
+            }
+            if (tid == 0) sh_mti = 0;
+            __syncthreads();
+        }
+        const int mti = sh_mti, carry = sh_carry, avail = 624 - mti;
+        for (int j = tid; j < avail; j += blockDim.x)
+            uni[carry + j] = ((double)mt_temper(mt[mti + j]) + 0.5) * (1.0 / 4294967296.0);
+        __syncthreads();
+        const int npairs = (carry + avail) / 2;
+        // accept flags and their exclusive prefix sum (one pair per thread)
+        bool   acc = false;
+        double x1 = 0, x2 = 0, rsq = 0;
+        if (tid < npairs) {
+            x1  = 2.0 * uni[2 * tid] - 1.0;
+            x2  = 2.0 * uni[2 * tid + 1] - 1.0;
+            rsq = x1 * x1 + x2 * x2;
+            acc = !(rsq >= 1.0 || rsq == 0.0);
+        }
+        const unsigned ball = __ballot_sync(0xffffffffu, acc);
+        if (lane == 0) wsum[wid] = __popc(ball);
+        __syncthreads();
+        if (wid == 0) {
+            int v = lane < kThermoThreads / 32 ? wsum[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += t;
+            }
+            if (lane < kThermoThreads / 32) wsum[lane] = v;  // inclusive per warp
+        }
+        __syncthreads();
+        const int before = sh_taken + (wid ? wsum[wid - 1] : 0) + __popc(ball & ((1u << lane) - 1u));
+        const int total  = sh_taken + wsum[kThermoThreads / 32 - 1];
+        if (acc && before < need) {
+            const double factor = sqrt(-2.0 * log(rsq) / rsq);
+            const double g[2]   = {factor * x1, factor * x2};
+            const int    n = before / 3, k = before % 3;
+            for (int e = 0; e < 2; e++) {
+                const int q = 2 * k + e;  // normal index of particle n
+                if (q < 3)
+                    s.v[3 * n + q] += g[e] * ph.noise_v * ph.imass;
+                else if (ph.rotation)
+                    s.omega[3 * n + q - 3] += g[e] * ph.noise_o * ph.imoi;
+            }
+            if (before == need - 1) sh_used = 2 * (tid + 1);  // uniforms consumed this round
+        }
+        __syncthreads();
+        if (tid == 0) {
+            if (total >= need) {
+                sh_mti += sh_used - carry;  // state words consumed this round
+                sh_done = 1;
+            } else {
+                sh_taken = total;
+                if ((carry + avail) & 1) {  // odd output left: it starts the next pair
+                    uni[0]   = uni[carry + avail - 1];
+                    sh_carry = 1;
+                } else {
+                    sh_carry = 0;
+                }
+                sh_mti = 624;
+            }
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < 624; i += blockDim.x) mt_g[i] = mt[i];
+    if (tid == 0) mt_g[624] = (unsigned int)sh_mti;
 }
 
-__global__ void p_thermostat_serial(Phys ph, PState s, unsigned int *mt) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    for (int n = 0; n < ph.np; n++) {
-        double g[6];
-        gauss2(mt, g[0], g[1]);
-        gauss2(mt, g[2], g[3]);
-        gauss2(mt, g[4], g[5]);
-        for (int d = 0; d < 3; d++) {
-            s.v[3 * n + d] += g[d] * ph.noise_v * ph.imass;
-            if (ph.rotation) s.omega[3 * n + d] += g[d + 3] * ph.noise_o * ph.imoi;
-        }
-    }
-}
 
 }  // namespace spm
