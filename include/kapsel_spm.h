@@ -47,6 +47,7 @@ extern "C" {
 
 #define SPM_EQ_NAVIER_STOKES 0  /* constitutive_eq.type = Navier_Stokes */
 #define SPM_EQ_LEES_EDWARDS 1   /* Shear_Navier_Stokes_Lees_Edwards */
+#define SPM_EQ_ELECTROLYTE 2    /* Electrolyte: charged colloids with mobile ions */
 
 #define SPM_PREC_FP64 0        /* every field and reduction in FP64 */
 #define SPM_PREC_FP32_MIXED 1  /* fields/FFT/projection FP32, particle reductions and updates FP64 */
@@ -73,6 +74,18 @@ typedef struct spm_params {
     double body_force[3];        /* constant force added to every particle's fr */
     int    precision;            /* SPM_PREC_* */
     unsigned int mt_seed;        /* MT19937 seed of the thermostat (reference: 0) */
+    /* Electrolyte (constitutive_eq.Electrolyte, input.cxx:834-930; read when
+     * equation == SPM_EQ_ELECTROLYTE) */
+    double dielectric;           /* Dielectric_cst */
+    int    salt;                 /* Add_salt: 0 saltfree (one counterion species), 1 salt (two species) */
+    int    init_pb;              /* INIT_profile: 0 Uniform, 1 Poisson_Boltzmann */
+    double valency[2];           /* saltfree: Valency_counterion; salt: positive, negative ion */
+    double onsager[2];           /* Onsager coefficients in the same order */
+    double debye_length;         /* salt: Debye_length */
+    double surface_charge;       /* Particle_spec[0].Surface_charge */
+    int    e_field;              /* Electric_field: 0 OFF, 1 DC, 2 AC */
+    double e_ext[3];             /* Ex, Ey, Ez */
+    double e_frequency;          /* AC: Frequency */
 } spm_params;
 
 typedef struct spm_ctx spm_ctx;
@@ -134,6 +147,10 @@ int spm_get_time(spm_ctx *ctx, int *ts, double *time);
  * apparent}.  For a Lees-Edwards run spm_get_velocity returns the oblique
  * (contravariant) velocity on the sheared grid. */
 int spm_get_shear_state(spm_ctx *ctx, double *degree_oblique, double stress[8]);
+/* Electrolyte runs: the k-space concentration of ion species `species`
+ * (0: the counterion of a saltfree run or the positive ion; 1: the negative
+ * ion of a salt run), in the reference's r2c layout (Concentration[n]). */
+int spm_get_concentration(spm_ctx *ctx, int species, double *conc_k);
 /* Checkpoint / restart (the reference's restart files, resume.cxx:10-74,
  * 381-588): writes, or reads back into a context created with the same
  * parameters, every piece of device state the next steps read (zeta with its

@@ -16,6 +16,7 @@ SPM_OK = 0
 SPM_PARTICLE_WORDS = 44
 SPM_EQ_NAVIER_STOKES = 0
 SPM_EQ_LEES_EDWARDS = 1
+SPM_EQ_ELECTROLYTE = 2
 SPM_PREC_FP64 = 0
 SPM_PREC_FP32_MIXED = 1
 
@@ -40,6 +41,10 @@ class SpmParams(C.Structure):
         ("body_force", C.c_double * 3),
         ("precision", C.c_int),
         ("mt_seed", C.c_uint),
+        ("dielectric", C.c_double), ("salt", C.c_int), ("init_pb", C.c_int),
+        ("valency", C.c_double * 2), ("onsager", C.c_double * 2), ("debye_length", C.c_double),
+        ("surface_charge", C.c_double), ("e_field", C.c_int), ("e_ext", C.c_double * 3),
+        ("e_frequency", C.c_double),
     ]
 
 
@@ -104,6 +109,7 @@ _SIGS = {
     "spm_get_phi": (C.c_int, [_P, _D]),
     "spm_get_time": (C.c_int, [_P, C.POINTER(C.c_int), _D]),
     "spm_get_shear_state": (C.c_int, [_P, _D, _D]),
+    "spm_get_concentration": (C.c_int, [_P, C.c_int, _D]),
     "spm_save_state": (C.c_int, [_P, C.c_char_p]),
     "spm_load_state": (C.c_int, [_P, C.c_char_p]),
     "spm_avs_open": (C.c_int, [_P, C.c_char_p, C.c_char_p, C.c_int]),

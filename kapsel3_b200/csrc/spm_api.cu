@@ -23,6 +23,7 @@
 #include "spm_fft_plan.cuh"
 #include "spm_kernels.cuh"
 #include "spm_le.cuh"
+#include "spm_electrolyte.cuh"
 
 using namespace spm;
 
@@ -139,8 +140,12 @@ enum Slot { Z0 = 0, Z1, U0, U1, U2, A0, A1, UP0, UP1, UP2, PHIS, NSLOT };
 constexpr int ZL0 = NSLOT, ZL1 = NSLOT + 1;
 
 // Field slots a run needs.
+// Electrolyte runs: concentrations, solute right-hand sides, grad psi,
+// solute flux, surface normal, charge, raw phi, work, solute velocity
+constexpr int EL_EXTRA_SLOTS = 19;
 int slots_for(const spm_params &p) {
     if (p.equation == SPM_EQ_LEES_EDWARDS) return NSLOT + LE_EXTRA_SLOTS;
+    if (p.equation == SPM_EQ_ELECTROLYTE) return NSLOT + EL_EXTRA_SLOTS;
     return p.precision == SPM_PREC_FP32_MIXED ? NSLOT + 2 : NSLOT;
 }
 
@@ -186,6 +191,7 @@ struct spm_ctx {
     long long    launches = 0;
     int          sm_count = 148;
     LEState      le{};
+    ELState      el{};
     // optional CUDA-event timing of the strided FFT passes inside real steps
     bool                     prof_on = false;
     std::vector<cudaEvent_t> prof_ev;
@@ -235,6 +241,12 @@ struct spm_ctx {
     }
 };
 
+#define SPM_TRY(expr)                   \
+    do {                                \
+        int _rc = (expr);               \
+        if (_rc != SPM_OK) return _rc;  \
+    } while (0)
+
 #define LAUNCH(ctx, kern, grid, block, smem, ...)                                           \
     do {                                                                                    \
         kern<<<(grid), (block), (smem), (ctx)->st>>>(__VA_ARGS__);                          \
@@ -256,7 +268,21 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
     if (p.n_particles < 0) return fail(SPM_ERR_ARG, "negative particle count");
     if (!(p.dx > 0) || !(p.rho > 0) || !(p.eta > 0) || !(p.dt > 0)) return fail(SPM_ERR_ARG, "DX, RHO, ETA, dt must be > 0");
     if (p.precision != SPM_PREC_FP64 && p.precision != SPM_PREC_FP32_MIXED) return fail(SPM_ERR_ARG, "bad precision");
-    if (p.equation != SPM_EQ_NAVIER_STOKES && p.equation != SPM_EQ_LEES_EDWARDS) return fail(SPM_ERR_ARG, "bad equation");
+    if (p.equation != SPM_EQ_NAVIER_STOKES && p.equation != SPM_EQ_LEES_EDWARDS && p.equation != SPM_EQ_ELECTROLYTE)
+        return fail(SPM_ERR_ARG, "bad equation");
+    if (p.equation == SPM_EQ_ELECTROLYTE) {
+        // Init_rho_ion's checks (operate_electrolyte.cxx:668-720)
+        if (p.precision != SPM_PREC_FP64) return fail(SPM_ERR_ARG, "Electrolyte runs are FP64 only");
+        if (p.surface_charge == 0.0) return fail(SPM_ERR_ARG, "Electrolyte needs a nonzero Surface_charge");
+        if (!(p.dielectric > 0.0)) return fail(SPM_ERR_ARG, "Dielectric_cst must be > 0");
+        if (p.init_pb) return fail(SPM_ERR_ARG, "INIT_profile Poisson_Boltzmann is not supported (Uniform only)");
+        if (p.salt == 0 && !(p.valency[0] * p.surface_charge < 0.0))
+            return fail(SPM_ERR_ARG, "Valency_counterion must have the opposite sign of Surface_charge");
+        if (p.salt == 1 && !(p.valency[0] > 0.0 && p.valency[1] < 0.0))
+            return fail(SPM_ERR_ARG, "salt needs Valency_positive_ion > 0 and Valency_negative_ion < 0");
+        if (p.salt == 1 && !(p.debye_length > 0.0)) return fail(SPM_ERR_ARG, "Debye_length must be > 0");
+        if (p.e_field < 0 || p.e_field > 2) return fail(SPM_ERR_ARG, "bad Electric_field");
+    }
     if (p.lj_powers < 0 || p.lj_powers > 2) return fail(SPM_ERR_ARG, "LJ_powers must be 12:6, 24:12 or 36:18");
     g.nx  = 1 << p.npx;
     g.ny  = 1 << p.npy;
@@ -690,11 +716,19 @@ int initialize_impl(spm_ctx *c) {
 
 }  // namespace
 #include "spm_le_step.inc"
+#include "spm_electrolyte.inc"
 namespace {
 
 template <typename T>
 int step_impl(spm_ctx *c) {
     if (c->P.equation == SPM_EQ_LEES_EDWARDS) return step_le_impl<T>(c);
+    if (c->P.equation == SPM_EQ_ELECTROLYTE) {
+        const int rc = step_el<T>(c);
+        if (rc != SPM_OK) return rc;
+        c->ts++;
+        c->time += c->ph.dt;
+        return SPM_OK;
+    }
     return step_ns<T>(c);
 }
 
@@ -860,6 +894,38 @@ int download_particles(spm_ctx *c, double *rec) {
 
 void avs_release(spm_ctx *c);
 
+// Electrolyte run constants from the parameters (Init_rho_ion,
+// operate_electrolyte.cxx:667-720, 490-520; Elementary_charge = 1,
+// input.cxx:293; Angular_Frequency = PI2 Frequency, input.cxx:514).
+void el_init_state(ELState &el, const spm_params &p) {
+    const double e = 1.0;
+    el.enabled     = 1;
+    el.nspec       = p.salt ? 2 : 1;
+    el.iepsilon    = 1.0 / p.dielectric;
+    el.qe          = p.surface_charge * e;
+    el.abs_q       = 0.0;
+    for (int n = 0; n < p.n_particles; n++) el.abs_q += fabs(el.qe);
+    const double surface_ion_number = -p.surface_charge * p.n_particles;
+    for (int n = 0; n < el.nspec; n++) {
+        el.val_e[n] = p.valency[n] * e;
+        el.ons[n]   = p.onsager[n];
+    }
+    if (el.nspec == 1) {
+        el.counterion_number = surface_ion_number / p.valency[0];
+    } else {
+        const double qn = p.surface_charge * (double)p.n_particles;
+        el.ion_number[0] = p.surface_charge < 0. ? fabs(qn / p.valency[0]) : 0.0;
+        el.ion_number[1] = p.surface_charge > 0. ? fabs(qn / p.valency[1]) : 0.0;
+        const double rho_inf = p.kbt * p.dielectric / ((e * p.debye_length) * (e * p.debye_length));
+        el.rho_inf[0]        = rho_inf / (p.valency[0] * (p.valency[0] - p.valency[1]));
+        el.rho_inf[1]        = -rho_inf / (p.valency[1] * (p.valency[0] - p.valency[1]));
+    }
+    el.e_on  = p.e_field != 0;
+    el.e_ac  = p.e_field == 2;
+    for (int d = 0; d < 3; d++) el.e_ext[d] = el.e_on ? p.e_ext[d] : 0.0;
+    el.e_omega = 2. * M_PI * p.e_frequency;
+}
+
 void destroy_ctx(spm_ctx *c) {
     if (!c) return;
     avs_release(c);
@@ -878,6 +944,8 @@ void destroy_ctx(spm_ctx *c) {
     dev_free(c->le.dev);
     dev_free(c->le.ppart);
     dev_free(c->le.partial);
+    dev_free(c->el.dev);
+    dev_free(c->el.partial);
     if (c->side) cudaStreamDestroy(c->side);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
@@ -1025,6 +1093,15 @@ int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *
     c->ps.mdf                   = c->ps.torque_r_previous + (size_t)np * 3;
     c->ps.lj_stress             = c->ps.mdf + (size_t)np * 3;
     le_init(c->le, c->g, c->ph, p);
+    if (p.equation == SPM_EQ_ELECTROLYTE) {
+        el_init_state(c->el, p);
+        if (dev_alloc((void **)&c->el.dev, kElScalars * sizeof(double)) != cudaSuccess ||
+            dev_alloc((void **)&c->el.partial, (size_t)c->grid_blocks() * sizeof(double)) != cudaSuccess) {
+            destroy_ctx(c);
+            return fail(SPM_ERR_NOMEM, "Electrolyte buffers");
+        }
+        cudaMemset(c->el.dev, 0, kElScalars * sizeof(double));
+    }
     if (c->le.enabled) {
         if (dev_alloc((void **)&c->le.dev, sizeof(LEDev)) != cudaSuccess ||
             dev_alloc((void **)&c->le.ppart, (size_t)np * 6 * sizeof(double)) != cudaSuccess ||
@@ -1117,6 +1194,7 @@ int spm_initialize(spm_ctx *c, const double *particles_host) {
     le_reset(c->le);
     rc = c->fp64() ? initialize_impl<double>(c) : initialize_impl<float>(c);
     if (rc != SPM_OK) return rc;
+    if (c->el.enabled && (rc = el_init_ions<double>(c)) != SPM_OK) return rc;
     return check_device_error(c);
 }
 

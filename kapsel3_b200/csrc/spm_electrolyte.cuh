@@ -1,0 +1,408 @@
+// Electrolyte (charged colloids in a solution of mobile ions): the device
+// kernels of the reference's spectral Electrolyte step
+// (NSsolute_solver_Euler and Rhs_NS_Nernst_Planck, fluid_solver.cxx:171-346;
+// operate_electrolyte.cxx; solute_rhs.cxx; the Electrolyte branch of
+// Time_evolution_hydro, sp_3d_ns.cxx:75-100).  Fields are FP64 rows of
+// 2*hnzp reals (real space) or hnzp complex (k space), as for the
+// Navier_Stokes step.
+#pragma once
+
+#include "spm_kernels.cuh"
+
+namespace spm {
+
+// Run constants of an Electrolyte context (Init_rho_ion,
+// operate_electrolyte.cxx:667-791; input.cxx:834-930).
+struct ELState {
+    int     enabled = 0;
+    int     nspec   = 0;           // 1: saltfree counterions, 2: positive and negative ions
+    double  val_e[2] = {0, 0};     // Valency_e = Valency * Elementary_charge
+    double  ons[2]   = {0, 0};     // Onsager coefficients
+    double  iepsilon = 0.0;        // 1 / Dielectric_cst
+    double  qe       = 0.0;        // Surface_charge_e of the particle species
+    double  abs_q    = 0.0;        // sum over particles of |Surface_charge_e|
+    double  counterion_number = 0; // saltfree: Surface_ion_number / Valency_counterion
+    double  ion_number[2] = {0, 0};// salt: positive / negative ion numbers from the surface charge
+    double  rho_inf[2]    = {0, 0};// salt: Rho_inf of each species
+    int     e_on    = 0;           // External_field
+    int     e_ac    = 0;           // AC field
+    double  e_ext[3] = {0, 0, 0};  // E_ext
+    double  e_omega = 0.0;         // Angular_Frequency = 2 pi Frequency
+    double *dev     = nullptr;     // device scalars (kEl*)
+    double *partial = nullptr;     // per-CTA partial sums of the field reductions
+};
+// device scalars
+constexpr int kElTotal  = 0;  // [0, 1]: Total_solute of each species
+constexpr int kElQSum   = 2;  // sum of |surface charge field|
+constexpr int kElCSum   = 3;  // [3, 4]: (1 - phi) c sums of each species
+constexpr int kElVolume = 5;  // sum of (1 - phi)
+constexpr int kElScalars = 8;
+
+// Total_solute[n] = (1 - phi) c sum * DX3 (Count_single_solute)
+__global__ void k_el_total(double *dev, int n, double dx3) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) dev[kElTotal + n] = dev[kElCSum + n] * dx3;
+}
+
+// |phi_s'(x)| of the compact sine profile (DPhi_compact_sin, profile.h:164-173)
+__device__ __forceinline__ double dphi_compact_sin(double x, double radius, double xi) {
+    const double hxi   = xi * .5;
+    const double ixi   = 1. / xi;
+    const double dmy_x = radius - x;
+    if (fabs(dmy_x) < hxi) return M_PI * .5 * ixi * cos(M_PI * dmy_x * ixi);
+    return 0.;
+}
+
+// Make_phi_qq_particle (operate_electrolyte.cxx:173-208): phi += Phi and
+// surface += Surface_charge_e * |phi_s'| over each particle's stencil.
+template <typename T>
+__global__ void s_el_phi_qq(Grid g, Phys ph, const double *__restrict__ x, const int *__restrict__ cells, int ncells,
+                            T *__restrict__ phi, T *__restrict__ surface, double qe, unsigned int *err) {
+    const int p = blockIdx.y;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ph.np || m >= ncells) return;
+    const double xp[3] = {x[3 * p], x[3 * p + 1], x[3 * p + 2]};
+    if (!particle_in_box(ph, xp)) {
+        if (m == 0) atomicOr(err, (unsigned)SPM_DEVERR_PARTICLE_OUT_OF_BOX);
+        return;
+    }
+    StencilPoint s;
+    stencil_point(g, ph, xp, cells[m], s);
+    const double v  = phi_prof(s.dist, ph.radius, ph.hxi, g.dx);
+    const double dq = qe * dphi_compact_sin(s.dist, ph.radius, 2.0 * ph.hxi);
+    if (v != 0.0) atomicAdd(&phi[s.idx], (T)v);
+    if (dq != 0.0) atomicAdd(&surface[s.idx], (T)dq);
+}
+
+// Make_surface_normal (make_phi.cxx:17-55): sum of r / |r| over the stencil
+// cells with ||r| - RADIUS| < XI / 2, r the cell offset from the particle.
+template <typename T>
+__global__ void s_el_surface_normal(Grid g, Phys ph, const double *__restrict__ x, const int *__restrict__ cells,
+                                    int ncells, T *__restrict__ n0, T *__restrict__ n1, T *__restrict__ n2) {
+    const int p = blockIdx.y;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ph.np || m >= ncells) return;
+    const double xp[3] = {x[3 * p], x[3 * p + 1], x[3 * p + 2]};
+    if (!particle_in_box(ph, xp)) return;
+    StencilPoint s;
+    stencil_point(g, ph, xp, cells[m], s);
+    const double dmy_r = sqrt(s.r[0] * s.r[0] + s.r[1] * s.r[1] + s.r[2] * s.r[2]);
+    const double dmy   = fabs(dmy_r - ph.radius);
+    if (dmy < ph.hxi) {
+        const double ir = 1. / dmy_r;
+        atomicAdd(&n0[s.idx], (T)(s.r[0] * ir));
+        atomicAdd(&n1[s.idx], (T)(s.r[1] * ir));
+        atomicAdd(&n2[s.idx], (T)(s.r[2] * ir));
+    }
+}
+
+// Sums over the real cells (i < NX, j < NY, k < NZ), one partial per CTA:
+// mode 0: (1 - phi) a (Count_single_solute), 1: |a|, 2: (1 - phi).
+template <typename T>
+__global__ void __launch_bounds__(256) r_el_sum(Grid g, const T *__restrict__ a, const T *__restrict__ phi, int mode,
+                                                double *__restrict__ partial) {
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    double       acc    = 0.0;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if ((int)(idx % rowlen) >= g.nz) continue;
+        if (mode == 0)
+            acc += (1. - (double)phi[idx]) * (double)a[idx];
+        else if (mode == 1)
+            acc += fabs((double)a[idx]);
+        else
+            acc += (1. - (double)phi[idx]);
+    }
+    __shared__ double red[8];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+        partial[blockIdx.x] = t;
+    }
+}
+// out = sum of the nb partials (one thread, fixed order)
+__global__ void k_el_sum_finish(const double *__restrict__ partial, int nb, double *__restrict__ out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double t = 0.0;
+    for (int b = 0; b < nb; b++) t += partial[b];
+    *out = t;
+}
+
+// a *= s over the real cells, s = num / (den * dx3) from device scalars
+// (the surface-charge normalisation of Make_phi_qq_particle and the solute
+// rescale of Rescale_solute, solute_rhs.cxx:91-116; the latter on every
+// element of a k-space field: scale_all).
+template <typename T>
+__global__ void r_el_scale(Grid g, T *__restrict__ a, double num, const double *__restrict__ num_dev,
+                           const double *__restrict__ den_dev, double dx3, int scale_all) {
+    const double s      = (num_dev ? *num_dev : num) / (*den_dev * dx3);
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if (!scale_all && (int)(idx % rowlen) >= g.nz) continue;
+        a[idx] = (T)((double)a[idx] * s);
+    }
+}
+
+// charge += Valency_e c (1 - phi) over the real cells (Conc_k2charge_field)
+template <typename T>
+__global__ void r_el_charge_add(Grid g, T *__restrict__ charge, const T *__restrict__ c, const T *__restrict__ phi,
+                                double val_e) {
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if ((int)(idx % rowlen) >= g.nz) continue;
+        charge[idx] = (T)((double)charge[idx] + val_e * (double)c[idx] * (1. - (double)phi[idx]));
+    }
+}
+
+// a = value on the real cells (the uniform initial ion density)
+template <typename T>
+__global__ void r_el_fill(Grid g, T *__restrict__ a, double value) {
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x)
+        a[idx] = (int)(idx % rowlen) < g.nz ? (T)value : (T)0;
+}
+
+// Coulomb potential of a charge field in k space
+// (Charge_field_k2Coulomb_potential_k_PBC, operate_electrolyte.cxx:69-81):
+// a *= IK2 / Dielectric_cst; with `truncate` modes outside the 2/3 box are
+// zeroed (Truncate_two_third_rule).
+template <typename T>
+__global__ void k_el_poisson(Grid g, cplx<T> *__restrict__ a, double iepsilon, int truncate) {
+    const size_t n = g.field_elems_c();
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        KPoint p;
+        size_t row;
+        if (!k_point(g, idx, p, row)) continue;
+        const double k2sum = p.kx * p.kx + p.ky * p.ky + p.kz * p.kz;
+        const double f     = (k2sum > 0.0 ? 1.0 / k2sum : 0.0) * iepsilon;
+        cplx<T>      v     = a[idx];
+        v.re               = (T)((double)v.re * f);
+        v.im               = (T)((double)v.im * f);
+        if (truncate && !p.keep) v = cplx<T>{0, 0};
+        a[idx] = v;
+    }
+}
+
+// Gradient in k space of s a (A_k2da_k, fft_wrapper.cxx:200-225): g_d =
+// (-k_d s a.im, k_d s a.re); at k = 0 the real parts get -e_d
+// (Add_constant_field_k, fluid_solver.cxx:221-231, e_d = E_ext NX NY NZ or
+// the AC amplitude; 0 without a field).
+template <typename T>
+__global__ void k_el_grad(Grid g, const cplx<T> *__restrict__ a, cplx<T> *__restrict__ g0, cplx<T> *__restrict__ g1,
+                          cplx<T> *__restrict__ g2, double s, int scaled, double e0, double e1, double e2) {
+    const size_t n = g.field_elems_c();
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        KPoint p;
+        size_t row;
+        if (!k_point(g, idx, p, row)) {
+            g0[idx] = g1[idx] = g2[idx] = cplx<T>{0, 0};
+            continue;
+        }
+        double re = (double)a[idx].re, im = (double)a[idx].im;
+        if (scaled) re = s * re, im = s * im;
+        cplx<T> d0 = {(T)(-p.kx * im), (T)(p.kx * re)};
+        cplx<T> d1 = {(T)(-p.ky * im), (T)(p.ky * re)};
+        cplx<T> d2 = {(T)(-p.kz * im), (T)(p.kz * re)};
+        if (idx == 0) {
+            d0.re = (T)((double)d0.re - e0);
+            d1.re = (T)((double)d1.re - e1);
+            d2.re = (T)((double)d2.re - e2);
+        }
+        g0[idx] = d0, g1[idx] = d1, g2[idx] = d2;
+    }
+}
+
+// The kz = 0 and kz = NZ/2 planes as the reference's inverse transform reads
+// them.  Its Ooura rdft3d takes a packed half spectrum: rdft3dsort(-1)
+// (fftsg3d.c:632-655) keeps, on kz = 0, the rows 0 < j < NY/2 and i <= NX/2 of
+// the rows j = 0, NY/2; on kz = NZ/2, the rows j > NY/2 and i > NX/2 of the
+// rows j = 0, NY/2; at the four self-conjugate points only the real part.
+// Every other entry of the two planes is implied as the conjugate of its
+// partner (-i, -j).  A field that is not Hermitian there (the gradient i k a
+// at the Nyquist wavenumbers, whose partner has the same +N/2) is rewritten
+// that way, after which any inverse real transform gives the reference's
+// result.  Discarded entries read only kept partners, so one pass is
+// race-free.  One thread per (plane, i, j), three fields.
+template <typename T>
+__global__ void k_el_hermitian_planes(Grid g, cplx<T> *__restrict__ f0, cplx<T> *__restrict__ f1,
+                                      cplx<T> *__restrict__ f2) {
+    const int n = 2 * g.nx * g.ny;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int plane = t / (g.nx * g.ny);
+    const int i     = (t / g.ny) % g.nx;
+    const int j     = t % g.ny;
+    const int h1 = g.nx / 2, h2 = g.ny / 2;
+    const int kz       = plane ? g.hnz - 1 : 0;
+    const bool edge_j  = (j == 0 || j == h2);
+    const bool self_cj = edge_j && (i == 0 || i == h1);
+    bool       drop;
+    if (plane == 0)
+        drop = j > h2 || (edge_j && i > h1);
+    else
+        drop = (j > 0 && j < h2) || (edge_j && i > 0 && i < h1);
+    const size_t idx = ((size_t)i * g.ny + j) * g.hnzp + kz;
+    cplx<T>     *fs[3] = {f0, f1, f2};
+    if (drop) {
+        const size_t pidx = ((size_t)((g.nx - i) % g.nx) * g.ny + (g.ny - j) % g.ny) * g.hnzp + kz;
+        for (int d = 0; d < 3; d++) {
+            const cplx<T> v = fs[d][pidx];
+            fs[d][idx]      = cplx<T>{v.re, -v.im};
+        }
+    } else if (self_cj) {
+        for (int d = 0; d < 3; d++) fs[d][idx].im = (T)0;
+    }
+}
+
+// Solute flux of one species in real space (Rhs_NS_solute,
+// fluid_solver.cxx:190-206): on entry f = diffusion flux; adds the
+// electro-migration term c Onsager (grad psi Valency_e)
+// (Solute_solver_rhs_nonlinear_x_single), removes the component along the
+// surface normal (Solute_impermeability; applying it once per cell is the
+// same projection the reference applies once per particle whose stencil
+// holds the cell), then adds the advection flux -c u (Add_advection_flux).
+template <typename T>
+__global__ void r_el_flux(Grid g, T *__restrict__ f0, T *__restrict__ f1, T *__restrict__ f2, const T *__restrict__ c,
+                          const T *__restrict__ gp0, const T *__restrict__ gp1, const T *__restrict__ gp2,
+                          const T *__restrict__ n0, const T *__restrict__ n1, const T *__restrict__ n2,
+                          const T *__restrict__ u0, const T *__restrict__ u1, const T *__restrict__ u2, double ons,
+                          double val_e) {
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if ((int)(idx % rowlen) >= g.nz) continue;
+        const double cc   = (double)c[idx];
+        double       f[3] = {(double)f0[idx], (double)f1[idx], (double)f2[idx]};
+        const double gp[3] = {(double)gp0[idx], (double)gp1[idx], (double)gp2[idx]};
+        for (int d = 0; d < 3; d++) f[d] += cc * (ons * (gp[d] * val_e));
+        const double nn[3] = {(double)n0[idx], (double)n1[idx], (double)n2[idx]};
+        double       norm2 = 0.;
+        for (int d = 0; d < 3; d++) norm2 += nn[d] * nn[d];
+        if (norm2 > 0.) {
+            double dmy = 0.;
+            for (int d = 0; d < 3; d++) dmy += f[d] * nn[d];
+            dmy /= norm2;
+            for (int d = 0; d < 3; d++) f[d] -= nn[d] * dmy;
+        }
+        const double uu[3] = {(double)u0[idx], (double)u1[idx], (double)u2[idx]};
+        for (int d = 0; d < 3; d++) f[d] += cc * -uu[d];
+        f0[idx] = (T)f[0], f1[idx] = (T)f[1], f2[idx] = (T)f[2];
+    }
+}
+
+// Divergence in k space (U_k2divergence_k, fft_wrapper.cxx:867-891)
+template <typename T>
+__global__ void k_el_div(Grid g, const cplx<T> *__restrict__ f0, const cplx<T> *__restrict__ f1,
+                         const cplx<T> *__restrict__ f2, cplx<T> *__restrict__ div) {
+    const size_t n = g.field_elems_c();
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        KPoint p;
+        size_t row;
+        if (!k_point(g, idx, p, row)) {
+            div[idx] = cplx<T>{0, 0};
+            continue;
+        }
+        const cplx<T> a = f0[idx], b = f1[idx], c = f2[idx];
+        div[idx] = cplx<T>{(T)(-(p.kx * (double)a.im + p.ky * (double)b.im + p.kz * (double)c.im)),
+                           (T)(p.kx * (double)a.re + p.ky * (double)b.re + p.kz * (double)c.re)};
+    }
+}
+
+// Explicit Euler of NSsolute_solver_Euler over the retained modes
+// (Field_solver_Euler, fluid_solver.cxx:120-136): zeta += dt (f_ns -
+// nu K2 zeta) with f_ns the zeta form of the advection products
+// (U2advection_k, operate_omega.cxx:12-98; Add_zeta_viscous_term,
+// operate_omega.cxx:157-169), and c_n += dt rhs_n for each species.
+template <typename T>
+__global__ void k_el_update(Grid g, cplx<T> *__restrict__ z0p, cplx<T> *__restrict__ z1p,
+                            const cplx<T> *__restrict__ p_u2u3, const cplx<T> *__restrict__ p_u3u1,
+                            const cplx<T> *__restrict__ p_u1u2, const cplx<T> *__restrict__ p_a0,
+                            const cplx<T> *__restrict__ p_a1, double nu, double dt, cplx<T> *__restrict__ c0,
+                            const cplx<T> *__restrict__ r0, cplx<T> *__restrict__ c1, const cplx<T> *__restrict__ r1,
+                            int nspec) {
+    const size_t n = g.field_elems_c();
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        KPoint p;
+        size_t row;
+        if (!k_point(g, idx, p, row) || !p.keep) continue;
+        const T k1 = (T)p.kx, k2 = (T)p.ky, k3 = (T)p.kz;
+        const T k1k2 = k1 * k2, k2k3 = k2 * k3, k3k1 = k3 * k1;
+        const T c0k = (k3 - k2) * (k3 + k2), c1k = (k1 - k3) * (k1 + k3), c2k = (k2 - k1) * (k2 + k1);
+        const cplx<T> u2u3 = p_u2u3[idx], u3u1 = p_u3u1[idx], u1u2 = p_u1u2[idx];
+        const cplx<T> a0 = p_a0[idx], a1 = p_a1[idx];
+        const cplx<T> a2 = {-a1.re - a0.re, -a1.im - a0.im};
+        cplx<T> om[3];
+        om[0] = {-(k2k3 * a0.re + c0k * u2u3.re + k3k1 * u1u2.re - k1k2 * u3u1.re),
+                 -(k2k3 * a0.im + c0k * u2u3.im + k3k1 * u1u2.im - k1k2 * u3u1.im)};
+        om[1] = {-(k3k1 * a1.re + c1k * u3u1.re + k1k2 * u2u3.re - k2k3 * u1u2.re),
+                 -(k3k1 * a1.im + c1k * u3u1.im + k1k2 * u2u3.im - k2k3 * u1u2.im)};
+        om[2] = {-(k1k2 * a2.re + c2k * u1u2.re + k2k3 * u3u1.re - k3k1 * u2u3.re),
+                 -(k1k2 * a2.im + c2k * u1u2.im + k2k3 * u3u1.im - k3k1 * u2u3.im)};
+        cplx<T> f0, f1;
+        omega_to_zeta<T>(p, om, f0, f1);
+        const T       nk2 = (T)(nu * (p.kx * p.kx + p.ky * p.ky + p.kz * p.kz));
+        cplx<T>       z0 = z0p[idx], z1 = z1p[idx];
+        const cplx<T> r0z = {f0.re + -(nk2 * z0.re), f0.im + -(nk2 * z0.im)};
+        const cplx<T> r1z = {f1.re + -(nk2 * z1.re), f1.im + -(nk2 * z1.im)};
+        z0.re += (T)dt * r0z.re, z0.im += (T)dt * r0z.im;
+        z1.re += (T)dt * r1z.re, z1.im += (T)dt * r1z.im;
+        z0p[idx] = z0, z1p[idx] = z1;
+        cplx<T> c = c0[idx];
+        c.re += (T)dt * r0[idx].re, c.im += (T)dt * r0[idx].im;
+        c0[idx] = c;
+        if (nspec > 1) {
+            c = c1[idx];
+            c.re += (T)dt * r1[idx].re, c.im += (T)dt * r1[idx].im;
+            c1[idx] = c;
+        }
+    }
+}
+
+// Coulomb body force on the fluid and its velocity kick
+// (Make_Coulomb_force_x_on_fluid, operate_electrolyte.cxx:83-171, then
+// u += f dt / RHO, sp_3d_ns.cxx:85-96): f_d = charge (-grad_d psi + E_d).
+template <typename T>
+__global__ void r_el_coulomb(Grid g, const T *__restrict__ charge, const T *__restrict__ gp0, const T *__restrict__ gp1,
+                             const T *__restrict__ gp2, T *__restrict__ u0, T *__restrict__ u1, T *__restrict__ u2,
+                             int e_on, double e0, double e1, double e2, double dmy) {
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if ((int)(idx % rowlen) >= g.nz) continue;
+        const double q  = (double)charge[idx];
+        double       ef = -(double)gp0[idx];
+        if (e_on) ef += e0;
+        u0[idx] = (T)((double)u0[idx] + q * ef * dmy);
+        ef = -(double)gp1[idx];
+        if (e_on) ef += e1;
+        u1[idx] = (T)((double)u1[idx] + q * ef * dmy);
+        ef = -(double)gp2[idx];
+        if (e_on) ef += e2;
+        u2[idx] = (T)((double)u2[idx] + q * ef * dmy);
+    }
+}
+
+// f = up - phi u with the raw (unclamped) phi sum: on the Electrolyte step
+// the phi array handed to Make_f_particle_dt_sole is the one Rescale_solute
+// last filled by Make_phi_particle (solute_rhs.cxx:98-99).
+template <typename T>
+__global__ void r_el_make_f(Grid g, T *__restrict__ up0, T *__restrict__ up1, T *__restrict__ up2,
+                            const T *__restrict__ u0, const T *__restrict__ u1, const T *__restrict__ u2,
+                            const T *__restrict__ phi) {
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if ((int)(idx % rowlen) >= g.nz) continue;
+        const T ph = phi[idx];
+        up0[idx]   = up0[idx] - ph * u0[idx];
+        up1[idx]   = up1[idx] - ph * u1[idx];
+        up2[idx]   = up2[idx] - ph * u2[idx];
+    }
+}
+
+}  // namespace spm

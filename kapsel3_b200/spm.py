@@ -19,7 +19,7 @@ from typing import Dict, Optional, Tuple
 import numpy as np
 
 from . import _native as N
-from .udf import EQ_LE, SPMConfig
+from .udf import EQ_EL, EQ_LE, SPMConfig
 
 RECORD = [("x", 3), ("x_nopbc", 3), ("v", 3), ("v_old", 3), ("omega", 3), ("omega_old", 3),
           ("q", 4), ("q_old", 4), ("f_hydro", 3), ("f_hydro_previous", 3),
@@ -58,7 +58,8 @@ def params_from_config(cfg: SPMConfig, precision: int = N.SPM_PREC_FP64,
     p.npx, p.npy, p.npz = cfg.npx, cfg.npy, cfg.npz
     p.dx, p.rho, p.eta, p.kbt = cfg.dx, cfg.rho, cfg.eta, cfg.kbt
     p.alpha_v, p.alpha_o = cfg.alpha_v, cfg.alpha_o
-    p.equation = N.SPM_EQ_LEES_EDWARDS if cfg.equation == EQ_LE else N.SPM_EQ_NAVIER_STOKES
+    p.equation = {EQ_LE: N.SPM_EQ_LEES_EDWARDS, EQ_EL: N.SPM_EQ_ELECTROLYTE}.get(cfg.equation,
+                                                                                N.SPM_EQ_NAVIER_STOKES)
     p.shear_rate = cfg.shear_rate
     p.n_particles = cfg.n_particles
     p.mass_ratio = cfg.mass_ratio
@@ -73,6 +74,14 @@ def params_from_config(cfg: SPMConfig, precision: int = N.SPM_PREC_FP64,
     p.dt = cfg.dt
     p.precision = precision
     p.mt_seed = mt_seed
+    p.dielectric, p.salt, p.init_pb = cfg.dielectric, int(cfg.salt), int(cfg.init_pb)
+    for n in range(2):
+        p.valency[n], p.onsager[n] = float(cfg.valency[n]), float(cfg.onsager[n])
+    p.debye_length, p.surface_charge = cfg.debye_length, cfg.surface_charge
+    p.e_field = {"OFF": 0, "DC": 1, "AC": 2}[cfg.e_field]
+    for d in range(3):
+        p.e_ext[d] = float(cfg.e_ext[d])
+    p.e_frequency = cfg.e_frequency
     return p
 
 
@@ -101,13 +110,16 @@ def config_from_udf(path: str) -> Tuple[SPMConfig, Dict[str, np.ndarray]]:
     cfg = SPMConfig(
         npx=p.npx, npy=p.npy, npz=p.npz, dx=p.dx, rho=p.rho, eta=p.eta, kbt=p.kbt,
         alpha_v=p.alpha_v, alpha_o=p.alpha_o,
-        equation=EQ_LE if p.equation == N.SPM_EQ_LEES_EDWARDS else "Navier_Stokes",
+        equation={N.SPM_EQ_LEES_EDWARDS: EQ_LE, N.SPM_EQ_ELECTROLYTE: EQ_EL}.get(p.equation, "Navier_Stokes"),
         shear_rate=p.shear_rate, n_particles=p.n_particles, mass_ratio=p.mass_ratio, a=p.a, a_xi=p.a_xi,
         epsilon=p.epsilon, lj_powers=("12:6", "24:12", "36:18")[p.lj_powers],
         lj_truncate={1: "ON", 0: "OFF", -1: "NONE"}[p.lj_truncate], rotation=bool(p.rotation),
         fix_cell=tuple(bool(p.fix_cell[d]) for d in range(3)), dt=p.dt,
         gts=int(kv.get("output.GTS", 1)), num_snap=int(kv.get("output.Num_snap", 1)),
-        body_force=tuple(float(p.body_force[d]) for d in range(3)))
+        body_force=tuple(float(p.body_force[d]) for d in range(3)),
+        dielectric=p.dielectric, salt=bool(p.salt), init_pb=bool(p.init_pb), valency=tuple(p.valency),
+        onsager=tuple(p.onsager), debye_length=p.debye_length, surface_charge=p.surface_charge,
+        e_field=("OFF", "DC", "AC")[p.e_field], e_ext=tuple(p.e_ext), e_frequency=p.e_frequency)
     return cfg, unpack_particles(rec[:p.n_particles])
 
 
@@ -223,6 +235,12 @@ class SPMRun:
         ts, t = C.c_int(), C.c_double()
         N.check(self.L.spm_get_time(self.h, C.byref(ts), C.byref(t)), "spm_get_time")
         return ts.value, t.value
+
+    def concentration(self, species: int = 0) -> np.ndarray:
+        """k-space concentration of one ion species of an Electrolyte run."""
+        a = self._kfield()
+        N.check(self.L.spm_get_concentration(self.h, int(species), N.dptr(a)), "spm_get_concentration")
+        return self._as_k(a)
 
     def shear_state(self):
         deg, st = C.c_double(), np.zeros(8)

@@ -27,6 +27,7 @@ import numpy as np
 
 EQ_NS = "Navier_Stokes"
 EQ_LE = "Shear_Navier_Stokes_Lees_Edwards"
+EQ_EL = "Electrolyte"
 
 
 @dataclasses.dataclass
@@ -57,6 +58,17 @@ class SPMConfig:
     gts: int = 1                 # output.GTS
     num_snap: int = 1            # output.Num_snap (MSTEP = GTS*Num_snap)
     body_force: tuple = (0.0, 0.0, 0.0)  # constant force on every particle
+    # Electrolyte (constitutive_eq.Electrolyte, input.cxx:834-930)
+    dielectric: float = 1.0      # Dielectric_cst
+    salt: bool = False           # Add_salt: salt (two ion species) or saltfree (counterions)
+    init_pb: bool = False        # INIT_profile: Poisson_Boltzmann or Uniform
+    valency: tuple = (-1.0, 0.0)  # saltfree: (counterion, -); salt: (positive, negative)
+    onsager: tuple = (1.0, 1.0)  # Onsager coefficients in the same order
+    debye_length: float = 10.0   # salt: Debye_length
+    surface_charge: float = 0.0  # Particle_spec[0].Surface_charge
+    e_field: str = "OFF"         # Electric_field: OFF, DC or AC
+    e_ext: tuple = (0.0, 0.0, 0.0)  # Ex, Ey, Ez
+    e_frequency: float = 0.0     # AC Frequency
 
     # ------------------------------------------------------------------
     @property
@@ -158,9 +170,36 @@ def udf_keys(cfg: SPMConfig, particles: Dict[str, np.ndarray],
     k["resume.CONTINUE.Saved_Data.jikan.ts"] = "0"
     k["constitutive_eq.type"] = eq
     base = f"constitutive_eq.{eq}"
-    for name, val in (("DX", cfg.dx), ("RHO", cfg.rho), ("ETA", cfg.eta), ("kBT", cfg.kbt),
-                      ("alpha_v", cfg.alpha_v), ("alpha_o", cfg.alpha_o)):
+    scalars = [("DX", cfg.dx), ("RHO", cfg.rho), ("ETA", cfg.eta), ("kBT", cfg.kbt)]
+    if eq != EQ_EL:
+        scalars += [("alpha_v", cfg.alpha_v), ("alpha_o", cfg.alpha_o)]
+    for name, val in scalars:
         k[f"{base}.{name}"] = _fmt(float(val))
+    if eq == EQ_EL:
+        k[f"{base}.Dielectric_cst"] = _fmt(float(cfg.dielectric))
+        k[f"{base}.INIT_profile"] = "Poisson_Boltzmann" if cfg.init_pb else "Uniform"
+        if cfg.salt:
+            k[f"{base}.Add_salt.type"] = "salt"
+            s = f"{base}.Add_salt.salt"
+            k[f"{s}.Valency_positive_ion"] = _fmt(float(cfg.valency[0]))
+            k[f"{s}.Valency_negative_ion"] = _fmt(float(cfg.valency[1]))
+            k[f"{s}.Onsager_coeff_positive_ion"] = _fmt(float(cfg.onsager[0]))
+            k[f"{s}.Onsager_coeff_negative_ion"] = _fmt(float(cfg.onsager[1]))
+            k[f"{s}.Debye_length"] = _fmt(float(cfg.debye_length))
+        else:
+            k[f"{base}.Add_salt.type"] = "saltfree"
+            k[f"{base}.Add_salt.saltfree.Valency_counterion"] = _fmt(float(cfg.valency[0]))
+            k[f"{base}.Add_salt.saltfree.Onsager_coeff_counterion"] = _fmt(float(cfg.onsager[0]))
+        if cfg.e_field == "OFF":
+            k[f"{base}.Electric_field.type"] = "OFF"
+        else:
+            k[f"{base}.Electric_field.type"] = "ON"
+            k[f"{base}.Electric_field.ON.type"] = cfg.e_field
+            f = f"{base}.Electric_field.ON.{cfg.e_field}"
+            for c, v in zip(("Ex", "Ey", "Ez"), cfg.e_ext):
+                k[f"{f}.{c}"] = _fmt(float(v))
+            if cfg.e_field == "AC":
+                k[f"{f}.Frequency"] = _fmt(float(cfg.e_frequency))
     if eq == EQ_LE:
         k[f"{base}.External_field.type"] = "DC"
         k[f"{base}.External_field.DC.Shear_rate"] = _fmt(float(cfg.shear_rate))
@@ -168,7 +207,7 @@ def udf_keys(cfg: SPMConfig, particles: Dict[str, np.ndarray],
     ps = "object_type.spherical_particle.Particle_spec[0]"
     k[f"{ps}.Particle_number"] = str(cfg.n_particles)
     k[f"{ps}.MASS_RATIO"] = _fmt(float(cfg.mass_ratio))
-    k[f"{ps}.Surface_charge"] = "0.0"
+    k[f"{ps}.Surface_charge"] = _fmt(float(cfg.surface_charge))
     k[f"{ps}.janus_axis"] = "NONE"
     k[f"{ps}.janus_propulsion"] = "OFF"
     k["A_XI"] = _fmt(float(cfg.a_xi))

@@ -29,6 +29,7 @@
 #include "fft_wrapper.h"
 #include "input.h"
 #include "operate_omega.h"
+#include "solute_rhs.h"
 #include "variable.h"
 
 extern double *phi;
@@ -140,6 +141,33 @@ void __wrap__Z17Output_field_dataPPdS_P8ParticleRK5CTime(double **zeta, double *
             U_k2u(uu);
             fwrite(g_tmp.data(), sizeof(double), 3 * n_field, g_dump);
         }
+    }
+    g_frame++;
+}
+
+// Electrolyte frames (Output_charge_field_data): zeta, phi and u as above,
+// then the N_spec k-space concentration fields; has_fields = 10 + N_spec.
+void __wrap__Z24Output_charge_field_dataPPdS_S0_P8ParticleRK5CTime(double **zeta, double *uk_dc, double **conc,
+                                                                     Particle *p, const CTime &jikan) {
+    (void)p;
+    if (!g_dump) return;
+    const size_t n_field    = (size_t)NX * NY * NZ_;
+    const int    has_fields = (g_fields_every > 0 && (g_frame % g_fields_every) == 0) ? 10 + N_spec : 0;
+    int          ihdr[2]    = {jikan.ts, has_fields};
+    fwrite(ihdr, sizeof(int), 2, g_dump);
+    double dhdr[5] = {jikan.time, degree_oblique, uk_dc[0], uk_dc[1], uk_dc[2]};
+    fwrite(dhdr, sizeof(double), 5, g_dump);
+    if (has_fields) {
+        fwrite(zeta[0], sizeof(double), n_field, g_dump);
+        fwrite(zeta[1], sizeof(double), n_field, g_dump);
+        fwrite(phi, sizeof(double), n_field, g_dump);
+        g_tmp.assign(3 * n_field, 0.0);
+        double *uu[3] = {g_tmp.data(), g_tmp.data() + n_field, g_tmp.data() + 2 * n_field};
+        double  dc[3] = {uk_dc[0], uk_dc[1], uk_dc[2]};
+        Zeta_k2u_k(zeta, dc, uu);
+        U_k2u(uu);
+        fwrite(g_tmp.data(), sizeof(double), 3 * n_field, g_dump);
+        for (int n = 0; n < N_spec; n++) fwrite(conc[n], sizeof(double), n_field, g_dump);
     }
     g_frame++;
 }

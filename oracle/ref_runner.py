@@ -13,6 +13,8 @@ oracle/ref_build/ref_dump.cxx:
           f64[5]:   time, degree_oblique, uk_dc[3]
           has_fields>=1: zeta0, zeta1, phi (each NX*NY*NZ_ f64, reference layout)
           has_fields==2: u (3 real fields, padded rows; Navier_Stokes runs)
+          has_fields==10+N_spec: u, then N_spec k-space concentration fields
+                      (Electrolyte runs)
           f64[Np*44]: per particle x, x_nopbc, v, v_old, omega, omega_old,
                       q(s,v), q_old(s,v), f_hydro, f_hydro_previous,
                       torque_hydro, torque_hydro_previous, fr, fr_previous
@@ -114,8 +116,11 @@ def read_dump(path: str) -> Dict:
             z1 = take(nfield).reshape(nx, ny, nz_)
             fr["zeta"] = np.stack([z0, z1]).view(np.complex128)  # [2, NX, NY, NZ/2+1]
             fr["phi"] = take(nfield).reshape(nx, ny, nz_)[:, :, :nz].copy()
-            if has_fields == 2:
+            if has_fields == 2 or has_fields >= 10:
                 fr["u"] = take(3 * nfield).reshape(3, nx, ny, nz_)[..., :nz].copy()
+            if has_fields >= 10:  # Electrolyte: k-space concentration of each ion species
+                ns = has_fields - 10
+                fr["conc"] = take(ns * nfield).reshape(ns, nx, ny, nz_).view(np.complex128)
         prec = np.frombuffer(raw, dtype=np.float64, count=npart * PARTICLE_WORDS, offset=off)
         off += 8 * npart * PARTICLE_WORDS
         prec = prec.reshape(npart, PARTICLE_WORDS)

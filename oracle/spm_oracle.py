@@ -81,6 +81,34 @@ class MT19937:
         return factor * x1, factor * x2
 
 
+def ooura_packed_planes(ak: np.ndarray) -> np.ndarray:
+    """The kz = 0 and kz = NZ/2 planes of a k-space field [..., NX, NY, NZ/2+1]
+    as A_k2a's inverse reads them.  rdft3dsort(-1) (fftsg3d.c:632-655) packs
+    both planes into one half spectrum before rdft3d: it keeps, on kz = 0, the
+    rows 0 < j < NY/2 and the entries i <= NX/2 of the rows j = 0, NY/2; on
+    kz = NZ/2, the rows j > NY/2 and the entries i > NX/2 of the rows j = 0,
+    NY/2; at the four self-conjugate points (i in {0, NX/2}, j in {0, NY/2})
+    the real part only.  Every other entry is implied as the conjugate of its
+    partner (-i, -j).  The result is Hermitian on both planes, so irfftn of it
+    equals the reference's inverse also for a field that is not (a gradient
+    i k a keeps +N/2 at the Nyquist wavenumber on both partners)."""
+    out = np.array(ak, dtype=np.complex128, copy=True)
+    nx, ny = out.shape[-3], out.shape[-2]
+    h1, h2 = nx // 2, ny // 2
+    i = np.arange(nx)[:, None]
+    j = np.arange(ny)[None, :]
+    edge = (j == 0) | (j == h2)
+    selfc = edge & ((i == 0) | (i == h1))
+    drops = ((j > h2) | (edge & (i > h1)), ((j > 0) & (j < h2)) | (edge & (i > 0) & (i < h1)))
+    pi, pj = (nx - i) % nx, (ny - j) % ny
+    for kz, drop in ((0, drops[0]), (out.shape[-1] - 1, drops[1])):
+        plane = out[..., kz]
+        partner = np.conj(plane[..., pi, pj])
+        fixed = np.where(drop, partner, np.where(selfc, plane.real + 0j, plane))
+        out[..., kz] = fixed
+    return out
+
+
 def nint(a: np.ndarray) -> np.ndarray:
     """macro.h:44-52: round half away from zero via int truncation."""
     return np.where(a >= 0.0, np.trunc(a + 0.5), np.trunc(a - 0.5))
@@ -174,8 +202,10 @@ class OracleSPM:
         return np.fft.rfftn(a, axes=(-3, -2, -1))
 
     def ifft(self, ak: np.ndarray) -> np.ndarray:
-        """A_k2a (fft_wrapper.h:662-681)."""
-        return np.fft.irfftn(ak, s=(self.NX, self.NY, self.NZ), axes=(-3, -2, -1))
+        """A_k2a (fft_wrapper.h:662-681).  Exact for a field that is Hermitian
+        on the kz = 0 and kz = NZ/2 planes; any other goes through
+        ooura_packed_planes first."""
+        return np.fft.irfftn(ooura_packed_planes(ak), s=(self.NX, self.NY, self.NZ), axes=(-3, -2, -1))
 
     def truncate(self, ak: np.ndarray) -> np.ndarray:
         return np.where(self.keep, ak, 0.0)

@@ -57,10 +57,10 @@ def test_udf_key_file_roundtrip():
 def test_udf_rejects_out_of_scope_equation():
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "in.keys")
-        open(path, "w").write("constitutive_eq.type = Electrolyte\n")
+        open(path, "w").write("constitutive_eq.type = Shear_Navier_Stokes\n")
         p = N.SpmParams()
         assert N.lib().spm_params_from_udf_keys(path.encode(), C.byref(p), None, 0) == 1
-        assert b"Electrolyte" in N.lib().spm_last_error()
+        assert b"Shear_Navier_Stokes" in N.lib().spm_last_error()
 
 
 def test_create_without_device_fails_cleanly():

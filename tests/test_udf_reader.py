@@ -253,7 +253,7 @@ def test_every_reference_example_parses_and_in_scope_ones_load():
         rc = N.lib().spm_params_from_udf(f.encode(), C.byref(p), None, 0)
         spherical = kv["object_type.type"] == "spherical_particle"
         janus = spherical and kv["object_type.spherical_particle.Particle_spec[0].janus_propulsion"] != "OFF"
-        in_scope = (kv["constitutive_eq.type"] in ("Navier_Stokes", EQ_LE) and spherical and not janus
+        in_scope = (kv["constitutive_eq.type"] in ("Navier_Stokes", EQ_LE, "Electrolyte") and spherical and not janus
                     and "object_type.spherical_particle.Particle_spec[1].Particle_number" not in kv)
         assert (rc == 0) == in_scope, (f, N.lib().spm_last_error())
         if rc == 0:
@@ -265,9 +265,18 @@ def test_every_reference_example_parses_and_in_scope_ones_load():
             assert p.eta == float(kv[f"constitutive_eq.{eq}.ETA"])
             if eq == EQ_LE:
                 assert p.shear_rate == float(kv[f"constitutive_eq.{eq}.External_field.DC.Shear_rate"])
+            if eq == "Electrolyte":
+                e = "constitutive_eq.Electrolyte."
+                assert p.equation == N.SPM_EQ_ELECTROLYTE and p.dielectric == float(kv[e + "Dielectric_cst"])
+                assert p.salt == (kv[e + "Add_salt.type"] == "salt")
+                assert p.surface_charge == float(kv["object_type.spherical_particle.Particle_spec[0].Surface_charge"])
+                if p.salt:
+                    assert p.debye_length == float(kv[e + "Add_salt.salt.Debye_length"])
+                    assert list(p.valency) == [float(kv[e + "Add_salt.salt.Valency_positive_ion"]),
+                                               float(kv[e + "Add_salt.salt.Valency_negative_ion"])]
             if kv["time_increment.type"] == "manual":
                 assert p.dt == float(kv["time_increment.manual.delta_t"])
-            else:
+            elif eq != "Electrolyte":
                 # DT = factor / (NU * KMAX2), KMAX2 from the 2/3-rule wavenumbers
                 k2 = sum((2 * math.pi / ((1 << n) * p.dx) * (((1 << n) + 2) // 3)) ** 2 for n in (p.npx, p.npy, p.npz))
                 assert p.dt == pytest.approx(float(kv["time_increment.auto.factor"]) / (p.eta / p.rho * k2), rel=1e-14)
