@@ -94,6 +94,10 @@ typedef struct spm_pool spm_pool;
 /* ---- context ----------------------------------------------------------- */
 const char *spm_last_error(void);
 int spm_device_count(int *count);
+/* sizeof(spm_params) in the library.  A binding compiled against another
+ * version of this header compares it with its own sizeof(spm_params) and
+ * refuses to run on a mismatch (the struct grows at its end). */
+size_t spm_params_size(void);
 /* Fills p with the reference's defaults for a Navier_Stokes run. */
 int spm_params_default(spm_params *p);
 /* Reads a UDF key file (lines "<udf.path> = <value>", the UDF paths of

@@ -91,6 +91,7 @@ _D = C.POINTER(C.c_double)
 _SIGS = {
     "spm_last_error": (C.c_char_p, []),
     "spm_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+    "spm_params_size": (C.c_size_t, []),
     "spm_params_default": (C.c_int, [C.POINTER(SpmParams)]),
     "spm_params_from_udf_keys": (C.c_int, [C.c_char_p, C.POINTER(SpmParams), _D, C.c_int]),
     "spm_params_from_udf": (C.c_int, [C.c_char_p, C.POINTER(SpmParams), _D, C.c_int]),
@@ -186,6 +187,9 @@ def lib(build_if_missing: bool = True):
         fn = getattr(L, name)
         fn.restype = res
         fn.argtypes = args
+    if L.spm_params_size() != C.sizeof(SpmParams):
+        raise SpmError(f"{path} was built from another kapsel_spm.h: spm_params is {L.spm_params_size()} bytes "
+                       f"there, {C.sizeof(SpmParams)} in this binding")
     _lib = L
     return L
 

@@ -517,6 +517,16 @@ int fft_inv(spm_ctx *c, int slot, int nf) {
     return z_pass<T>(c, slot, nf, false);
 }
 
+// Inverse transform of fields that may carry entries outside the 2/3 box
+// (state getters, output frames, the Coulomb force path): the packed-plane
+// reading of the reference's A_k2a first (k_packed_planes), then fft_inv.
+template <typename T>
+int fft_inv_packed(spm_ctx *c, int slot, int nf) {
+    LAUNCH(c, k_packed_planes<T>, dim3((2 * c->g.nx * c->g.ny + 255) / 256, nf), 256, 0, c->g, c->cx<T>(slot),
+           c->slot_stride_c);
+    return fft_inv<T>(c, slot, nf);
+}
+
 __global__ void k_zero3(double *uk_dc) {
     if (threadIdx.x < 3) uk_dc[threadIdx.x] = 0.0;
 }
@@ -534,7 +544,7 @@ int zeta_to_velocity(spm_ctx *L, int truncate) {
     if (!truncate) {
         LAUNCH(L, (k_zeta_to_u<T, 0>), L->pw_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
                L->cx<T>(U1), L->cx<T>(U2), 0, L->fstride_c);
-        return fft_inv<T>(L, U0, 3);
+        return fft_inv_packed<T>(L, U0, 3);
     }
     int rc;
     LAUNCH(L, (k_zeta_to_u<T, 1>), L->box_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
@@ -1173,6 +1183,8 @@ int spm_device_bytes(const spm_params *p, size_t *bytes) {
     *bytes = nslot * fld + (size_t)std::max(p->n_particles, 1) * kPWords * 8 + sc + 64 * 1024;
     return SPM_OK;
 }
+
+size_t spm_params_size(void) { return sizeof(spm_params); }
 
 int spm_create(const spm_params *p, void *stream, spm_ctx **out) {
     if (!p || !out) return fail(SPM_ERR_ARG, "null argument");

@@ -158,6 +158,15 @@ __global__ void r_el_charge_add(Grid g, T *__restrict__ charge, const T *__restr
     }
 }
 
+// out = a + b over the real cells
+template <typename T>
+__global__ void r_el_sum2(Grid g, T *__restrict__ out, const T *__restrict__ a, const T *__restrict__ b) {
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x)
+        out[idx] = (int)(idx % rowlen) < g.nz ? a[idx] + b[idx] : (T)0;
+}
+
 // a = value on the real cells (the uniform initial ion density)
 template <typename T>
 __global__ void r_el_fill(Grid g, T *__restrict__ a, double value) {
@@ -214,48 +223,6 @@ __global__ void k_el_grad(Grid g, const cplx<T> *__restrict__ a, cplx<T> *__rest
             d2.re = (T)((double)d2.re - e2);
         }
         g0[idx] = d0, g1[idx] = d1, g2[idx] = d2;
-    }
-}
-
-// The kz = 0 and kz = NZ/2 planes as the reference's inverse transform reads
-// them.  Its Ooura rdft3d takes a packed half spectrum: rdft3dsort(-1)
-// (fftsg3d.c:632-655) keeps, on kz = 0, the rows 0 < j < NY/2 and i <= NX/2 of
-// the rows j = 0, NY/2; on kz = NZ/2, the rows j > NY/2 and i > NX/2 of the
-// rows j = 0, NY/2; at the four self-conjugate points only the real part.
-// Every other entry of the two planes is implied as the conjugate of its
-// partner (-i, -j).  A field that is not Hermitian there (the gradient i k a
-// at the Nyquist wavenumbers, whose partner has the same +N/2) is rewritten
-// that way, after which any inverse real transform gives the reference's
-// result.  Discarded entries read only kept partners, so one pass is
-// race-free.  One thread per (plane, i, j), three fields.
-template <typename T>
-__global__ void k_el_hermitian_planes(Grid g, cplx<T> *__restrict__ f0, cplx<T> *__restrict__ f1,
-                                      cplx<T> *__restrict__ f2) {
-    const int n = 2 * g.nx * g.ny;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const int plane = t / (g.nx * g.ny);
-    const int i     = (t / g.ny) % g.nx;
-    const int j     = t % g.ny;
-    const int h1 = g.nx / 2, h2 = g.ny / 2;
-    const int kz       = plane ? g.hnz - 1 : 0;
-    const bool edge_j  = (j == 0 || j == h2);
-    const bool self_cj = edge_j && (i == 0 || i == h1);
-    bool       drop;
-    if (plane == 0)
-        drop = j > h2 || (edge_j && i > h1);
-    else
-        drop = (j > 0 && j < h2) || (edge_j && i > 0 && i < h1);
-    const size_t idx = ((size_t)i * g.ny + j) * g.hnzp + kz;
-    cplx<T>     *fs[3] = {f0, f1, f2};
-    if (drop) {
-        const size_t pidx = ((size_t)((g.nx - i) % g.nx) * g.ny + (g.ny - j) % g.ny) * g.hnzp + kz;
-        for (int d = 0; d < 3; d++) {
-            const cplx<T> v = fs[d][pidx];
-            fs[d][idx]      = cplx<T>{v.re, -v.im};
-        }
-    } else if (self_cj) {
-        for (int d = 0; d < 3; d++) fs[d][idx].im = (T)0;
     }
 }
 

@@ -71,6 +71,41 @@ __device__ __forceinline__ bool k_point(const Grid &g, size_t idx, KPoint &p, si
     return true;
 }
 
+// The kz = 0 and kz = NZ/2 planes as the reference's inverse transform reads
+// them (A_k2a, fft_wrapper.h:662-681).  Its Ooura rdft3d takes a packed half
+// spectrum: rdft3dsort(-1) (fftsg3d.c:632-655) keeps, on kz = 0, the rows
+// 0 < j < NY/2 and i <= NX/2 of the rows j = 0, NY/2; on kz = NZ/2, the rows
+// j > NY/2 and i > NX/2 of the rows j = 0, NY/2; at the four self-conjugate
+// points only the real part.  Every other entry of the two planes is implied
+// as the conjugate of its partner (-i, -j).  A field that is not Hermitian
+// there (a gradient i k a, or u from zeta, at the Nyquist wavenumbers whose
+// partner keeps the same +N/2; an oblique Lees-Edwards zeta) is rewritten
+// that way, after which any inverse real transform gives the reference's
+// result.  Discarded entries read only kept partners, so one pass is
+// race-free.  Thread per (plane, i, j); blockIdx.y = field, fields
+// fstride_c complex values apart.
+template <typename T>
+__global__ void k_packed_planes(Grid g, cplx<T> *__restrict__ f, size_t fstride_c) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * g.nx * g.ny) return;
+    cplx<T>   *a     = f + (size_t)blockIdx.y * fstride_c;
+    const int  plane = t / (g.nx * g.ny);
+    const int  i     = (t / g.ny) % g.nx;
+    const int  j     = t % g.ny;
+    const int  h1 = g.nx / 2, h2 = g.ny / 2;
+    const int  kz      = plane ? g.hnz - 1 : 0;
+    const bool edge_j  = (j == 0 || j == h2);
+    const bool self_cj = edge_j && (i == 0 || i == h1);
+    const bool drop    = plane == 0 ? (j > h2 || (edge_j && i > h1)) : ((j > 0 && j < h2) || (edge_j && i > 0 && i < h1));
+    const size_t idx   = ((size_t)i * g.ny + j) * g.hnzp + kz;
+    if (drop) {
+        const cplx<T> v = a[((size_t)((g.nx - i) % g.nx) * g.ny + (g.ny - j) % g.ny) * g.hnzp + kz];
+        a[idx]          = cplx<T>{v.re, -v.im};
+    } else if (self_cj) {
+        a[idx].im = (T)0;
+    }
+}
+
 // Calls f(idx, p, valid) for the modes a k-space kernel visits.  BOX == 1:
 // only the retained 2/3 box; a warp walks one (kx, ky) row at a time with its
 // lanes on consecutive kz, so there is no per-element index division.

@@ -65,6 +65,12 @@ spm_ctx *ctx() {
         fprintf(stderr, "kapsel_b200: the GPU boundary serves Navier_Stokes runs with one particle species\n");
         exit_job(EXIT_FAILURE);
     }
+    if (spm_params_size() != sizeof(spm_params)) {
+        fprintf(stderr, "kapsel_b200: libkapsel_spm was built from another kapsel_spm.h (spm_params %zu bytes, "
+                        "this program %zu): rebuild the program\n",
+                spm_params_size(), sizeof(spm_params));
+        exit_job(EXIT_FAILURE);
+    }
     spm_params p;
     check(spm_params_default(&p), "spm_params_default");
     p.npx         = log2_exact(NX, "X");

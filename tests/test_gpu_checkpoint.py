@@ -5,7 +5,8 @@ the original: after n2 more steps the particle state and zeta agree within
 1e-12 relative (the shared-profile scatters use float atomics, whose order
 may differ where three or more profiles overlap a cell).  Covered: FP64
 Navier_Stokes with the thermostat (MT19937 state), FP32-mixed (compensated
-zeta words) and Lees-Edwards (degree_oblique and its device scalars).  A
+zeta words), Lees-Edwards (degree_oblique and its device scalars) and
+Electrolyte (ion concentrations and Total_solute; AC field in time).  A
 checkpoint is refused by a context with other parameters, and a truncated
 file is refused."""
 import os
@@ -15,7 +16,7 @@ import pytest
 
 from kapsel3_b200 import _native as N
 from kapsel3_b200.spm import SPMRun
-from kapsel3_b200.udf import EQ_LE, SPMConfig, make_particles
+from kapsel3_b200.udf import EQ_EL, EQ_LE, SPMConfig, make_particles
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
@@ -33,6 +34,10 @@ CASES = {
                                 body_force=(1e-3, 0.0, 0.0)), N.SPM_PREC_FP32_MIXED),
     "lees_edwards_fp64": (SPMConfig(npx=5, npy=5, npz=5, n_particles=3, a=3.5, a_xi=2.0, dt=0.05, equation=EQ_LE,
                                     shear_rate=0.3, kbt=1e-5), N.SPM_PREC_FP64),
+    "electrolyte_salt_ac": (SPMConfig(npx=5, npy=5, npz=5, n_particles=3, a=4.0, a_xi=2.0, dt=0.01, equation=EQ_EL,
+                                      kbt=1.0, salt=True, valency=(1.0, -1.0), onsager=(1.0, 1.5), debye_length=5.0,
+                                      surface_charge=-12.0, e_field="AC", e_ext=(0.1, 0.05, 0.0), e_frequency=4.0),
+                            N.SPM_PREC_FP64),
 }
 
 
@@ -48,16 +53,20 @@ def test_restored_run_continues_like_the_original(gpu, name, tmp_path):
         a.step(6)
         pa, (za, dca), ta = a.particles(), a.zeta(), a.time()
         sa = a.shear_state() if cfg.equation == EQ_LE else None
+        ca = [a.concentration(n) for n in range(2)] if cfg.equation == EQ_EL else []
     with SPMRun(cfg, precision=prec) as b:
         b.load_state(path)
         assert b.time()[0] == 7
         b.step(6)
         pb, (zb, dcb), tb = b.particles(), b.zeta(), b.time()
         sb = b.shear_state() if cfg.equation == EQ_LE else None
+        cb = [b.concentration(n) for n in range(2)] if cfg.equation == EQ_EL else []
     assert ta == tb
     for k in ("x", "v", "omega", "q", "f_hydro_previous"):
         assert rel(pb[k], pa[k]) <= TOL, (name, k)
     assert rel(zb, za) <= TOL and rel(dcb, dca) <= TOL
+    for n, (x, y) in enumerate(zip(ca, cb)):
+        assert rel(y, x) <= TOL, (name, "conc", n)
     if sa is not None:
         assert sb[0] == sa[0]
         assert rel(sb[1], sa[1]) <= TOL

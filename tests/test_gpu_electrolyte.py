@@ -5,8 +5,10 @@ inputs: particle state, zeta, the real-space velocity and the k-space ion
 concentrations after every step, FP64, within 1e-10 relative.
 
 Cases: counterions only (saltfree) under a DC field, a salt solution
-(positive and negative ions) without a field, and a salt solution under an
-AC field along x and y."""
+(positive and negative ions) without a field, a salt solution under an AC
+field along x and y, and two colloids inside the Lennard-Jones range (the
+Force() call of the velocity update).  The legacy AVS files of an
+Electrolyte run (Output_charge_field_data) match the reference's own."""
 import os
 
 import numpy as np
@@ -40,11 +42,25 @@ CASES = {
 }
 
 
+CASES["salt_lj_contact"] = SPMConfig(npx=5, npy=5, npz=5, n_particles=2, a=4.0, a_xi=2.0, dt=0.01, equation=EQ_EL,
+                                     kbt=1.0, salt=True, valency=(1.0, -1.0), onsager=(1.0, 1.0),
+                                     debye_length=5.0, surface_charge=10.0, gts=1, num_snap=8)
+
+
+def _particles(name, cfg):
+    parts = make_particles(cfg, seed=7, v_sd=1e-3, random_orientation=True)
+    if name == "salt_lj_contact":
+        # centres 8.6 apart: inside the cut-off 2^(1/6) SIGMA = 8.98 (SIGMA = 2 A DX)
+        parts["x"][0] = (12.0, 16.0, 15.5)
+        parts["x"][1] = (20.6, 16.0, 15.5)
+    return parts
+
+
 @pytest.mark.skipif(not ref_runner.available(), reason="oracle/_ref is not built")
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_electrolyte_matches_the_reference_program(gpu, name, tmp_path):
     cfg = CASES[name]
-    parts = make_particles(cfg, seed=7, v_sd=1e-3, random_orientation=True)
+    parts = _particles(name, cfg)
     keys, dump = str(tmp_path / "in.keys"), str(tmp_path / "d.bin")
     write_udf_keys(keys, cfg, parts, out_dir=str(tmp_path / "avs"))
     ref_runner.run_reference(keys, dump, fields_every=1, timeout=600)
@@ -77,3 +93,42 @@ def test_electrolyte_parameter_checks(gpu):
             SPMRun(SPMConfig(**{**base, **bad}), precision=N.SPM_PREC_FP64)
     with pytest.raises(N.SpmError, match="FP64"):
         SPMRun(SPMConfig(**base), precision=N.SPM_PREC_FP32_MIXED)
+
+
+AVS_REF = os.path.join(ref_runner.REF_DIR, "kapsel_ref_avs")
+
+
+@pytest.mark.skipif(not os.access(AVS_REF, os.X_OK), reason="oracle/_ref/kapsel_ref_avs is not built")
+def test_electrolyte_avs_files_match_the_reference_program(gpu, tmp_path):
+    """Headers byte for byte; the seven float fields (u, phi, surface charge
+    4 pi RADIUS^2, ion charge density, Coulomb potential) and the particle
+    files to FP32 rounding."""
+    cfg = SPMConfig(npx=5, npy=4, npz=5, n_particles=2, a=4.0, a_xi=2.0, dt=0.01, equation=EQ_EL, kbt=1.0,
+                    salt=True, valency=(2.0, -1.0), onsager=(1.0, 2.0), debye_length=6.0, surface_charge=-15.0,
+                    e_field="DC", e_ext=(0.1, 0.0, 0.05), gts=2, num_snap=2)
+    parts = make_particles(cfg, seed=5, v_sd=1e-3, random_orientation=True)
+    keys = str(tmp_path / "in.keys")
+    write_udf_keys(keys, cfg, parts, out_dir=str(tmp_path / "ref"))
+    ref_runner.run_reference_avs(keys)
+    with SPMRun(cfg, precision=N.SPM_PREC_FP64) as run:
+        run.initialize(parts)
+        run.avs_open(str(tmp_path / "gpu"), "frame", cfg.num_snap)
+        for ts in range(cfg.mstep + 1):
+            if ts % cfg.gts == 0:
+                run.avs_frame()
+            run.step(1)
+        run.avs_close()
+    ref, ours = tmp_path / "ref", tmp_path / "gpu"
+    for name in ("frame.fld", "framep.fld", "frame.cod"):
+        assert (ours / name).read_bytes() == (ref / name).read_bytes(), name
+    nx, ny, nz = cfg.shape
+    for ts in range(0, cfg.mstep + 1, cfg.gts):
+        a = np.fromfile(ours / "avs" / f"frame_{ts}.dat", dtype=np.float32).reshape(7, nz, ny, nx)
+        b = np.fromfile(ref / "avs" / f"frame_{ts}.dat", dtype=np.float32).reshape(7, nz, ny, nx)
+        for f in range(7):
+            scale = max(float(np.abs(b[f]).max()), 1e-30)
+            assert float(np.abs(a[f] - b[f]).max()) <= 2e-6 * scale, (ts, f)
+        for ext in ("cod", "dat"):
+            pa = np.fromfile(ours / "avs" / f"framep_{ts}.{ext}", dtype=np.float32)
+            pb = np.fromfile(ref / "avs" / f"framep_{ts}.{ext}", dtype=np.float32)
+            np.testing.assert_allclose(pa, pb, rtol=2e-6, atol=1e-6)
