@@ -122,12 +122,22 @@ __global__ void __launch_bounds__(256) r_el_sum(Grid g, const T *__restrict__ a,
         partial[blockIdx.x] = t;
     }
 }
-// out = sum of the nb partials (one thread, fixed order)
-__global__ void k_el_sum_finish(const double *__restrict__ partial, int nb, double *__restrict__ out) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    double t = 0.0;
-    for (int b = 0; b < nb; b++) t += partial[b];
-    *out = t;
+// out = sum of the nb partials by one block of kElFinishThreads: thread t
+// adds partials t, t + T, ... in order, then a fixed tree over the threads,
+// so the result does not depend on scheduling.
+constexpr int kElFinishThreads = 256;
+__global__ void __launch_bounds__(kElFinishThreads) k_el_sum_finish(const double *__restrict__ partial, int nb,
+                                                                     double *__restrict__ out) {
+    __shared__ double red[kElFinishThreads];
+    double            t = 0.0;
+    for (int b = threadIdx.x; b < nb; b += kElFinishThreads) t += partial[b];
+    red[threadIdx.x] = t;
+    __syncthreads();
+    for (int w = kElFinishThreads / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
 }
 
 // a *= s over the real cells, s = num / (den * dx3) from device scalars
