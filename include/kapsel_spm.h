@@ -49,6 +49,16 @@ extern "C" {
 #define SPM_EQ_LEES_EDWARDS 1   /* Shear_Navier_Stokes_Lees_Edwards */
 #define SPM_EQ_ELECTROLYTE 2    /* Electrolyte: charged colloids with mobile ions */
 
+/* Particle_spec[0].janus_propulsion (input.cxx:1427-1441) and janus_axis (1410-1425) */
+#define SPM_JANUS_OFF 0       /* "OFF": passive colloids */
+#define SPM_JANUS_TUMBLER 1   /* "TUMBLER": body-frame self force / torque */
+#define SPM_JANUS_SQUIRMER 2  /* "SQUIRMER": surface slip velocity, self-consistent slip iteration */
+#define SPM_JANUS_OBSTACLE 3  /* "OBSTACLE": fixed particles */
+#define SPM_AXIS_NONE 0
+#define SPM_AXIS_X 1
+#define SPM_AXIS_Y 2
+#define SPM_AXIS_Z 3
+
 #define SPM_PREC_FP64 0        /* every field and reduction in FP64 */
 #define SPM_PREC_FP32_MIXED 1  /* fields/FFT/projection FP32, particle reductions and updates FP64 */
 
@@ -86,6 +96,17 @@ typedef struct spm_params {
     int    e_field;              /* Electric_field: 0 OFF, 1 DC, 2 AC */
     double e_ext[3];             /* Ex, Ey, Ez */
     double e_frequency;          /* AC: Frequency */
+    /* Janus particles (Particle_spec[0].janus_*, input.cxx:1403-1470; Navier_Stokes runs) */
+    int    janus_axis;           /* SPM_AXIS_*: the body axis e3 of the slip profile */
+    int    janus_propulsion;     /* SPM_JANUS_* */
+    double janus_force[3];       /* TUMBLER: janus_force, body frame */
+    double janus_torque[3];      /* TUMBLER: janus_torque, body frame */
+    double slip_vel;             /* SQUIRMER: janus_slip_vel (B1) */
+    double slip_mode;            /* SQUIRMER: janus_slip_mode (alpha = B2/B1) */
+    double rotlet_c1;            /* SQUIRMER: janus_rotlet_C1 */
+    double rotlet_c2;            /* SQUIRMER: janus_rotlet_dipole_C2 */
+    double slip_tol;             /* switch.SLIP_tol */
+    int    slip_iter;            /* switch.SLIP_iter */
 } spm_params;
 
 typedef struct spm_ctx spm_ctx;

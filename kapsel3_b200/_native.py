@@ -17,6 +17,8 @@ SPM_PARTICLE_WORDS = 44
 SPM_EQ_NAVIER_STOKES = 0
 SPM_EQ_LEES_EDWARDS = 1
 SPM_EQ_ELECTROLYTE = 2
+SPM_JANUS_OFF, SPM_JANUS_TUMBLER, SPM_JANUS_SQUIRMER, SPM_JANUS_OBSTACLE = 0, 1, 2, 3
+SPM_AXIS_NONE, SPM_AXIS_X, SPM_AXIS_Y, SPM_AXIS_Z = 0, 1, 2, 3
 SPM_PREC_FP64 = 0
 SPM_PREC_FP32_MIXED = 1
 
@@ -45,6 +47,16 @@ class SpmParams(C.Structure):
         ("valency", C.c_double * 2), ("onsager", C.c_double * 2), ("debye_length", C.c_double),
         ("surface_charge", C.c_double), ("e_field", C.c_int), ("e_ext", C.c_double * 3),
         ("e_frequency", C.c_double),
+        ("janus_axis", C.c_int),
+        ("janus_propulsion", C.c_int),
+        ("janus_force", C.c_double * 3),
+        ("janus_torque", C.c_double * 3),
+        ("slip_vel", C.c_double),
+        ("slip_mode", C.c_double),
+        ("rotlet_c1", C.c_double),
+        ("rotlet_c2", C.c_double),
+        ("slip_tol", C.c_double),
+        ("slip_iter", C.c_int),
     ]
 
 

@@ -24,6 +24,7 @@
 #include "spm_kernels.cuh"
 #include "spm_le.cuh"
 #include "spm_electrolyte.cuh"
+#include "spm_janus.cuh"
 
 using namespace spm;
 
@@ -192,6 +193,11 @@ struct spm_ctx {
     int          sm_count = 148;
     LEState      le{};
     ELState      el{};
+    // squirmers: per-particle slip state (kSlipWords each) and the
+    // convergence value of the last slip iteration
+    double      *slip     = nullptr;
+    double      *slip_eps = nullptr;
+    int          slip_iters = 0;  // iterations of the last step's slip loop
     // optional CUDA-event timing of the strided FFT passes inside real steps
     bool                     prof_on = false;
     std::vector<cudaEvent_t> prof_ev;
@@ -284,6 +290,17 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
         if (p.e_field < 0 || p.e_field > 2) return fail(SPM_ERR_ARG, "bad Electric_field");
     }
     if (p.lj_powers < 0 || p.lj_powers > 2) return fail(SPM_ERR_ARG, "LJ_powers must be 12:6, 24:12 or 36:18");
+    // Janus particles (input.cxx:1403-1470, 1868-1872)
+    if (p.janus_propulsion < SPM_JANUS_OFF || p.janus_propulsion > SPM_JANUS_OBSTACLE)
+        return fail(SPM_ERR_ARG, "bad janus_propulsion");
+    if (p.janus_axis < SPM_AXIS_NONE || p.janus_axis > SPM_AXIS_Z) return fail(SPM_ERR_ARG, "bad janus_axis");
+    if (p.janus_propulsion != SPM_JANUS_OFF && p.equation != SPM_EQ_NAVIER_STOKES)
+        return fail(SPM_ERR_ARG, "janus particles are served in Navier_Stokes runs only");
+    if (p.janus_propulsion == SPM_JANUS_SQUIRMER) {
+        if (p.janus_axis == SPM_AXIS_NONE) return fail(SPM_ERR_ARG, "a SQUIRMER needs a janus_axis (X, Y or Z)");
+        if (!(p.slip_vel > 0.0)) return fail(SPM_ERR_ARG, "a SQUIRMER needs janus_slip_vel (B1) > 0");
+        if (p.slip_iter < 1 || !(p.slip_tol >= 0.0)) return fail(SPM_ERR_ARG, "SLIP_iter >= 1 and SLIP_tol >= 0");
+    }
     g.nx  = 1 << p.npx;
     g.ny  = 1 << p.npy;
     g.nz  = 1 << p.npz;
@@ -342,6 +359,18 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
     ph.noise_v = 1.439 * sqrt(zeta_drag * p.dt * p.kbt * p.alpha_v);
     ph.noise_o = 1.22 * sqrt(zeta_drag_rot * p.dt * p.kbt * p.alpha_o);
     ph.np      = p.n_particles;
+    ph.janus_prop = p.janus_propulsion;
+    ph.janus_axis = p.janus_axis;
+    for (int d = 0; d < 3; d++) {
+        ph.janus_force[d]  = p.janus_propulsion == SPM_JANUS_TUMBLER ? p.janus_force[d] : 0.0;
+        ph.janus_torque[d] = p.janus_propulsion == SPM_JANUS_TUMBLER ? p.janus_torque[d] : 0.0;
+    }
+    const bool squirm = p.janus_propulsion == SPM_JANUS_SQUIRMER;
+    ph.slip_b1   = squirm ? p.slip_vel : 0.0;
+    ph.slip_mode = squirm ? p.slip_mode / 2.0 : 0.0;  // alpha/2 = B2/(2 B1) (input.cxx:581-585)
+    ph.slip_c1   = squirm ? p.rotlet_c1 : 0.0;
+    ph.slip_c2   = squirm ? p.rotlet_c2 : 0.0;
+    ph.xi        = xi;
     return SPM_OK;
 }
 
@@ -527,6 +556,24 @@ int fft_inv_packed(spm_ctx *c, int slot, int nf) {
     return fft_inv<T>(c, slot, nf);
 }
 
+// Transforms of fields that are zero outside the 2/3 box, or whose modes
+// outside it are never used: the pruned passes of the Navier_Stokes step.
+// fft_inv_box = truncate, then inverse (only lines |K| < TRN and kz < TRN_Z
+// are read); fft_fwd_box = forward, valid inside the box only (rows kz >=
+// kz_span and lines outside it are not written).
+template <typename T>
+int fft_inv_box(spm_ctx *c, int slot, int nf) {
+    SPM_TRY((fft_strided_pass<T, +1>(c, slot, nf, 0, prune_inverse(c->g, 0))));
+    SPM_TRY((fft_strided_pass<T, +1>(c, slot, nf, 1, prune_inverse(c->g, 1))));
+    return z_pass<T>(c, slot, nf, false, c->g.trn[2]);
+}
+template <typename T>
+int fft_fwd_box(spm_ctx *c, int slot, int nf) {
+    SPM_TRY(z_pass<T>(c, slot, nf, true, 1 << 30, c->g.kz_span()));
+    SPM_TRY((fft_strided_pass<T, -1>(c, slot, nf, 1, prune_forward(c->g, 1))));
+    return fft_strided_pass<T, -1>(c, slot, nf, 0, prune_forward(c->g, 0));
+}
+
 __global__ void k_zero3(double *uk_dc) {
     if (threadIdx.x < 3) uk_dc[threadIdx.x] = 0.0;
 }
@@ -594,6 +641,51 @@ int up_scatter(spm_ctx *c, bool clear = true) {
     dim3 grid((c->ncells + 127) / 128, c->ph.np);
     LAUNCH(c, s_up_scatter<T>, grid, 128, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells, c->ncells,
            c->real<T>(PHIS), c->real<T>(UP0), c->real<T>(UP1), c->real<T>(UP2));
+    return SPM_OK;
+}
+
+// The self-consistent slip iteration of squirmers (the SW_JANUS_SLIP branch
+// of Time_evolution_hydro, sp_3d_ns.cxx:121-161), after the hydrodynamic
+// force: the particle and surface moments, then until convergence the slip
+// force field (droplet counter-flow + surface slip) in UP, its solenoidal
+// projection, the slip force and the velocity update; between iterations
+// v_slip relaxes and v returns to v_old.  At the end u += UP (Swap_mem of
+// u and up + u) and UP keeps the slip field, to which the rigidity force f
+// is added.  The convergence value is read on the host every iteration.
+template <typename T>
+int slip_loop(spm_ctx *c) {
+    const int  pb = (c->ph.np + 127) / 128;
+    const dim3 sgrid((c->ncells + 127) / 128, c->ph.np);
+    LAUNCH(c, s_slip_moments<T>, c->ph.np, 256, 0, c->g, c->ph, c->ps.x, c->ps.q, c->cells, c->ncells,
+           c->real<T>(U0), c->real<T>(U1), c->real<T>(U2), c->slip);
+    LAUNCH(c, p_slip_relax, pb, 128, 0, c->ph, c->ps, c->slip, 0);
+    for (int iter = 0;;) {
+        for (int d = 0; d < 3; d++) SPM_CUDA_CHECK(cudaMemsetAsync(c->real<T>(UP0 + d), 0, c->field_bytes(), c->st));
+        LAUNCH(c, p_slip_droplet, pb, 128, 0, c->ph, c->slip);
+        LAUNCH(c, s_slip_scatter<T>, sgrid, 128, 0, c->g, c->ph, c->ps.x, c->ps.q, c->cells, c->ncells, c->slip,
+               c->real<T>(U0), c->real<T>(U1), c->real<T>(U2), c->real<T>(UP0), c->real<T>(UP1), c->real<T>(UP2));
+        SPM_TRY(fft_fwd_box<T>(c, UP0, 3));
+        LAUNCH(c, k_truncate_project<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(UP0), c->cx<T>(UP1), c->cx<T>(UP2),
+               1);
+        SPM_TRY(fft_inv_box<T>(c, UP0, 3));
+        LAUNCH(c, s_slip_force<T>, c->ph.np, 256, 0, c->g, c->ph, c->ps.x, c->cells, c->ncells, c->real<T>(UP0),
+               c->real<T>(UP1), c->real<T>(UP2), c->slip);
+        LAUNCH(c, p_velocity_slip, pb, 128, 0, c->ph, c->ps, c->slip, c->ts_dev, 0);
+        iter++;
+        LAUNCH(c, k_slip_converge, 1, 256, 0, c->ph, c->ps, c->slip, c->slip_eps);
+        double eps = 0.0;
+        SPM_CUDA_CHECK(cudaMemcpyAsync(&eps, c->slip_eps, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        SPM_CUDA_CHECK(cudaStreamSynchronize(c->st));
+        if (eps < c->P.slip_tol || iter == c->P.slip_iter) {
+            LAUNCH(c, p_velocity_slip, pb, 128, 0, c->ph, c->ps, c->slip, c->ts_dev, 2);
+            c->slip_iters = iter;
+            break;
+        }
+        LAUNCH(c, p_slip_relax, pb, 128, 0, c->ph, c->ps, c->slip, iter);
+        LAUNCH(c, p_velocity_slip, pb, 128, 0, c->ph, c->ps, c->slip, c->ts_dev, 1);
+    }
+    LAUNCH(c, r_add3<T>, c->grid_blocks(), 256, 0, c->g, c->real<T>(U0), c->real<T>(U1), c->real<T>(U2),
+           c->real<T>(UP0), c->real<T>(UP1), c->real<T>(UP2));
     return SPM_OK;
 }
 
@@ -686,8 +778,14 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
         LAUNCH(c, s_hydro_force_cached<T>, c->ph.np, 256, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
                c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS), c->real<T>(U0), c->real<T>(U1), c->real<T>(U2),
                c->ps.f_hydro, c->ps.torque_hydro);
-        LAUNCH(c, p_velocity, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev);
-        if (c->P.kbt > 0.0) LAUNCH(c, p_thermostat, 1, kThermoThreads, 0, c->ph, c->ps, c->mt);
+        if (c->ph.janus_prop == SPM_JANUS_SQUIRMER) {
+            SPM_TRY(slip_loop<T>(c));  // lone runs only; leaves the slip field in UP
+        } else {
+            LAUNCH(c, p_velocity, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev);
+        }
+        // obstacles draw no noise (fluct.cxx:23)
+        if (c->P.kbt > 0.0 && c->ph.janus_prop != SPM_JANUS_OBSTACLE)
+            LAUNCH(c, p_thermostat, 1, kThermoThreads, 0, c->ph, c->ps, c->mt);
         const dim3 sgrid((c->ncells + 127) / 128, c->ph.np);
         LAUNCH(c, s_f_scatter_cached<T>, sgrid, 128, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
                c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS), c->real<T>(U0), c->real<T>(U1), c->real<T>(U2),
@@ -956,6 +1054,8 @@ void destroy_ctx(spm_ctx *c) {
     dev_free(c->le.partial);
     dev_free(c->el.dev);
     dev_free(c->el.partial);
+    dev_free(c->slip);
+    dev_free(c->slip_eps);
     if (c->side) cudaStreamDestroy(c->side);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
@@ -1103,6 +1203,14 @@ int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *
     c->ps.mdf                   = c->ps.torque_r_previous + (size_t)np * 3;
     c->ps.lj_stress             = c->ps.mdf + (size_t)np * 3;
     le_init(c->le, c->g, c->ph, p);
+    if (p.janus_propulsion == SPM_JANUS_SQUIRMER) {
+        if (dev_alloc((void **)&c->slip, (size_t)std::max(np, 1) * kSlipWords * sizeof(double)) != cudaSuccess ||
+            dev_alloc((void **)&c->slip_eps, sizeof(double)) != cudaSuccess) {
+            destroy_ctx(c);
+            return fail(SPM_ERR_NOMEM, "slip buffers");
+        }
+        cudaMemset(c->slip, 0, (size_t)std::max(np, 1) * kSlipWords * sizeof(double));
+    }
     if (p.equation == SPM_EQ_ELECTROLYTE) {
         el_init_state(c->el, p);
         if (dev_alloc((void **)&c->el.dev, kElScalars * sizeof(double)) != cudaSuccess ||
@@ -1167,6 +1275,8 @@ int spm_params_default(spm_params *p) {
     p->dt        = 0.05;
     p->precision = SPM_PREC_FP64;
     p->mt_seed   = 0;
+    p->slip_tol  = 1e-5;
+    p->slip_iter = 100;
     return SPM_OK;
 }
 
@@ -1212,7 +1322,8 @@ int spm_initialize(spm_ctx *c, const double *particles_host) {
 
 int spm_step(spm_ctx *c, int nsteps) {
     if (!c || nsteps < 0) return fail(SPM_ERR_ARG, "bad argument");
-    const bool graph = c->use_graph && !c->pool && !c->prof_on && c->P.equation == SPM_EQ_NAVIER_STOKES;
+    const bool graph = c->use_graph && !c->pool && !c->prof_on && c->P.equation == SPM_EQ_NAVIER_STOKES &&
+                       c->P.janus_propulsion != SPM_JANUS_SQUIRMER;  // the slip loop reads its convergence on the host
     for (int i = 0; i < nsteps; i++) {
         int rc = graph ? (c->fp64() ? step_graphed<double>(c) : step_graphed<float>(c))
                        : (c->fp64() ? step_impl<double>(c) : step_impl<float>(c));

@@ -42,6 +42,13 @@ struct Phys {
     int    np;
     int    lc[3];       // reference cell-list cells per axis (md_force.cxx:56-58)
     double cell_len;    // Cell_length * DX (md_force.cxx:14, 59-61)
+    // Janus particles (one species): propulsion 0 OFF, 1 TUMBLER, 2 SQUIRMER,
+    // 3 OBSTACLE; axis 0 none, 1 x, 2 y, 3 z
+    int    janus_prop, janus_axis;
+    double janus_force[3], janus_torque[3];  // TUMBLER, body frame
+    double slip_b1, slip_mode;               // SQUIRMER: B1, alpha/2
+    double slip_c1, slip_c2;                 // SQUIRMER: rotlet C1, rotlet dipole C2
+    double xi;                               // XI = A_XI DX
 };
 
 // k index decomposition: element (i, j, kz) of a k-space field.
@@ -891,7 +898,7 @@ __device__ __forceinline__ void qtn_normalize_d(double *q) {
 // captured step graph serves every step.
 __global__ void p_position(Phys ph, PState s, const int *__restrict__ ts_dev, int wrap) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= ph.np) return;
+    if (n >= ph.np || ph.janus_prop == 3) return;  // OBSTACLE: fixed (particle_solver.cxx:44)
     const int euler = *ts_dev == 0;
     for (int d = 0; d < 3; d++) {
         const int i       = 3 * n + d;
@@ -1043,19 +1050,45 @@ __global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift) {
 // 239-281) followed by reset_Forces (particle_solver.cxx:11-37).
 // Velocity / angular-velocity update of particle n (Euler at step 0, AB2
 // after) and the shift of the current forces to the previous ones.
+// qvq = q (0, v) q* (qtn_qvq_prod, quaternion.h:189-196); conj: with q*.
+__device__ __forceinline__ void qtn_rotate_d(const double *q, const double *v, double *out, bool conj) {
+    const double s = q[0], a = conj ? -q[1] : q[1], b = conj ? -q[2] : q[2], c = conj ? -q[3] : q[3];
+    const double qs2 = s * s - (a * a + b * b + c * c);
+    const double dot = a * v[0] + b * v[1] + c * v[2];
+    out[0] = qs2 * v[0] + 2.0 * (dot * a + s * (b * v[2] - c * v[1]));
+    out[1] = qs2 * v[1] + 2.0 * (dot * b + s * (c * v[0] - a * v[2]));
+    out[2] = qs2 * v[2] + 2.0 * (dot * c + s * (a * v[1] - b * v[0]));
+}
+
+// self_propulsion (particle_solver.cxx:88-101): a TUMBLER's body-frame force
+// and torque in the space frame (rigid_body_rotation BODY2SPACE).
+__device__ __forceinline__ void self_propulsion_d(const Phys &ph, const double *q, double *f, double *t) {
+    if (ph.janus_prop == 1) {
+        qtn_rotate_d(q, ph.janus_force, f, false);
+        qtn_rotate_d(q, ph.janus_torque, t, false);
+    } else {
+        f[0] = f[1] = f[2] = t[0] = t[1] = t[2] = 0.0;
+    }
+}
+
 __device__ __forceinline__ void velocity_update_one(const Phys &ph, const PState &s, int n, int euler) {
     const double dmy = (euler ? ph.dt : ph.hdt) * ph.imass;
     const double dmr = (euler ? ph.dt : ph.hdt) * ph.imoi;
+    double       sf[3], st[3];
+    self_propulsion_d(ph, s.q + 4 * n, sf, st);
     for (int d = 0; d < 3; d++) {
         const int i      = 3 * n + d;
         s.v_old[i]       = s.v[i];
         s.omega_old[i]   = s.omega[i];
-        if (euler) {
-            s.v[i] += dmy * (s.f_hydro[i] + s.fr[i]);
-            s.omega[i] += dmr * (s.torque_hydro[i] + s.torque_r[i]);
+        if (ph.janus_prop == 3) {  // OBSTACLE
+            s.v[i]     = 0.0;
+            s.omega[i] = 0.0;
+        } else if (euler) {
+            s.v[i] += dmy * (s.f_hydro[i] + s.fr[i] + sf[d]);
+            s.omega[i] += dmr * (s.torque_hydro[i] + s.torque_r[i] + st[d]);
         } else {
-            s.v[i] += dmy * (2.0 * s.f_hydro[i] + s.fr[i] + s.fr_previous[i]);
-            s.omega[i] += dmr * (2.0 * s.torque_hydro[i] + s.torque_r[i] + s.torque_r_previous[i]);
+            s.v[i] += dmy * (2.0 * (s.f_hydro[i] + sf[d]) + s.fr[i] + s.fr_previous[i]);
+            s.omega[i] += dmr * (2.0 * (s.torque_hydro[i] + st[d]) + s.torque_r[i] + s.torque_r_previous[i]);
         }
         s.fr_previous[i]           = s.fr[i];
         s.fr[i]                    = 0.0;

@@ -82,6 +82,14 @@ def params_from_config(cfg: SPMConfig, precision: int = N.SPM_PREC_FP64,
     for d in range(3):
         p.e_ext[d] = float(cfg.e_ext[d])
     p.e_frequency = cfg.e_frequency
+    p.janus_axis = {"NONE": N.SPM_AXIS_NONE, "X": N.SPM_AXIS_X, "Y": N.SPM_AXIS_Y, "Z": N.SPM_AXIS_Z}[cfg.janus_axis]
+    p.janus_propulsion = {"OFF": N.SPM_JANUS_OFF, "TUMBLER": N.SPM_JANUS_TUMBLER, "SQUIRMER": N.SPM_JANUS_SQUIRMER,
+                          "OBSTACLE": N.SPM_JANUS_OBSTACLE}[cfg.janus_propulsion]
+    for d in range(3):
+        p.janus_force[d], p.janus_torque[d] = float(cfg.janus_force[d]), float(cfg.janus_torque[d])
+    p.slip_vel, p.slip_mode = cfg.slip_vel, cfg.slip_mode
+    p.rotlet_c1, p.rotlet_c2 = cfg.rotlet_c1, cfg.rotlet_c2
+    p.slip_tol, p.slip_iter = cfg.slip_tol, int(cfg.slip_iter)
     return p
 
 
@@ -119,7 +127,12 @@ def config_from_udf(path: str) -> Tuple[SPMConfig, Dict[str, np.ndarray]]:
         body_force=tuple(float(p.body_force[d]) for d in range(3)),
         dielectric=p.dielectric, salt=bool(p.salt), init_pb=bool(p.init_pb), valency=tuple(p.valency),
         onsager=tuple(p.onsager), debye_length=p.debye_length, surface_charge=p.surface_charge,
-        e_field=("OFF", "DC", "AC")[p.e_field], e_ext=tuple(p.e_ext), e_frequency=p.e_frequency)
+        e_field=("OFF", "DC", "AC")[p.e_field], e_ext=tuple(p.e_ext), e_frequency=p.e_frequency,
+        janus_axis=("NONE", "X", "Y", "Z")[p.janus_axis],
+        janus_propulsion=("OFF", "TUMBLER", "SQUIRMER", "OBSTACLE")[p.janus_propulsion],
+        janus_force=tuple(p.janus_force), janus_torque=tuple(p.janus_torque), slip_vel=p.slip_vel,
+        slip_mode=p.slip_mode, rotlet_c1=p.rotlet_c1, rotlet_c2=p.rotlet_c2, slip_tol=p.slip_tol,
+        slip_iter=p.slip_iter)
     return cfg, unpack_particles(rec[:p.n_particles])
 
 

@@ -69,6 +69,17 @@ class SPMConfig:
     e_field: str = "OFF"         # Electric_field: OFF, DC or AC
     e_ext: tuple = (0.0, 0.0, 0.0)  # Ex, Ey, Ez
     e_frequency: float = 0.0     # AC Frequency
+    # Janus particles (Particle_spec[0].janus_*, input.cxx:1403-1470)
+    janus_axis: str = "NONE"           # NONE, X, Y, Z
+    janus_propulsion: str = "OFF"      # OFF, TUMBLER, SQUIRMER, OBSTACLE
+    janus_force: tuple = (0.0, 0.0, 0.0)   # TUMBLER, body frame
+    janus_torque: tuple = (0.0, 0.0, 0.0)  # TUMBLER, body frame
+    slip_vel: float = 0.0              # SQUIRMER: janus_slip_vel (B1)
+    slip_mode: float = 0.0             # SQUIRMER: janus_slip_mode (alpha = B2/B1)
+    rotlet_c1: float = 0.0             # SQUIRMER: janus_rotlet_C1
+    rotlet_c2: float = 0.0             # SQUIRMER: janus_rotlet_dipole_C2
+    slip_tol: float = 1e-5             # switch.SLIP_tol
+    slip_iter: int = 100               # switch.SLIP_iter
 
     # ------------------------------------------------------------------
     @property
@@ -208,8 +219,18 @@ def udf_keys(cfg: SPMConfig, particles: Dict[str, np.ndarray],
     k[f"{ps}.Particle_number"] = str(cfg.n_particles)
     k[f"{ps}.MASS_RATIO"] = _fmt(float(cfg.mass_ratio))
     k[f"{ps}.Surface_charge"] = _fmt(float(cfg.surface_charge))
-    k[f"{ps}.janus_axis"] = "NONE"
-    k[f"{ps}.janus_propulsion"] = "OFF"
+    k[f"{ps}.janus_axis"] = cfg.janus_axis
+    k[f"{ps}.janus_propulsion"] = cfg.janus_propulsion
+    if cfg.janus_propulsion == "TUMBLER":
+        for c, f, t in zip("xyz", cfg.janus_force, cfg.janus_torque):
+            k[f"{ps}.janus_force.{c}"] = _fmt(float(f))
+            k[f"{ps}.janus_torque.{c}"] = _fmt(float(t))
+    if cfg.janus_propulsion == "SQUIRMER":
+        k[f"{ps}.janus_slip_vel"] = _fmt(float(cfg.slip_vel))
+        k[f"{ps}.janus_slip_mode"] = _fmt(float(cfg.slip_mode))
+        if cfg.rotlet_c1 or cfg.rotlet_c2:
+            k[f"{ps}.janus_rotlet_C1"] = _fmt(float(cfg.rotlet_c1))
+            k[f"{ps}.janus_rotlet_dipole_C2"] = _fmt(float(cfg.rotlet_c2))
     k["A_XI"] = _fmt(float(cfg.a_xi))
     k["A"] = _fmt(float(cfg.a))
     # Gravity is never used as such (MASS_RATIO=1); a nonzero G only makes the
@@ -226,8 +247,8 @@ def udf_keys(cfg: SPMConfig, particles: Dict[str, np.ndarray],
     k["switch.LJ_truncate"] = cfg.lj_truncate
     k["switch.INIT_distribution.type"] = "user_specify"
     k["switch.INIT_orientation"] = "user_specify"
-    k["switch.SLIP_tol"] = "1e-5"
-    k["switch.SLIP_iter"] = "100"
+    k["switch.SLIP_tol"] = _fmt(float(cfg.slip_tol))
+    k["switch.SLIP_iter"] = str(int(cfg.slip_iter))
     for d, on in zip("xyz", cfg.fix_cell):
         k[f"switch.FIX_CELL.{d}"] = _fmt(bool(on))
     k["switch.pin.type"] = "NO"

@@ -77,3 +77,26 @@ def _gpu_visible():
     n = C.c_int()
     N.lib().spm_device_count(C.byref(n))
     return n.value > 0
+
+
+def test_janus_parameter_checks():
+    """Janus runs are Navier_Stokes only; a SQUIRMER needs an axis, B1 > 0 and
+    a slip iteration budget (input.cxx:1410-1466, 1868-1872).  derive()
+    runs without a device."""
+    L = N.lib()
+    nb = C.c_size_t()
+    def bytes_rc(**kw):
+        p = N.SpmParams()
+        L.spm_params_default(C.byref(p))
+        p.n_particles = 2
+        for k, v in kw.items():
+            setattr(p, k, v)
+        return L.spm_device_bytes(C.byref(p), C.byref(nb)), L.spm_last_error().decode()
+    ok = dict(janus_propulsion=N.SPM_JANUS_SQUIRMER, janus_axis=N.SPM_AXIS_Z, slip_vel=0.01)
+    assert bytes_rc(**ok)[0] == 0
+    assert bytes_rc(janus_propulsion=N.SPM_JANUS_TUMBLER)[0] == 0
+    for bad, msg in ((dict(ok, janus_axis=N.SPM_AXIS_NONE), "janus_axis"), (dict(ok, slip_vel=0.0), "B1"),
+                     (dict(ok, slip_iter=0), "SLIP_iter"), (dict(ok, equation=N.SPM_EQ_LEES_EDWARDS), "Navier_Stokes"),
+                     (dict(janus_propulsion=7), "janus_propulsion")):
+        rc, err = bytes_rc(**bad)
+        assert rc == 1 and msg in err, (bad, err)  # SPM_ERR_ARG

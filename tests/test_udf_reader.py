@@ -43,6 +43,11 @@ CASES = {
     "le_no_rotation": SPMConfig(npx=5, npy=5, npz=5, n_particles=2, a=4.0, a_xi=2.0, dt=0.05, equation=EQ_LE,
                                 shear_rate=0.25, rotation=False, lj_truncate="OFF", lj_powers="24:12"),
     "body_force": SPMConfig(npx=5, npy=5, npz=5, n_particles=2, a=4.0, body_force=(1e-3, 0.0, 0.0)),
+    "squirmer": SPMConfig(npx=5, npy=5, npz=5, n_particles=2, a=4.0, janus_axis="Y", janus_propulsion="SQUIRMER",
+                          slip_vel=0.015, slip_mode=-2.5, rotlet_c1=0.003, rotlet_c2=-0.001, slip_tol=2e-3,
+                          slip_iter=7),
+    "tumbler": SPMConfig(npx=5, npy=5, npz=5, n_particles=2, a=4.0, janus_axis="Z", janus_propulsion="TUMBLER",
+                         janus_force=(0.01, 0.0, -0.02), janus_torque=(0.0, 0.005, 0.0)),
 }
 
 
@@ -252,8 +257,11 @@ def test_every_reference_example_parses_and_in_scope_ones_load():
         p = N.SpmParams()
         rc = N.lib().spm_params_from_udf(f.encode(), C.byref(p), None, 0)
         spherical = kv["object_type.type"] == "spherical_particle"
-        janus = spherical and kv["object_type.spherical_particle.Particle_spec[0].janus_propulsion"] != "OFF"
-        in_scope = (kv["constitutive_eq.type"] in ("Navier_Stokes", EQ_LE, "Electrolyte") and spherical and not janus
+        ps = "object_type.spherical_particle.Particle_spec[0]."
+        janus = spherical and kv[ps + "janus_propulsion"] != "OFF"
+        eq_ok = kv["constitutive_eq.type"] == "Navier_Stokes" or (
+            kv["constitutive_eq.type"] in (EQ_LE, "Electrolyte") and not janus)
+        in_scope = (eq_ok and spherical
                     and "object_type.spherical_particle.Particle_spec[1].Particle_number" not in kv)
         assert (rc == 0) == in_scope, (f, N.lib().spm_last_error())
         if rc == 0:
@@ -274,6 +282,15 @@ def test_every_reference_example_parses_and_in_scope_ones_load():
                     assert p.debye_length == float(kv[e + "Add_salt.salt.Debye_length"])
                     assert list(p.valency) == [float(kv[e + "Add_salt.salt.Valency_positive_ion"]),
                                                float(kv[e + "Add_salt.salt.Valency_negative_ion"])]
+            if janus:
+                jp = ("OFF", "TUMBLER", "SQUIRMER", "OBSTACLE")[p.janus_propulsion]
+                assert jp == kv[ps + "janus_propulsion"]
+                assert ("NONE", "X", "Y", "Z")[p.janus_axis] == kv[ps + "janus_axis"]
+                if jp == "SQUIRMER":
+                    assert p.slip_vel == float(kv[ps + "janus_slip_vel"])
+                    assert p.slip_mode == float(kv[ps + "janus_slip_mode"])
+                    assert p.slip_tol == float(kv["switch.SLIP_tol"])
+                    assert p.slip_iter == int(kv["switch.SLIP_iter"])
             if kv["time_increment.type"] == "manual":
                 assert p.dt == float(kv["time_increment.manual.delta_t"])
             elif eq != "Electrolyte":
@@ -281,3 +298,15 @@ def test_every_reference_example_parses_and_in_scope_ones_load():
                 k2 = sum((2 * math.pi / ((1 << n) * p.dx) * (((1 << n) + 2) // 3)) ** 2 for n in (p.npx, p.npy, p.npz))
                 assert p.dt == pytest.approx(float(kv["time_increment.auto.factor"]) / (p.eta / p.rho * k2), rel=1e-14)
     assert loaded >= 4
+
+
+def test_janus_config_round_trip(tmp_path):
+    for name in ("squirmer", "tumbler"):
+        cfg = CASES[name]
+        parts = make_particles(cfg, seed=3, random_orientation=True)
+        path = str(tmp_path / f"{name}.udf")
+        write_udf(path, cfg, parts)
+        got, _ = config_from_udf(path)
+        for f in ("janus_axis", "janus_propulsion", "janus_force", "janus_torque", "slip_vel", "slip_mode",
+                  "rotlet_c1", "rotlet_c2", "slip_tol", "slip_iter"):
+            assert getattr(got, f) == getattr(cfg, f), (name, f)
