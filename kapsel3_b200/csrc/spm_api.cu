@@ -281,7 +281,8 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
         if (p.precision != SPM_PREC_FP64) return fail(SPM_ERR_ARG, "Electrolyte runs are FP64 only");
         if (p.surface_charge == 0.0) return fail(SPM_ERR_ARG, "Electrolyte needs a nonzero Surface_charge");
         if (!(p.dielectric > 0.0)) return fail(SPM_ERR_ARG, "Dielectric_cst must be > 0");
-        if (p.init_pb) return fail(SPM_ERR_ARG, "INIT_profile Poisson_Boltzmann is not supported (Uniform only)");
+        if (p.init_pb && p.salt == 1 && p.n_particles == 1 && p.valency[0] != -p.valency[1])
+            return fail(SPM_ERR_ARG, "Poisson_Boltzmann with salt needs Valency_positive_ion = -Valency_negative_ion");
         if (p.salt == 0 && !(p.valency[0] * p.surface_charge < 0.0))
             return fail(SPM_ERR_ARG, "Valency_counterion must have the opposite sign of Surface_charge");
         if (p.salt == 1 && !(p.valency[0] > 0.0 && p.valency[1] < 0.0))
@@ -1014,6 +1015,8 @@ void el_init_state(ELState &el, const spm_params &p) {
     el.abs_q       = 0.0;
     for (int n = 0; n < p.n_particles; n++) el.abs_q += fabs(el.qe);
     const double surface_ion_number = -p.surface_charge * p.n_particles;
+    el.surface_ion_number           = surface_ion_number;
+    el.init_pb                      = p.init_pb;
     for (int n = 0; n < el.nspec; n++) {
         el.val_e[n] = p.valency[n] * e;
         el.ons[n]   = p.onsager[n];
@@ -1316,7 +1319,7 @@ int spm_initialize(spm_ctx *c, const double *particles_host) {
     le_reset(c->le);
     rc = c->fp64() ? initialize_impl<double>(c) : initialize_impl<float>(c);
     if (rc != SPM_OK) return rc;
-    if (c->el.enabled && (rc = el_init_ions<double>(c)) != SPM_OK) return rc;
+    if (c->el.enabled && (rc = el_init_profile<double>(c)) != SPM_OK) return rc;
     return check_device_error(c);
 }
 

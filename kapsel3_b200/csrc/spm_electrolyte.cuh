@@ -28,6 +28,10 @@ struct ELState {
     int     e_ac    = 0;           // AC field
     double  e_ext[3] = {0, 0, 0};  // E_ext
     double  e_omega = 0.0;         // Angular_Frequency = 2 pi Frequency
+    int     init_pb = 0;           // INIT_profile Poisson_Boltzmann
+    double  surface_ion_number = 0;// -sum over particles of Surface_charge
+    int     init_iters = 0;        // iterations of the last initial-profile loop
+    int     conc_in_box = 0;       // the ion fields are zero outside the 2/3 box (pruned inverses apply)
     double *dev     = nullptr;     // device scalars (kEl*)
     double *partial = nullptr;     // per-CTA partial sums of the field reductions
 };
@@ -36,7 +40,9 @@ constexpr int kElTotal  = 0;  // [0, 1]: Total_solute of each species
 constexpr int kElQSum   = 2;  // sum of |surface charge field|
 constexpr int kElCSum   = 3;  // [3, 4]: (1 - phi) c sums of each species
 constexpr int kElVolume = 5;  // sum of (1 - phi)
-constexpr int kElScalars = 8;
+constexpr int kElScratch = 6;  // [6, 8]: sums read by the host in the initial-profile loops
+constexpr int kElScalars = 10;
+constexpr double kElTol = 1.e-4;  // TOL of the initial-profile loops (operate_electrolyte.h:21)
 
 // Total_solute[n] = (1 - phi) c sum * DX3 (Count_single_solute)
 __global__ void k_el_total(double *dev, int n, double dx3) {
@@ -95,22 +101,43 @@ __global__ void s_el_surface_normal(Grid g, Phys ph, const double *__restrict__ 
     }
 }
 
-// Sums over the real cells (i < NX, j < NY, k < NZ), one partial per CTA:
-// mode 0: (1 - phi) a (Count_single_solute), 1: |a|, 2: (1 - phi).
+// Sums over the real cells (i < NX, j < NY, k < NZ), one partial per CTA,
+// of (b = phi for the modes that use it):
+//   0: (1 - phi) a (Count_single_solute)     1: |a|       2: (1 - phi)
+//   3: (1 - phi) exp(-coef a)  (the Poisson-Boltzmann normalisations,
+//      operate_electrolyte.cxx:445-455, 597-606)
+//   4: (1 - phi) a (log a - 1)  (ideal-gas free energy, :306-316)
+//   5: a (coef b - (e . (i, j, k)) DX)  (electrostatic free energy with the
+//      external field's potential, :325-352, Add_external_electric_field_x)
+struct ElSumArgs {
+    int    mode;
+    double coef, e[3];
+};
 template <typename T>
-__global__ void __launch_bounds__(256) r_el_sum(Grid g, const T *__restrict__ a, const T *__restrict__ phi, int mode,
-                                                double *__restrict__ partial) {
+__global__ void __launch_bounds__(256) r_el_sum(Grid g, const T *__restrict__ a, const T *__restrict__ b,
+                                                ElSumArgs m, double *__restrict__ partial) {
     const size_t rowlen = 2 * (size_t)g.hnzp;
     const size_t n      = (size_t)g.nx * g.ny * rowlen;
     double       acc    = 0.0;
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
-        if ((int)(idx % rowlen) >= g.nz) continue;
-        if (mode == 0)
-            acc += (1. - (double)phi[idx]) * (double)a[idx];
-        else if (mode == 1)
-            acc += fabs((double)a[idx]);
-        else
-            acc += (1. - (double)phi[idx]);
+        const int k = (int)(idx % rowlen);
+        if (k >= g.nz) continue;
+        switch (m.mode) {
+            case 0: acc += (1. - (double)b[idx]) * (double)a[idx]; break;
+            case 1: acc += fabs((double)a[idx]); break;
+            case 2: acc += (1. - (double)b[idx]); break;
+            case 3: acc += (1. - (double)b[idx]) * exp(-m.coef * (double)a[idx]); break;
+            case 4: {
+                const double c = (double)a[idx];
+                acc += (1. - (double)b[idx]) * c * (log(c) - 1.);
+            } break;
+            default: {
+                const size_t row = idx / rowlen;
+                const int    j = (int)(row % (size_t)g.ny), i = (int)(row / (size_t)g.ny);
+                const double ext = (m.e[0] * (double)i + m.e[1] * (double)j + m.e[2] * (double)k) * g.dx;
+                acc += (double)a[idx] * (m.coef * (double)b[idx] - ext);
+            }
+        }
     }
     __shared__ double red[8];
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -165,6 +192,91 @@ __global__ void r_el_charge_add(Grid g, T *__restrict__ charge, const T *__restr
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
         if ((int)(idx % rowlen) >= g.nz) continue;
         charge[idx] = (T)((double)charge[idx] + val_e * (double)c[idx] * (1. - (double)phi[idx]));
+    }
+}
+
+// Counterions, Poisson-Boltzmann (Set_Poisson_Boltzmann_ion_charge_density_
+// nosalt, operate_electrolyte.cxx:456-478): with rho_0 = num / (dev[s] DX^3)
+// and dmy = rho_0 exp(-coef psi), c = (1 - alp) c + alp dmy; w0 = |dmy|,
+// w1 = |c - dmy| for the convergence sums.  Real fields.
+template <typename T>
+__global__ void r_el_pb_mix(Grid g, T *__restrict__ c, const T *__restrict__ psi, double num,
+                            const double *__restrict__ dev_sum, double dx3, double coef, double alp,
+                            T *__restrict__ w0, T *__restrict__ w1) {
+    const double rho0   = num / (*dev_sum * dx3);
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if ((int)(idx % rowlen) >= g.nz) continue;
+        const double dmy = rho0 * exp(-coef * (double)psi[idx]);
+        const double cn  = (1. - alp) * (double)c[idx] + alp * dmy;
+        c[idx]           = (T)cn;
+        w0[idx]          = (T)fabs(dmy);
+        w1[idx]          = (T)fabs(cn - dmy);
+    }
+}
+
+// Salt, Poisson-Boltzmann (Set_Poisson_Boltzmann_ion_charge_density_salt,
+// operate_electrolyte.cxx:595-630): nu from the quadratic a nu^2 + b nu + c
+// = 0 with a = z+ rho+ I+, b = -Surface_ion_number, c = z- rho- I-, I the
+// sums in dev[sp], dev[sn] (times DX^3); c+ = rho+ exp(-d0 psi) nu, c- =
+// rho- exp(-d1 psi) / nu.  Real fields.
+template <typename T>
+__global__ void r_el_pb_salt(Grid g, T *__restrict__ c0, T *__restrict__ c1, const T *__restrict__ psi,
+                             const double *__restrict__ dev, int sp, int sn, double dx3, double z0, double z1,
+                             double rho_p, double rho_n, double surface_ion_number, double d0, double d1) {
+    const double a  = z0 * rho_p * (dev[sp] * dx3);
+    const double b  = -surface_ion_number;
+    const double cq = z1 * rho_n * (dev[sn] * dx3);
+    const double nu = (-b + sqrt(b * b - 4. * a * cq)) / (2. * a);
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if ((int)(idx % rowlen) >= g.nz) {
+            c0[idx] = c1[idx] = (T)0;
+            continue;
+        }
+        const double pot = (double)psi[idx];
+        c0[idx]          = (T)(rho_p * exp(-d0 * pot) * nu);
+        c1[idx]          = (T)(rho_n * exp(-d1 * pot) / nu);
+    }
+}
+
+// psi += alp (psi_new - psi); w0 = |psi|, w1 = |alp (psi_new - psi)|
+// (operate_electrolyte.cxx:640-655).  Real fields.
+template <typename T>
+__global__ void r_el_pb_relax(Grid g, T *__restrict__ psi, const T *__restrict__ psi_new, double alp,
+                              T *__restrict__ w0, T *__restrict__ w1) {
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if ((int)(idx % rowlen) >= g.nz) continue;
+        const double dmy = alp * ((double)psi_new[idx] - (double)psi[idx]);
+        const double p   = (double)psi[idx] + dmy;
+        psi[idx]         = (T)p;
+        w0[idx]          = (T)fabs(p);
+        w1[idx]          = (T)fabs(dmy);
+    }
+}
+
+// c_n += dt rhs_n inside the 2/3 box (Field_solver_Euler of the ions alone,
+// Ion_diffusion_solver_Euler, fluid_solver.cxx:262-296).
+template <typename T>
+__global__ void k_el_conc_update(Grid g, double dt, cplx<T> *__restrict__ c0, const cplx<T> *__restrict__ r0,
+                                 cplx<T> *__restrict__ c1, const cplx<T> *__restrict__ r1, int nspec) {
+    const size_t n = g.field_elems_c();
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        KPoint p;
+        size_t row;
+        if (!k_point(g, idx, p, row) || !p.keep) continue;
+        cplx<T> c = c0[idx];
+        c.re += (T)dt * r0[idx].re, c.im += (T)dt * r0[idx].im;
+        c0[idx] = c;
+        if (nspec > 1) {
+            c = c1[idx];
+            c.re += (T)dt * r1[idx].re, c.im += (T)dt * r1[idx].im;
+            c1[idx] = c;
+        }
     }
 }
 

@@ -6,8 +6,13 @@ concentrations after every step, FP64, within 1e-10 relative.
 
 Cases: counterions only (saltfree) under a DC field, a salt solution
 (positive and negative ions) without a field, a salt solution under an AC
-field along x and y, and two colloids inside the Lennard-Jones range (the
-Force() call of the velocity update).  The legacy AVS files of an
+field along x and y, two colloids inside the Lennard-Jones range (the
+Force() call of the velocity update), and the Poisson-Boltzmann initial
+profiles of Init_rho_ion: counterions alone (with and without a field, the
+latter followed by the steady-state relaxation), salt around one colloid
+(the potential iteration) and salt around two colloids under a field
+(uniform start and steady state).  The initial ion fields are compared
+from step 0.  The legacy AVS files of an
 Electrolyte run (Output_charge_field_data) match the reference's own."""
 import os
 
@@ -45,6 +50,18 @@ CASES = {
 CASES["salt_lj_contact"] = SPMConfig(npx=5, npy=5, npz=5, n_particles=2, a=4.0, a_xi=2.0, dt=0.01, equation=EQ_EL,
                                      kbt=1.0, salt=True, valency=(1.0, -1.0), onsager=(1.0, 1.0),
                                      debye_length=5.0, surface_charge=10.0, gts=1, num_snap=8)
+
+
+PB = dict(npx=5, npy=5, npz=5, a=4.0, a_xi=2.0, dt=0.01, equation=EQ_EL, kbt=1.0, init_pb=True, gts=1, num_snap=4)
+CASES["pb_counterions"] = SPMConfig(n_particles=1, dielectric=1.0, valency=(1.0, 0.0), onsager=(1.0, 1.0),
+                                    surface_charge=-10.0, **PB)
+CASES["pb_counterions_dc"] = SPMConfig(n_particles=2, dielectric=2.0, valency=(2.0, 0.0), onsager=(1.0, 1.0),
+                                       surface_charge=-12.0, e_field="DC", e_ext=(0.05, 0.0, 0.0), **PB)
+CASES["pb_salt_one"] = SPMConfig(n_particles=1, dielectric=1.0, salt=True, valency=(1.0, -1.0), onsager=(1.0, 1.0),
+                                 debye_length=4.0, surface_charge=-15.0, **PB)
+CASES["pb_salt_two_dc"] = SPMConfig(n_particles=2, dielectric=1.0, salt=True, valency=(1.0, -1.0),
+                                    onsager=(1.0, 1.5), debye_length=5.0, surface_charge=10.0, e_field="DC",
+                                    e_ext=(0.0, 0.05, 0.0), **PB)
 
 
 def _particles(name, cfg):
@@ -88,7 +105,8 @@ def test_electrolyte_parameter_checks(gpu):
     base = dict(npx=5, npy=5, npz=5, n_particles=2, a=4.0, equation=EQ_EL, kbt=1.0, surface_charge=-10.0,
                 valency=(1.0, 0.0))
     for bad, msg in ((dict(surface_charge=0.0), "Surface_charge"), (dict(valency=(-1.0, 0.0)), "opposite sign"),
-                     (dict(init_pb=True), "Poisson_Boltzmann"), (dict(salt=True, valency=(1.0, 1.0)), "salt")):
+                     (dict(init_pb=True, salt=True, valency=(2.0, -1.0), n_particles=1, debye_length=5.0),
+                      "Poisson_Boltzmann"), (dict(salt=True, valency=(1.0, 1.0)), "salt")):
         with pytest.raises(N.SpmError, match=msg):
             SPMRun(SPMConfig(**{**base, **bad}), precision=N.SPM_PREC_FP64)
     with pytest.raises(N.SpmError, match="FP64"):
