@@ -212,7 +212,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream leg")
     ap.add_argument("--serve-runs", type=int, default=256)
-    ap.add_argument("--profile-run", choices=["fp32", "fp64"], default=None,
+    ap.add_argument("--profile-run", choices=["fp32", "fp64", "electrolyte", "squirmer"], default=None,
                     help="only run warm-up + timed steps of one precision (for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -399,6 +399,26 @@ def profile_run(args):
     ncu launch lists and captures under profiles/ were taken with."""
     from kapsel3_b200 import _native as N
     from kapsel3_b200.spm import SPMRun
+    from kapsel3_b200.udf import EQ_EL, SPMConfig, make_particles
+    if args.profile_run in ("electrolyte", "squirmer"):
+        # the Electrolyte and squirmer workloads of the profiles/ launch lists (FP64)
+        if args.profile_run == "electrolyte":
+            cfg = SPMConfig(npx=7, npy=7, npz=7, n_particles=50, a=5.0, a_xi=2.0, dt=0.005, equation=EQ_EL, kbt=1.0,
+                            salt=True, valency=(1.0, -1.0), onsager=(1.0, 1.0), debye_length=4.0,
+                            surface_charge=-20.0, e_field="DC", e_ext=(0.05, 0.0, 0.0), dielectric=1.0)
+            parts = make_particles(cfg, seed=3, v_sd=1e-3, random_orientation=True)
+        else:
+            cfg = SPMConfig(npx=6, npy=6, npz=6, n_particles=50, a=5.0, a_xi=2.0, dt=0.1, janus_axis="Z",
+                            janus_propulsion="SQUIRMER", slip_vel=0.015, slip_mode=2.0, slip_tol=0.005, slip_iter=4)
+            parts = make_particles(cfg, seed=9, random_orientation=True)
+        with SPMRun(cfg, precision=N.SPM_PREC_FP64) as run:
+            run.initialize(parts)
+            run.step(args.warmup)
+            run.synchronize()
+            ms = run.time_steps(args.steps)
+            print(json.dumps({"profile_run": args.profile_run, "grid": cfg.shape, "steps": args.steps,
+                              "ms_per_step": ms / args.steps}), flush=True)
+        return 0
     cfg = workload_config()
     if os.environ.get("SPM_PROFILE_GRID"):
         import dataclasses
