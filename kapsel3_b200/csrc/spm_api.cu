@@ -184,6 +184,7 @@ struct spm_ctx {
     int          ncells  = 0;
     double *     uk_dc   = nullptr;  // rw->uk_dc
     double *     pbuf    = nullptr;  // particle state arrays
+    double *     rec_stage = nullptr;  // particle records in transit (SPM_PARTICLE_WORDS per particle)
     PState       ps{};
     unsigned int *mt  = nullptr;  // 625 words
     unsigned int *err = nullptr;  // device error word (&rw->err)
@@ -945,59 +946,72 @@ int download_field_sum(spm_ctx *c, int slot_hi, int slot_lo, double *h) {
     return SPM_OK;
 }
 
+// Particle records <-> device state.  The records (SPM_PARTICLE_WORDS doubles
+// each) travel as one block between the caller's buffer and a device staging
+// buffer; the AoS <-> SoA reordering runs on the device.  Record offsets of
+// the twelve 3-vectors in the order of the device arrays (see spm_create),
+// then q (18) and q_old (22).
+__constant__ int kRecVec[12] = {0, 3, 6, 9, 12, 15, 26, 29, 32, 35, 38, 41};
+
+__global__ void k_records_in(const double *__restrict__ rec, double *__restrict__ pbuf, PState s, int np,
+                             int normalize_q) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= np) return;
+    const double *r = rec + (size_t)n * SPM_PARTICLE_WORDS;
+    double        q[4], qo[4];
+    for (int k = 0; k < 4; k++) q[k] = r[18 + k], qo[k] = r[22 + k];
+    if (normalize_q) {
+        const double nn = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+        for (int k = 0; k < 4; k++) q[k] *= 1.0 / nn;
+        for (int k = 0; k < 4; k++) qo[k] = q[k];
+    }
+    for (int a = 0; a < 12; a++)
+        for (int d = 0; d < 3; d++) pbuf[(size_t)a * np * 3 + 3 * n + d] = r[kRecVec[a] + d];
+    for (int k = 0; k < 4; k++) {
+        pbuf[(size_t)12 * np * 3 + 4 * n + k]                    = q[k];
+        pbuf[(size_t)12 * np * 3 + (size_t)np * 4 + 4 * n + k] = qo[k];
+    }
+    // x_previous, torque_r, torque_r_previous, lj_stress, mdf start at x / zero
+    for (int d = 0; d < 3; d++) {
+        s.x_previous[3 * n + d]        = r[d];
+        s.torque_r[3 * n + d]          = 0.0;
+        s.torque_r_previous[3 * n + d] = 0.0;
+        s.mdf[3 * n + d]               = 0.0;
+    }
+    s.lj_stress[n] = 0.0;
+}
+
+__global__ void k_records_out(const double *__restrict__ pbuf, double *__restrict__ rec, int np) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= np) return;
+    double *r = rec + (size_t)n * SPM_PARTICLE_WORDS;
+    for (int a = 0; a < 12; a++)
+        for (int d = 0; d < 3; d++) r[kRecVec[a] + d] = pbuf[(size_t)a * np * 3 + 3 * n + d];
+    for (int k = 0; k < 4; k++) {
+        r[18 + k] = pbuf[(size_t)12 * np * 3 + 4 * n + k];
+        r[22 + k] = pbuf[(size_t)12 * np * 3 + (size_t)np * 4 + 4 * n + k];
+    }
+}
+
+// Returns once the records have been read from `rec` (the caller may reuse
+// the buffer); the reordering kernel stays queued ahead of the next step.
 int upload_particles(spm_ctx *c, const double *rec, bool normalize_q) {
     const int np = c->ph.np;
     if (np == 0) return SPM_OK;
-    std::vector<double> h((size_t)np * 44, 0.0);
-    // host staging in the same order as the device arrays (see spm_create)
-    for (int n = 0; n < np; n++) {
-        const double *r = rec + (size_t)n * SPM_PARTICLE_WORDS;
-        double        q[4], qo[4];
-        for (int k = 0; k < 4; k++) {
-            q[k]  = r[18 + k];
-            qo[k] = r[22 + k];
-        }
-        if (normalize_q) {
-            const double nn = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
-            for (int k = 0; k < 4; k++) q[k] *= 1.0 / nn;
-            for (int k = 0; k < 4; k++) qo[k] = q[k];
-        }
-        // 3-vectors: record offsets -> device array index
-        const int voff[12] = {0, 3, 6, 9, 12, 15, 26, 29, 32, 35, 38, 41};
-        for (int a = 0; a < 12; a++)
-            for (int d = 0; d < 3; d++) h[(size_t)a * np * 3 + 3 * n + d] = r[voff[a] + d];
-        for (int k = 0; k < 4; k++) {
-            h[(size_t)12 * np * 3 + 4 * n + k] = q[k];
-            h[(size_t)12 * np * 3 + (size_t)np * 4 + 4 * n + k] = qo[k];
-        }
-    }
-    SPM_CUDA_CHECK(cudaMemcpyAsync(c->pbuf, h.data(), (size_t)np * 44 * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    // x_previous, torque_r, torque_r_previous, lj_stress start at zero / x
-    SPM_CUDA_CHECK(cudaMemcpyAsync(c->ps.x_previous, c->ps.x, (size_t)np * 3 * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-    SPM_CUDA_CHECK(cudaMemsetAsync(c->ps.torque_r, 0, (size_t)np * 3 * sizeof(double), c->st));
-    SPM_CUDA_CHECK(cudaMemsetAsync(c->ps.torque_r_previous, 0, (size_t)np * 3 * sizeof(double), c->st));
-    SPM_CUDA_CHECK(cudaMemsetAsync(c->ps.lj_stress, 0, (size_t)np * sizeof(double), c->st));
-    SPM_CUDA_CHECK(cudaMemsetAsync(c->ps.mdf, 0, (size_t)np * 3 * sizeof(double), c->st));
+    SPM_CUDA_CHECK(cudaMemcpyAsync(c->rec_stage, rec, (size_t)np * SPM_PARTICLE_WORDS * sizeof(double),
+                                   cudaMemcpyHostToDevice, c->st));
     SPM_CUDA_CHECK(cudaStreamSynchronize(c->st));
+    LAUNCH(c, k_records_in, (np + 127) / 128, 128, 0, c->rec_stage, c->pbuf, c->ps, np, normalize_q ? 1 : 0);
     return SPM_OK;
 }
 
 int download_particles(spm_ctx *c, double *rec) {
     const int np = c->ph.np;
     if (np == 0) return SPM_OK;
-    std::vector<double> h((size_t)np * 44);
-    SPM_CUDA_CHECK(cudaMemcpyAsync(h.data(), c->pbuf, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    LAUNCH(c, k_records_out, (np + 127) / 128, 128, 0, c->pbuf, c->rec_stage, np);
+    SPM_CUDA_CHECK(cudaMemcpyAsync(rec, c->rec_stage, (size_t)np * SPM_PARTICLE_WORDS * sizeof(double),
+                                   cudaMemcpyDeviceToHost, c->st));
     SPM_CUDA_CHECK(cudaStreamSynchronize(c->st));
-    const int voff[12] = {0, 3, 6, 9, 12, 15, 26, 29, 32, 35, 38, 41};
-    for (int n = 0; n < np; n++) {
-        double *r = rec + (size_t)n * SPM_PARTICLE_WORDS;
-        for (int a = 0; a < 12; a++)
-            for (int d = 0; d < 3; d++) r[voff[a] + d] = h[(size_t)a * np * 3 + 3 * n + d];
-        for (int k = 0; k < 4; k++) {
-            r[18 + k] = h[(size_t)12 * np * 3 + 4 * n + k];
-            r[22 + k] = h[(size_t)12 * np * 3 + (size_t)np * 4 + 4 * n + k];
-        }
-    }
     return SPM_OK;
 }
 
@@ -1051,6 +1065,7 @@ void destroy_ctx(spm_ctx *c) {
     dev_free(c->sc_idx);
     dev_free(c->sc_w);
     dev_free(c->pbuf);
+    dev_free(c->rec_stage);
     dev_free(c->mt);
     dev_free(c->le.dev);
     dev_free(c->le.ppart);
@@ -1165,6 +1180,7 @@ int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *
     const int np           = std::max(p.n_particles, 1);
     if (dev_alloc((void **)&c->cells, cells.size() * sizeof(int)) != cudaSuccess ||
         dev_alloc((void **)&c->pbuf, (size_t)np * kPWords * sizeof(double)) != cudaSuccess ||
+        dev_alloc((void **)&c->rec_stage, (size_t)std::max(np, 1) * SPM_PARTICLE_WORDS * sizeof(double)) != cudaSuccess ||
         dev_alloc((void **)&c->mt, 625 * sizeof(unsigned int)) != cudaSuccess) {
         destroy_ctx(c);
         return fail(SPM_ERR_NOMEM, "small device buffers");
