@@ -59,6 +59,8 @@ extern "C" {
 #define SPM_AXIS_Y 2
 #define SPM_AXIS_Z 3
 
+#define SPM_MAX_SPECIES 4  /* particle species (Particle_spec[0..3]) */
+
 #define SPM_PREC_FP64 0        /* every field and reduction in FP64 */
 #define SPM_PREC_FP32_MIXED 1  /* fields/FFT/projection FP32, particle reductions and updates FP64 */
 
@@ -107,6 +109,15 @@ typedef struct spm_params {
     double rotlet_c2;            /* SQUIRMER: janus_rotlet_dipole_C2 */
     double slip_tol;             /* switch.SLIP_tol */
     int    slip_iter;            /* switch.SLIP_iter */
+    /* Several particle species (Particle_spec[0..n_species-1], input.cxx:1403-1441).  n_species <= 1:
+     * one species, described by n_particles, mass_ratio and surface_charge above.  n_species > 1: the
+     * n_particles records are consecutive blocks of species_count[s] particles, species 0 first (the
+     * reference's p[n].spec order); each species has its own MASS_RATIO and Surface_charge, all share
+     * A, A_XI and the janus settings (which must be OFF). */
+    int    n_species;
+    int    species_count[SPM_MAX_SPECIES];
+    double species_mass_ratio[SPM_MAX_SPECIES];
+    double species_surface_charge[SPM_MAX_SPECIES];
 } spm_params;
 
 typedef struct spm_ctx spm_ctx;

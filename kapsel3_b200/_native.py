@@ -19,6 +19,7 @@ SPM_EQ_LEES_EDWARDS = 1
 SPM_EQ_ELECTROLYTE = 2
 SPM_JANUS_OFF, SPM_JANUS_TUMBLER, SPM_JANUS_SQUIRMER, SPM_JANUS_OBSTACLE = 0, 1, 2, 3
 SPM_AXIS_NONE, SPM_AXIS_X, SPM_AXIS_Y, SPM_AXIS_Z = 0, 1, 2, 3
+SPM_MAX_SPECIES = 4
 SPM_PREC_FP64 = 0
 SPM_PREC_FP32_MIXED = 1
 
@@ -57,6 +58,10 @@ class SpmParams(C.Structure):
         ("rotlet_c2", C.c_double),
         ("slip_tol", C.c_double),
         ("slip_iter", C.c_int),
+        ("n_species", C.c_int),
+        ("species_count", C.c_int * 4),
+        ("species_mass_ratio", C.c_double * 4),
+        ("species_surface_charge", C.c_double * 4),
     ]
 
 

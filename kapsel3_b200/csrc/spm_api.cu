@@ -273,6 +273,20 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
     if (p.npx < 3 || p.npx > 9 || p.npy < 3 || p.npy > 9 || p.npz < 3 || p.npz > 9)
         return fail(SPM_ERR_ARG, "mesh.NPX/NPY/NPZ must be in [3, 9] (grid 8..512 per axis)");
     if (p.n_particles < 0) return fail(SPM_ERR_ARG, "negative particle count");
+    // particle species (input.cxx:1403-1441)
+    const int nsp = p.n_species > 1 ? p.n_species : 1;
+    if (nsp > SPM_MAX_SPECIES) return fail(SPM_ERR_ARG, "at most SPM_MAX_SPECIES particle species");
+    if (nsp > 1) {
+        int sum = 0;
+        for (int s = 0; s < nsp; s++) {
+            if (p.species_count[s] < 0) return fail(SPM_ERR_ARG, "negative species_count");
+            if (!(p.species_mass_ratio[s] > 0.0)) return fail(SPM_ERR_ARG, "species_mass_ratio must be > 0");
+            sum += p.species_count[s];
+        }
+        if (sum != p.n_particles) return fail(SPM_ERR_ARG, "species_count must add up to n_particles");
+        if (p.janus_propulsion != SPM_JANUS_OFF) return fail(SPM_ERR_ARG, "janus particles need a single species");
+    }
+    auto charge_of = [&](int s) { return nsp > 1 ? p.species_surface_charge[s] : p.surface_charge; };
     if (!(p.dx > 0) || !(p.rho > 0) || !(p.eta > 0) || !(p.dt > 0)) return fail(SPM_ERR_ARG, "DX, RHO, ETA, dt must be > 0");
     if (p.precision != SPM_PREC_FP64 && p.precision != SPM_PREC_FP32_MIXED) return fail(SPM_ERR_ARG, "bad precision");
     if (p.equation != SPM_EQ_NAVIER_STOKES && p.equation != SPM_EQ_LEES_EDWARDS && p.equation != SPM_EQ_ELECTROLYTE)
@@ -280,11 +294,15 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
     if (p.equation == SPM_EQ_ELECTROLYTE) {
         // Init_rho_ion's checks (operate_electrolyte.cxx:668-720)
         if (p.precision != SPM_PREC_FP64) return fail(SPM_ERR_ARG, "Electrolyte runs are FP64 only");
-        if (p.surface_charge == 0.0) return fail(SPM_ERR_ARG, "Electrolyte needs a nonzero Surface_charge");
+        for (int s = 0; s < nsp; s++)
+            if (charge_of(s) == 0.0) return fail(SPM_ERR_ARG, "Electrolyte needs a nonzero Surface_charge");
+        for (int s = 1; s < nsp && p.salt == 0; s++)  // saltfree: colloids of one sign (operate_electrolyte.cxx:712-723)
+            if (charge_of(0) * charge_of(s) <= 0.0)
+                return fail(SPM_ERR_ARG, "saltfree runs need colloids of one sign; select salt in Add_salt");
         if (!(p.dielectric > 0.0)) return fail(SPM_ERR_ARG, "Dielectric_cst must be > 0");
         if (p.init_pb && p.salt == 1 && p.n_particles == 1 && p.valency[0] != -p.valency[1])
             return fail(SPM_ERR_ARG, "Poisson_Boltzmann with salt needs Valency_positive_ion = -Valency_negative_ion");
-        if (p.salt == 0 && !(p.valency[0] * p.surface_charge < 0.0))
+        if (p.salt == 0 && nsp == 1 && !(p.valency[0] * p.surface_charge < 0.0))
             return fail(SPM_ERR_ARG, "Valency_counterion must have the opposite sign of Surface_charge");
         if (p.salt == 1 && !(p.valency[0] > 0.0 && p.valency[1] < 0.0))
             return fail(SPM_ERR_ARG, "salt needs Valency_positive_ion > 0 and Valency_negative_ion < 0");
@@ -361,6 +379,16 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
     ph.noise_v = 1.439 * sqrt(zeta_drag * p.dt * p.kbt * p.alpha_v);
     ph.noise_o = 1.22 * sqrt(zeta_drag_rot * p.dt * p.kbt * p.alpha_o);
     ph.np      = p.n_particles;
+    ph.nsp     = nsp;
+    for (int s = 0, end = 0; s < SPM_MAX_SPECIES; s++) {
+        const double mr = nsp > 1 ? p.species_mass_ratio[s < nsp ? s : 0] : p.mass_ratio;
+        const double ms = mr * p.rho * 4.0 / 3.0 * M_PI * radius * radius * radius;
+        end += s < nsp ? (nsp > 1 ? p.species_count[s] : p.n_particles) : 0;
+        ph.spec_end[s] = end;
+        ph.imass_s[s]  = 1.0 / ms;
+        ph.imoi_s[s]   = 1.0 / (2.0 / 5.0 * ms * radius * radius);
+        ph.qe_s[s]     = s < nsp ? charge_of(s) : 0.0;  // Elementary_charge = 1
+    }
     ph.janus_prop = p.janus_propulsion;
     ph.janus_axis = p.janus_axis;
     for (int d = 0; d < 3; d++) {
@@ -1025,10 +1053,16 @@ void el_init_state(ELState &el, const spm_params &p) {
     el.enabled     = 1;
     el.nspec       = p.salt ? 2 : 1;
     el.iepsilon    = 1.0 / p.dielectric;
-    el.qe          = p.surface_charge * e;
+    const int nsp  = p.n_species > 1 ? p.n_species : 1;
+    auto      cnt  = [&](int s) { return nsp > 1 ? p.species_count[s] : p.n_particles; };
+    auto      chg  = [&](int s) { return nsp > 1 ? p.species_surface_charge[s] : p.surface_charge; };
+    el.qe          = chg(0) * e;
     el.abs_q       = 0.0;
-    for (int n = 0; n < p.n_particles; n++) el.abs_q += fabs(el.qe);
-    const double surface_ion_number = -p.surface_charge * p.n_particles;
+    double surface_ion_number = 0.0;
+    for (int s = 0; s < nsp; s++) {
+        for (int n = 0; n < cnt(s); n++) el.abs_q += fabs(chg(s) * e);
+        surface_ion_number -= chg(s) * cnt(s);
+    }
     el.surface_ion_number           = surface_ion_number;
     el.init_pb                      = p.init_pb;
     for (int n = 0; n < el.nspec; n++) {
@@ -1038,9 +1072,16 @@ void el_init_state(ELState &el, const spm_params &p) {
     if (el.nspec == 1) {
         el.counterion_number = surface_ion_number / p.valency[0];
     } else {
-        const double qn = p.surface_charge * (double)p.n_particles;
-        el.ion_number[0] = p.surface_charge < 0. ? fabs(qn / p.valency[0]) : 0.0;
-        el.ion_number[1] = p.surface_charge > 0. ? fabs(qn / p.valency[1]) : 0.0;
+        // counterions of every species by the sign of its charge (Set_uniform_ion_charge_density_salt,
+        // operate_electrolyte.cxx:498-507)
+        el.ion_number[0] = el.ion_number[1] = 0.0;
+        for (int s = 0; s < nsp; s++) {
+            const double qn = chg(s) * (double)cnt(s);
+            if (chg(s) < 0.)
+                el.ion_number[0] += fabs(qn / p.valency[0]);
+            else if (chg(s) > 0.)
+                el.ion_number[1] += fabs(qn / p.valency[1]);
+        }
         const double rho_inf = p.kbt * p.dielectric / ((e * p.debye_length) * (e * p.debye_length));
         el.rho_inf[0]        = rho_inf / (p.valency[0] * (p.valency[0] - p.valency[1]));
         el.rho_inf[1]        = -rho_inf / (p.valency[1] * (p.valency[0] - p.valency[1]));

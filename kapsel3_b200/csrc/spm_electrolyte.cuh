@@ -74,7 +74,7 @@ __global__ void s_el_phi_qq(Grid g, Phys ph, const double *__restrict__ x, const
     StencilPoint s;
     stencil_point(g, ph, xp, cells[m], s);
     const double v  = phi_prof(s.dist, ph.radius, ph.hxi, g.dx);
-    const double dq = qe * dphi_compact_sin(s.dist, ph.radius, 2.0 * ph.hxi);
+    const double dq = ph.qe_s[spec_of(ph, p)] * dphi_compact_sin(s.dist, ph.radius, 2.0 * ph.hxi);  // Surface_charge_e[p.spec]
     if (v != 0.0) atomicAdd(&phi[s.idx], (T)v);
     if (dq != 0.0) atomicAdd(&surface[s.idx], (T)dq);
 }

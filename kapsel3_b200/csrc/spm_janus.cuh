@@ -334,8 +334,8 @@ __global__ void p_velocity_slip(Phys ph, PState s, double *__restrict__ slip, co
     double *sp = slip + (size_t)n * kSlipWords;
     if (mode == 0) {
         const int    euler = *ts_dev == 0;
-        const double dmy   = (euler ? ph.dt : ph.hdt) * ph.imass;
-        const double dmr   = (euler ? ph.dt : ph.hdt) * ph.imoi;
+        const double dmy   = (euler ? ph.dt : ph.hdt) * ph.imass_s[spec_of(ph, n)];
+        const double dmr   = (euler ? ph.dt : ph.hdt) * ph.imoi_s[spec_of(ph, n)];
         double       sf[3], st[3];
         self_propulsion_d(ph, s.q + 4 * n, sf, st);
         for (int d = 0; d < 3; d++) {

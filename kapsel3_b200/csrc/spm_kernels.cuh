@@ -49,7 +49,19 @@ struct Phys {
     double slip_b1, slip_mode;               // SQUIRMER: B1, alpha/2
     double slip_c1, slip_c2;                 // SQUIRMER: rotlet C1, rotlet dipole C2
     double xi;                               // XI = A_XI DX
+    // particle species: particles [spec_end[s-1], spec_end[s]) are species s
+    int    nsp;
+    int    spec_end[4];
+    double imass_s[4], imoi_s[4];
+    double qe_s[4];  // Surface_charge_e per species (Electrolyte)
 };
+
+// p[n].spec: the species of particle n (consecutive blocks, species 0 first)
+__device__ __forceinline__ int spec_of(const Phys &ph, int n) {
+    int s = 0;
+    while (s + 1 < ph.nsp && n >= ph.spec_end[s]) s++;
+    return s;
+}
 
 // k index decomposition: element (i, j, kz) of a k-space field.
 struct KPoint {
@@ -1072,8 +1084,9 @@ __device__ __forceinline__ void self_propulsion_d(const Phys &ph, const double *
 }
 
 __device__ __forceinline__ void velocity_update_one(const Phys &ph, const PState &s, int n, int euler) {
-    const double dmy = (euler ? ph.dt : ph.hdt) * ph.imass;
-    const double dmr = (euler ? ph.dt : ph.hdt) * ph.imoi;
+    const int    sp  = spec_of(ph, n);
+    const double dmy = (euler ? ph.dt : ph.hdt) * ph.imass_s[sp];
+    const double dmr = (euler ? ph.dt : ph.hdt) * ph.imoi_s[sp];
     double       sf[3], st[3];
     self_propulsion_d(ph, s.q + 4 * n, sf, st);
     for (int d = 0; d < 3; d++) {
@@ -1118,8 +1131,9 @@ __global__ void p_velocity_mdf(Phys ph, PState s, const int *__restrict__ ts_dev
         const int i = 3 * n + d;
         s.mdf[i]    = euler ? ph.dt * s.fr[i] : ph.hdt * (s.fr[i] + s.fr_previous[i]);
     }
-    const double dmy = (euler ? ph.dt : ph.hdt) * ph.imass;
-    const double dmr = (euler ? ph.dt : ph.hdt) * ph.imoi;
+    const int    sp  = spec_of(ph, n);
+    const double dmy = (euler ? ph.dt : ph.hdt) * ph.imass_s[sp];
+    const double dmr = (euler ? ph.dt : ph.hdt) * ph.imoi_s[sp];
     for (int d = 0; d < 3; d++) {
         const int i    = 3 * n + d;
         s.v_old[i]     = s.v[i];
@@ -1259,9 +1273,9 @@ __global__ void __launch_bounds__(kThermoThreads) p_thermostat(Phys ph, PState s
             for (int e = 0; e < 2; e++) {
                 const int q = 2 * k + e;  // normal index of particle n
                 if (q < 3)
-                    s.v[3 * n + q] += g[e] * ph.noise_v * ph.imass;
+                    s.v[3 * n + q] += g[e] * ph.noise_v * ph.imass_s[spec_of(ph, n)];
                 else if (ph.rotation)
-                    s.omega[3 * n + q - 3] += g[e] * ph.noise_o * ph.imoi;
+                    s.omega[3 * n + q - 3] += g[e] * ph.noise_o * ph.imoi_s[spec_of(ph, n)];
             }
             if (before == need - 1) sh_used = 2 * (tid + 1);  // uniforms consumed this round
         }

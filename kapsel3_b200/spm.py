@@ -90,6 +90,10 @@ def params_from_config(cfg: SPMConfig, precision: int = N.SPM_PREC_FP64,
     p.slip_vel, p.slip_mode = cfg.slip_vel, cfg.slip_mode
     p.rotlet_c1, p.rotlet_c2 = cfg.rotlet_c1, cfg.rotlet_c2
     p.slip_tol, p.slip_iter = cfg.slip_tol, int(cfg.slip_iter)
+    if len(cfg.species) > 1:
+        p.n_species = len(cfg.species)
+        for i, (cnt, mr, q) in enumerate(cfg.species):
+            p.species_count[i], p.species_mass_ratio[i], p.species_surface_charge[i] = int(cnt), float(mr), float(q)
     return p
 
 
@@ -132,7 +136,9 @@ def config_from_udf(path: str) -> Tuple[SPMConfig, Dict[str, np.ndarray]]:
         janus_propulsion=("OFF", "TUMBLER", "SQUIRMER", "OBSTACLE")[p.janus_propulsion],
         janus_force=tuple(p.janus_force), janus_torque=tuple(p.janus_torque), slip_vel=p.slip_vel,
         slip_mode=p.slip_mode, rotlet_c1=p.rotlet_c1, rotlet_c2=p.rotlet_c2, slip_tol=p.slip_tol,
-        slip_iter=p.slip_iter)
+        slip_iter=p.slip_iter,
+        species=tuple((p.species_count[i], p.species_mass_ratio[i], p.species_surface_charge[i])
+                      for i in range(p.n_species)) if p.n_species > 1 else ())
     return cfg, unpack_particles(rec[:p.n_particles])
 
 

@@ -80,6 +80,10 @@ class SPMConfig:
     rotlet_c2: float = 0.0             # SQUIRMER: janus_rotlet_dipole_C2
     slip_tol: float = 1e-5             # switch.SLIP_tol
     slip_iter: int = 100               # switch.SLIP_iter
+    # Several particle species: ((count, MASS_RATIO, Surface_charge), ...) for Particle_spec[0..], the
+    # counts adding up to n_particles (species 0 first); empty: one species (n_particles, mass_ratio,
+    # surface_charge)
+    species: tuple = ()
 
     # ------------------------------------------------------------------
     @property
@@ -216,9 +220,15 @@ def udf_keys(cfg: SPMConfig, particles: Dict[str, np.ndarray],
         k[f"{base}.External_field.DC.Shear_rate"] = _fmt(float(cfg.shear_rate))
     k["object_type.type"] = "spherical_particle"
     ps = "object_type.spherical_particle.Particle_spec[0]"
-    k[f"{ps}.Particle_number"] = str(cfg.n_particles)
-    k[f"{ps}.MASS_RATIO"] = _fmt(float(cfg.mass_ratio))
-    k[f"{ps}.Surface_charge"] = _fmt(float(cfg.surface_charge))
+    spec = cfg.species if len(cfg.species) > 1 else ((cfg.n_particles, cfg.mass_ratio, cfg.surface_charge),)
+    for i, (cnt, mr, q) in enumerate(spec):
+        pi = f"object_type.spherical_particle.Particle_spec[{i}]"
+        k[f"{pi}.Particle_number"] = str(int(cnt))
+        k[f"{pi}.MASS_RATIO"] = _fmt(float(mr))
+        k[f"{pi}.Surface_charge"] = _fmt(float(q))
+        if i > 0:
+            k[f"{pi}.janus_axis"] = "NONE"
+            k[f"{pi}.janus_propulsion"] = "OFF"
     k[f"{ps}.janus_axis"] = cfg.janus_axis
     k[f"{ps}.janus_propulsion"] = cfg.janus_propulsion
     if cfg.janus_propulsion == "TUMBLER":

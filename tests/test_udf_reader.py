@@ -46,6 +46,7 @@ CASES = {
     "squirmer": SPMConfig(npx=5, npy=5, npz=5, n_particles=2, a=4.0, janus_axis="Y", janus_propulsion="SQUIRMER",
                           slip_vel=0.015, slip_mode=-2.5, rotlet_c1=0.003, rotlet_c2=-0.001, slip_tol=2e-3,
                           slip_iter=7),
+    "two_species": SPMConfig(npx=5, npy=5, npz=5, n_particles=3, a=4.0, species=((1, 1.0, 0.0), (2, 2.5, 0.0))),
     "tumbler": SPMConfig(npx=5, npy=5, npz=5, n_particles=2, a=4.0, janus_axis="Z", janus_propulsion="TUMBLER",
                          janus_force=(0.01, 0.0, -0.02), janus_torque=(0.0, 0.005, 0.0)),
 }
@@ -261,13 +262,21 @@ def test_every_reference_example_parses_and_in_scope_ones_load():
         janus = spherical and kv[ps + "janus_propulsion"] != "OFF"
         eq_ok = kv["constitutive_eq.type"] == "Navier_Stokes" or (
             kv["constitutive_eq.type"] in (EQ_LE, "Electrolyte") and not janus)
-        in_scope = (eq_ok and spherical
-                    and "object_type.spherical_particle.Particle_spec[1].Particle_number" not in kv)
+        in_scope = eq_ok and spherical
         assert (rc == 0) == in_scope, (f, N.lib().spm_last_error())
         if rc == 0:
             loaded += 1
             assert (p.npx, p.npy, p.npz) == tuple(int(kv[f"mesh.NP{a}"]) for a in "XYZ")
-            assert p.n_particles == int(kv["object_type.spherical_particle.Particle_spec[0].Particle_number"])
+            counts = []
+            while f"object_type.spherical_particle.Particle_spec[{len(counts)}].Particle_number" in kv:
+                counts.append(int(kv[f"object_type.spherical_particle.Particle_spec[{len(counts)}].Particle_number"]))
+            assert p.n_particles == sum(counts)
+            if len(counts) > 1:
+                assert p.n_species == len(counts) and list(p.species_count)[:len(counts)] == counts
+                for i in range(len(counts)):
+                    sp = f"object_type.spherical_particle.Particle_spec[{i}]."
+                    assert p.species_mass_ratio[i] == float(kv[sp + "MASS_RATIO"])
+                    assert p.species_surface_charge[i] == float(kv[sp + "Surface_charge"])
             assert p.a == float(kv["A"]) and p.a_xi == float(kv["A_XI"])
             eq = kv["constitutive_eq.type"]
             assert p.eta == float(kv[f"constitutive_eq.{eq}.ETA"])
@@ -301,12 +310,12 @@ def test_every_reference_example_parses_and_in_scope_ones_load():
 
 
 def test_janus_config_round_trip(tmp_path):
-    for name in ("squirmer", "tumbler"):
+    for name in ("squirmer", "tumbler", "two_species"):
         cfg = CASES[name]
         parts = make_particles(cfg, seed=3, random_orientation=True)
         path = str(tmp_path / f"{name}.udf")
         write_udf(path, cfg, parts)
         got, _ = config_from_udf(path)
         for f in ("janus_axis", "janus_propulsion", "janus_force", "janus_torque", "slip_vel", "slip_mode",
-                  "rotlet_c1", "rotlet_c2", "slip_tol", "slip_iter"):
+                  "rotlet_c1", "rotlet_c2", "slip_tol", "slip_iter", "species"):
             assert getattr(got, f) == getattr(cfg, f), (name, f)
