@@ -48,6 +48,7 @@ extern "C" {
 #define SPM_EQ_NAVIER_STOKES 0  /* constitutive_eq.type = Navier_Stokes */
 #define SPM_EQ_LEES_EDWARDS 1   /* Shear_Navier_Stokes_Lees_Edwards */
 #define SPM_EQ_ELECTROLYTE 2    /* Electrolyte: charged colloids with mobile ions */
+#define SPM_EQ_SHEAR_NAVIER_STOKES 3 /* Shear_Navier_Stokes: periodic box, mean shear sustained on fluid planes */
 
 /* Particle_spec[0].janus_propulsion (input.cxx:1427-1441) and janus_axis (1410-1425) */
 #define SPM_JANUS_OFF 0       /* "OFF": passive colloids */
@@ -118,6 +119,10 @@ typedef struct spm_params {
     int    species_count[SPM_MAX_SPECIES];
     double species_mass_ratio[SPM_MAX_SPECIES];
     double species_surface_charge[SPM_MAX_SPECIES];
+    /* Shear_Navier_Stokes (constitutive_eq.Shear_Navier_Stokes.External_field, input.cxx:770-793): the
+     * shear rate is shear_rate above; shear_ac = 0 DC, 1 AC with angular frequency shear_frequency */
+    int    shear_ac;
+    double shear_frequency;
 } spm_params;
 
 typedef struct spm_ctx spm_ctx;

@@ -17,6 +17,7 @@ SPM_PARTICLE_WORDS = 44
 SPM_EQ_NAVIER_STOKES = 0
 SPM_EQ_LEES_EDWARDS = 1
 SPM_EQ_ELECTROLYTE = 2
+SPM_EQ_SHEAR_NAVIER_STOKES = 3
 SPM_JANUS_OFF, SPM_JANUS_TUMBLER, SPM_JANUS_SQUIRMER, SPM_JANUS_OBSTACLE = 0, 1, 2, 3
 SPM_AXIS_NONE, SPM_AXIS_X, SPM_AXIS_Y, SPM_AXIS_Z = 0, 1, 2, 3
 SPM_MAX_SPECIES = 4
@@ -62,6 +63,8 @@ class SpmParams(C.Structure):
         ("species_count", C.c_int * 4),
         ("species_mass_ratio", C.c_double * 4),
         ("species_surface_charge", C.c_double * 4),
+        ("shear_ac", C.c_int),
+        ("shear_frequency", C.c_double),
     ]
 
 

@@ -217,7 +217,9 @@ struct spm_ctx {
 
     bool fp64() const { return P.precision == SPM_PREC_FP64; }
     // zeta kept as a compensated FP32 pair (FP32-mixed Navier_Stokes)
-    bool compensated() const { return !fp64() && P.equation == SPM_EQ_NAVIER_STOKES; }
+    bool compensated() const {
+        return !fp64() && (P.equation == SPM_EQ_NAVIER_STOKES || P.equation == SPM_EQ_SHEAR_NAVIER_STOKES);
+    }
     template <typename T>
     cplx<T> *zl(int d) const {
         return compensated() ? cx<T>(ZL0 + d) : nullptr;
@@ -289,8 +291,11 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
     auto charge_of = [&](int s) { return nsp > 1 ? p.species_surface_charge[s] : p.surface_charge; };
     if (!(p.dx > 0) || !(p.rho > 0) || !(p.eta > 0) || !(p.dt > 0)) return fail(SPM_ERR_ARG, "DX, RHO, ETA, dt must be > 0");
     if (p.precision != SPM_PREC_FP64 && p.precision != SPM_PREC_FP32_MIXED) return fail(SPM_ERR_ARG, "bad precision");
-    if (p.equation != SPM_EQ_NAVIER_STOKES && p.equation != SPM_EQ_LEES_EDWARDS && p.equation != SPM_EQ_ELECTROLYTE)
+    if (p.equation != SPM_EQ_NAVIER_STOKES && p.equation != SPM_EQ_LEES_EDWARDS && p.equation != SPM_EQ_ELECTROLYTE &&
+        p.equation != SPM_EQ_SHEAR_NAVIER_STOKES)
         return fail(SPM_ERR_ARG, "bad equation");
+    if (p.equation == SPM_EQ_SHEAR_NAVIER_STOKES && (p.shear_ac < 0 || p.shear_ac > 1))
+        return fail(SPM_ERR_ARG, "shear_ac must be 0 (DC) or 1 (AC)");
     if (p.equation == SPM_EQ_ELECTROLYTE) {
         // Init_rho_ion's checks (operate_electrolyte.cxx:668-720)
         if (p.precision != SPM_PREC_FP64) return fail(SPM_ERR_ARG, "Electrolyte runs are FP64 only");
@@ -314,8 +319,9 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
     if (p.janus_propulsion < SPM_JANUS_OFF || p.janus_propulsion > SPM_JANUS_OBSTACLE)
         return fail(SPM_ERR_ARG, "bad janus_propulsion");
     if (p.janus_axis < SPM_AXIS_NONE || p.janus_axis > SPM_AXIS_Z) return fail(SPM_ERR_ARG, "bad janus_axis");
-    if (p.janus_propulsion != SPM_JANUS_OFF && p.equation != SPM_EQ_NAVIER_STOKES)
-        return fail(SPM_ERR_ARG, "janus particles are served in Navier_Stokes runs only");
+    if (p.janus_propulsion != SPM_JANUS_OFF && p.equation != SPM_EQ_NAVIER_STOKES &&
+        p.equation != SPM_EQ_SHEAR_NAVIER_STOKES)
+        return fail(SPM_ERR_ARG, "janus particles are served in Navier_Stokes and Shear_Navier_Stokes runs only");
     if (p.janus_propulsion == SPM_JANUS_SQUIRMER) {
         if (p.janus_axis == SPM_AXIS_NONE) return fail(SPM_ERR_ARG, "a SQUIRMER needs a janus_axis (X, Y or Z)");
         if (!(p.slip_vel > 0.0)) return fail(SPM_ERR_ARG, "a SQUIRMER needs janus_slip_vel (B1) > 0");
@@ -371,7 +377,8 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
         ph.lc[d]         = n[d] / 16;
     }
     ph.cell_len = 16.0 * p.dx;
-    if (ph.lj_on && p.equation == SPM_EQ_NAVIER_STOKES && (ph.lc[0] < 1 || ph.lc[1] < 1 || ph.lc[2] < 1))
+    if (ph.lj_on && (p.equation == SPM_EQ_NAVIER_STOKES || p.equation == SPM_EQ_SHEAR_NAVIER_STOKES) &&
+        (ph.lc[0] < 1 || ph.lc[1] < 1 || ph.lc[2] < 1))
         return fail(SPM_ERR_ARG, "the reference LJ cell list needs N >= 16 on every axis");
     // Thermostat intensities (fluct.cxx:11-18).
     const double zeta_drag     = 6.0 * M_PI * p.eta * radius;
@@ -719,6 +726,29 @@ int slip_loop(spm_ctx *c) {
     return SPM_OK;
 }
 
+// Mean-shear sustaining step of NS_solver_slavedEuler_Shear_PBC (fluid_solver.
+// cxx:377-409): u of the updated zeta (every mode), u_x set on the shear
+// planes (DC) or to the oscillating profile at t = ts dt (AC), zeta and uk_dc
+// from it (U2zeta_k), then zeta truncated in place as Time_evolution_hydro
+// does next (sp_3d_ns.cxx:54-56); a fresh zeta has no compensation residue.
+template <typename T>
+int shear_sustain(spm_ctx *c) {
+    SPM_TRY(zeta_to_velocity<T>(c, 0));
+    const double t   = (double)c->ts * c->ph.dt;
+    const double amp = c->P.shear_ac ? cos(c->P.shear_frequency * t) : 1.0;
+    LAUNCH(c, r_shear_sustain<T>, c->grid_blocks(), 256, 0, c->g, c->real<T>(U0), c->P.shear_ac, c->P.shear_rate,
+           c->ph.L[1], amp);
+    SPM_TRY(fft_fwd<T>(c, U0, 3));
+    LAUNCH(c, k_u_to_zeta<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(U0), c->cx<T>(U1), c->cx<T>(U2),
+           c->cx<T>(Z0), c->cx<T>(Z1), c->uk_dc);
+    LAUNCH(c, k_truncate2<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(Z0), c->cx<T>(Z1));
+    if (c->compensated()) {
+        SPM_CUDA_CHECK(cudaMemsetAsync(c->real<T>(ZL0), 0, c->field_bytes(), c->st));
+        SPM_CUDA_CHECK(cudaMemsetAsync(c->real<T>(ZL1), 0, c->field_bytes(), c->st));
+    }
+    return SPM_OK;
+}
+
 // Zero UP0, UP1, UP2 and PHIS of every run of L in one memset (the slots are
 // consecutive; in a pool the span also covers free run slots).
 template <typename T>
@@ -799,6 +829,7 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
     }
     if (L->overlap) SPM_CUDA_CHECK(cudaEventRecord(L->ev_join, side));
     if ((rc = ns_solver<T>(L)) != SPM_OK) return rc;
+    if (L->P.equation == SPM_EQ_SHEAR_NAVIER_STOKES) SPM_TRY(shear_sustain<T>(L));  // lone runs only
     LAUNCH(L, k_fix_cell, (nr + 127) / 128, 128, 0, L->rw, nr);
     if ((rc = zeta_to_velocity<T>(L, 1)) != SPM_OK) return rc;
     if (L->overlap) SPM_CUDA_CHECK(cudaStreamWaitEvent(L->st, L->ev_join, 0));  // join
@@ -846,7 +877,9 @@ int initialize_impl(spm_ctx *c) {
     if ((rc = zeta_to_velocity<T>(c, 1)) != SPM_OK) return rc;
     if ((rc = rigidity_projection<T>(c)) != SPM_OK) return rc;
     LAUNCH(c, k_zero3, 1, 32, 0, c->uk_dc);
-    if (c->le.enabled && c->ph.np > 0) LAUNCH(c, p_le_zero_vx, particle_blocks(c), 128, 0, c->ph, c->ps);
+    // shear runs start with v_x = omega_z = 0 (init_particle.cxx:768-781)
+    if ((c->le.enabled || c->P.equation == SPM_EQ_SHEAR_NAVIER_STOKES) && c->ph.np > 0)
+        LAUNCH(c, p_le_zero_vx, particle_blocks(c), 128, 0, c->ph, c->ps);
     c->ts   = 0;
     c->time = 0.0;
     return SPM_OK;
@@ -1226,7 +1259,7 @@ int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *
         destroy_ctx(c);
         return fail(SPM_ERR_NOMEM, "small device buffers");
     }
-    if (p.equation == SPM_EQ_NAVIER_STOKES && p.n_particles > 0) {
+    if ((p.equation == SPM_EQ_NAVIER_STOKES || p.equation == SPM_EQ_SHEAR_NAVIER_STOKES) && p.n_particles > 0) {
         const size_t nsc = (size_t)p.n_particles * cells.size();
         if (dev_alloc((void **)&c->sc_idx, nsc * sizeof(int)) != cudaSuccess ||
             dev_alloc((void **)&c->sc_w, nsc * sizeof(double)) != cudaSuccess) {
@@ -1349,7 +1382,8 @@ int spm_device_bytes(const spm_params *p, size_t *bytes) {
     const size_t es  = p->precision == SPM_PREC_FP64 ? 8 : 4;
     const size_t fld = (size_t)g.nx * g.ny * g.hnzp * 2 * es;
     const size_t nslot = (size_t)slots_for(*p);
-    const size_t sc = p->equation == SPM_EQ_NAVIER_STOKES ? (size_t)p->n_particles * sekibun(*p).size() * 12 : 0;
+    const bool   ns = p->equation == SPM_EQ_NAVIER_STOKES || p->equation == SPM_EQ_SHEAR_NAVIER_STOKES;
+    const size_t sc = ns ? (size_t)p->n_particles * sekibun(*p).size() * 12 : 0;
     *bytes = nslot * fld + (size_t)std::max(p->n_particles, 1) * kPWords * 8 + sc + 64 * 1024;
     return SPM_OK;
 }

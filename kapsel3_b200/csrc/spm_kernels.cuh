@@ -56,6 +56,31 @@ struct Phys {
     double qe_s[4];  // Surface_charge_e per species (Electrolyte)
 };
 
+// Mean-shear sustaining force of Shear_Navier_Stokes on the real-space u_x
+// (Mean_shear_sustaining_yforce_PBC / _kforce_PBC, fluid_solver.cxx:41-119).
+// DC: u_x = -/+ Shear_rate (LY/4) DX on the planes j = NY/4, 3NY/4.  AC:
+// u_x = zigzag(j) cos(omega t) everywhere, zigzag = -rate j DX for j < LY/4,
+// rate (LY - j DX) in the last quarter, rate (j DX - LY/2) between.
+template <typename T>
+__global__ void r_shear_sustain(Grid g, T *__restrict__ u0, int ac, double rate, double ly, double amp) {
+    const size_t rowlen = 2 * (size_t)g.hnzp;
+    const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    const double qly = ly / 4., hly = ly / 2.;
+    const int    j1 = g.ny / 4, j2 = 3 * g.ny / 4;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if ((int)(idx % rowlen) >= g.nz) continue;
+        const int j = (int)((idx / rowlen) % (size_t)g.ny);
+        if (!ac) {
+            if (j == j1) u0[idx] = (T)(-(rate * qly * g.dx));
+            if (j == j2) u0[idx] = (T)(rate * qly * g.dx);
+        } else {
+            const int    q = (int)(j / qly);
+            const double v = q == 0 ? -rate * j * g.dx : (q == 3 ? rate * ly - rate * j * g.dx : -rate * hly + rate * j * g.dx);
+            u0[idx]        = (T)(v * amp);
+        }
+    }
+}
+
 // p[n].spec: the species of particle n (consecutive blocks, species 0 first)
 __device__ __forceinline__ int spec_of(const Phys &ph, int n) {
     int s = 0;

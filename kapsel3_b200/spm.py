@@ -19,7 +19,7 @@ from typing import Dict, Optional, Tuple
 import numpy as np
 
 from . import _native as N
-from .udf import EQ_EL, EQ_LE, SPMConfig
+from .udf import EQ_EL, EQ_LE, EQ_NS, EQ_SNS, SPMConfig
 
 RECORD = [("x", 3), ("x_nopbc", 3), ("v", 3), ("v_old", 3), ("omega", 3), ("omega_old", 3),
           ("q", 4), ("q_old", 4), ("f_hydro", 3), ("f_hydro_previous", 3),
@@ -58,8 +58,9 @@ def params_from_config(cfg: SPMConfig, precision: int = N.SPM_PREC_FP64,
     p.npx, p.npy, p.npz = cfg.npx, cfg.npy, cfg.npz
     p.dx, p.rho, p.eta, p.kbt = cfg.dx, cfg.rho, cfg.eta, cfg.kbt
     p.alpha_v, p.alpha_o = cfg.alpha_v, cfg.alpha_o
-    p.equation = {EQ_LE: N.SPM_EQ_LEES_EDWARDS, EQ_EL: N.SPM_EQ_ELECTROLYTE}.get(cfg.equation,
-                                                                                N.SPM_EQ_NAVIER_STOKES)
+    p.equation = {EQ_LE: N.SPM_EQ_LEES_EDWARDS, EQ_EL: N.SPM_EQ_ELECTROLYTE,
+                  EQ_SNS: N.SPM_EQ_SHEAR_NAVIER_STOKES}.get(cfg.equation, N.SPM_EQ_NAVIER_STOKES)
+    p.shear_ac, p.shear_frequency = int(cfg.shear_ac), float(cfg.shear_frequency)
     p.shear_rate = cfg.shear_rate
     p.n_particles = cfg.n_particles
     p.mass_ratio = cfg.mass_ratio
@@ -122,7 +123,9 @@ def config_from_udf(path: str) -> Tuple[SPMConfig, Dict[str, np.ndarray]]:
     cfg = SPMConfig(
         npx=p.npx, npy=p.npy, npz=p.npz, dx=p.dx, rho=p.rho, eta=p.eta, kbt=p.kbt,
         alpha_v=p.alpha_v, alpha_o=p.alpha_o,
-        equation={N.SPM_EQ_LEES_EDWARDS: EQ_LE, N.SPM_EQ_ELECTROLYTE: EQ_EL}.get(p.equation, "Navier_Stokes"),
+        equation={N.SPM_EQ_LEES_EDWARDS: EQ_LE, N.SPM_EQ_ELECTROLYTE: EQ_EL,
+                  N.SPM_EQ_SHEAR_NAVIER_STOKES: EQ_SNS}.get(p.equation, EQ_NS),
+        shear_ac=bool(p.shear_ac), shear_frequency=p.shear_frequency,
         shear_rate=p.shear_rate, n_particles=p.n_particles, mass_ratio=p.mass_ratio, a=p.a, a_xi=p.a_xi,
         epsilon=p.epsilon, lj_powers=("12:6", "24:12", "36:18")[p.lj_powers],
         lj_truncate={1: "ON", 0: "OFF", -1: "NONE"}[p.lj_truncate], rotation=bool(p.rotation),

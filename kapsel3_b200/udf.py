@@ -28,6 +28,7 @@ import numpy as np
 EQ_NS = "Navier_Stokes"
 EQ_LE = "Shear_Navier_Stokes_Lees_Edwards"
 EQ_EL = "Electrolyte"
+EQ_SNS = "Shear_Navier_Stokes"
 
 
 @dataclasses.dataclass
@@ -44,7 +45,9 @@ class SPMConfig:
     alpha_v: float = 1.0
     alpha_o: float = 1.0
     equation: str = EQ_NS        # constitutive_eq.type
-    shear_rate: float = 0.0      # ...Lees_Edwards.External_field.DC.Shear_rate
+    shear_rate: float = 0.0      # ...Lees_Edwards / Shear_Navier_Stokes .External_field.<DC|AC>.Shear_rate
+    shear_ac: bool = False       # Shear_Navier_Stokes: AC oscillatory shear (else DC)
+    shear_frequency: float = 0.0  # Shear_Navier_Stokes AC: Frequency
     n_particles: int = 2         # Particle_spec[0].Particle_number
     mass_ratio: float = 1.0
     a: float = 4.0               # A (radius in units of DX)
@@ -218,6 +221,12 @@ def udf_keys(cfg: SPMConfig, particles: Dict[str, np.ndarray],
     if eq == EQ_LE:
         k[f"{base}.External_field.type"] = "DC"
         k[f"{base}.External_field.DC.Shear_rate"] = _fmt(float(cfg.shear_rate))
+    if eq == EQ_SNS:
+        ft = "AC" if cfg.shear_ac else "DC"
+        k[f"{base}.External_field.type"] = ft
+        k[f"{base}.External_field.{ft}.Shear_rate"] = _fmt(float(cfg.shear_rate))
+        if cfg.shear_ac:
+            k[f"{base}.External_field.AC.Frequency"] = _fmt(float(cfg.shear_frequency))
     k["object_type.type"] = "spherical_particle"
     ps = "object_type.spherical_particle.Particle_spec[0]"
     spec = cfg.species if len(cfg.species) > 1 else ((cfg.n_particles, cfg.mass_ratio, cfg.surface_charge),)

@@ -124,7 +124,7 @@ void __wrap__Z17Output_field_dataPPdS_P8ParticleRK5CTime(double **zeta, double *
     const size_t n_field = (size_t)NX * NY * NZ_;
     // 0: no fields; 1: zeta and phi; 2: zeta, phi and the real-space velocity
     int has_fields = (g_fields_every > 0 && (g_frame % g_fields_every) == 0) ? 1 : 0;
-    if (has_fields && SW_EQ == Navier_Stokes) has_fields = 2;
+    if (has_fields && (SW_EQ == Navier_Stokes || SW_EQ == Shear_Navier_Stokes)) has_fields = 2;
     int          ihdr[2]    = {jikan.ts, has_fields};
     fwrite(ihdr, sizeof(int), 2, g_dump);
     double dhdr[5] = {jikan.time, degree_oblique, uk_dc[0], uk_dc[1], uk_dc[2]};

@@ -57,10 +57,10 @@ def test_udf_key_file_roundtrip():
 def test_udf_rejects_out_of_scope_equation():
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "in.keys")
-        open(path, "w").write("constitutive_eq.type = Shear_Navier_Stokes\n")
+        open(path, "w").write("constitutive_eq.type = Navier_Stokes_FDM\n")
         p = N.SpmParams()
         assert N.lib().spm_params_from_udf_keys(path.encode(), C.byref(p), None, 0) == 1
-        assert b"Shear_Navier_Stokes" in N.lib().spm_last_error()
+        assert b"Navier_Stokes_FDM" in N.lib().spm_last_error()
 
 
 def test_create_without_device_fails_cleanly():

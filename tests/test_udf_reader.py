@@ -260,7 +260,7 @@ def test_every_reference_example_parses_and_in_scope_ones_load():
         spherical = kv["object_type.type"] == "spherical_particle"
         ps = "object_type.spherical_particle.Particle_spec[0]."
         janus = spherical and kv[ps + "janus_propulsion"] != "OFF"
-        eq_ok = kv["constitutive_eq.type"] == "Navier_Stokes" or (
+        eq_ok = kv["constitutive_eq.type"] in ("Navier_Stokes", "Shear_Navier_Stokes") or (
             kv["constitutive_eq.type"] in (EQ_LE, "Electrolyte") and not janus)
         in_scope = eq_ok and spherical
         assert (rc == 0) == in_scope, (f, N.lib().spm_last_error())
@@ -280,8 +280,10 @@ def test_every_reference_example_parses_and_in_scope_ones_load():
             assert p.a == float(kv["A"]) and p.a_xi == float(kv["A_XI"])
             eq = kv["constitutive_eq.type"]
             assert p.eta == float(kv[f"constitutive_eq.{eq}.ETA"])
-            if eq == EQ_LE:
-                assert p.shear_rate == float(kv[f"constitutive_eq.{eq}.External_field.DC.Shear_rate"])
+            if eq in (EQ_LE, "Shear_Navier_Stokes"):
+                ft = kv[f"constitutive_eq.{eq}.External_field.type"]
+                assert p.shear_rate == float(kv[f"constitutive_eq.{eq}.External_field.{ft}.Shear_rate"])
+                assert p.shear_ac == (ft == "AC")
             if eq == "Electrolyte":
                 e = "constitutive_eq.Electrolyte."
                 assert p.equation == N.SPM_EQ_ELECTROLYTE and p.dielectric == float(kv[e + "Dielectric_cst"])
