@@ -59,10 +59,10 @@ __device__ __forceinline__ double dphi_compact_sin(double x, double radius, doub
 }
 
 // Make_phi_qq_particle (operate_electrolyte.cxx:173-208): phi += Phi and
-// surface += Surface_charge_e * |phi_s'| over each particle's stencil.
+// surface += Surface_charge_e[p.spec] * |phi_s'| over each particle's stencil.
 template <typename T>
 __global__ void s_el_phi_qq(Grid g, Phys ph, const double *__restrict__ x, const int *__restrict__ cells, int ncells,
-                            T *__restrict__ phi, T *__restrict__ surface, double qe, unsigned int *err) {
+                            T *__restrict__ phi, T *__restrict__ surface, unsigned int *err) {
     const int p = blockIdx.y;
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= ph.np || m >= ncells) return;
