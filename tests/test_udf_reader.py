@@ -9,9 +9,10 @@ Pins:
 - uniform_random placement and random orientation reproduce glibc's rand()
   stream after srand(10) (drawn here through ctypes from the C library
   itself) and, when the reference program is built, its initial frame;
-- every example input shipped with the reference parses, and the NS /
-  Lees-Edwards spherical-particle ones load (only where the reference tree
-  is present).
+- every example input shipped with the reference parses, and those of
+  spherical particles under Navier_Stokes, Shear_Navier_Stokes,
+  Lees-Edwards or Electrolyte load, squirmers and several species included
+  (only where the reference tree is present).
 No GPU work."""
 import ctypes as C
 import glob
