@@ -6,7 +6,7 @@
  * int status (SPM_OK = 0); on failure the context keeps its last good state
  * and spm_last_error() describes the failure.  The reference's own error
  * convention is exit_job(EXIT_FAILURE) (macro.h:178); the C++ shim that binds
- * the reference-named symbols turns a nonzero status into
+ * the reference-named symbols (kapsel3_b200/shim) turns a nonzero status into
  * exactly that.
  *
  * Field layout.  A k-space field is complex [NX][NY][NZ/2+1] stored as
@@ -268,16 +268,20 @@ int spm_calc_f_lennard_jones_host(spm_ctx *ctx, double *particles_host);
  * larger grids are rejected with SPM_ERR_ARG.  Working memory is one
  * file-scope device array of about 6.5 MB that every GPU loading this
  * library keeps until the process exits; the first call on a device looks
- * up its address (make that call before any stream capture).  Every call
- * shares that array: calls that overlap on the GPU race.  `stream` is a
- * cudaStream_t (NULL: the legacy default stream). */
+ * up its address and uploads the transform tables of every supported size
+ * into it (make that call before any stream capture); later calls only
+ * enqueue kernels and memsets on `stream` and return without waiting.  The
+ * transforms have no device-side waits, so there is no device error to
+ * report.  Every call shares that array: calls that overlap on the GPU
+ * race.  `stream` is a cudaStream_t (NULL: the legacy default stream). */
 int spm_make_f_particle_dt_sole_noalloc(const double *u0, const double *u1, const double *u2, const double *up0,
                                         const double *up1, const double *up2, const double *phi, double *f0,
                                         double *f1, double *f2, int npx, int npy, int npz, void *stream);
 
 /* ---- 3D FFT on device buffers ------------------------------------------- */
 /* In-place transforms of nfields device fields of the context's precision,
- * consecutive fields `field_stride` complex elements apart. */
+ * consecutive fields `field_stride` complex elements apart.  `data` and the
+ * field stride in bytes must be multiples of 16 (SPM_ERR_ARG otherwise). */
 int spm_fft_forward_dev(spm_ctx *ctx, void *data, int nfields, size_t field_stride);
 int spm_fft_inverse_dev(spm_ctx *ctx, void *data, int nfields, size_t field_stride);
 /* Complex elements per allocated field row (NZ/2+1 for FP64; FP32 rows may
@@ -291,6 +295,12 @@ int spm_time_steps(spm_ctx *ctx, int nsteps, float *ms);
  * dominant kernel; returns its average duration (us), algorithmic bytes per
  * launch (one read + one write of every transformed element) and count. */
 int spm_profile_pass(spm_ctx *ctx, int nsteps, double *avg_us, double *bytes_per_launch, long long *count);
+/* Runs n steps (direct launches) with CUDA events around every launch of the
+ * step's transform, k-space and stencil kernels on the stream it runs on, and
+ * writes a JSON summary to json[cap]: per kernel family its launches, total
+ * and per-launch device time (us) and algorithmic bytes per launch, plus the
+ * device time of the n steps. */
+int spm_profile_kernels(spm_ctx *ctx, int nsteps, char *json, size_t cap);
 /* Launches of this library's kernels since the last reset. */
 int spm_kernel_launches(spm_ctx *ctx, long long *count, int reset);
 
@@ -328,6 +338,17 @@ int spm_pool_stats(spm_pool *pool, long long *graph_kernels, int *captures);
 /* Host-side fault injection: the next `count` device allocations of contexts
  * and pools fail with SPM_ERR_NOMEM (0 switches it off). */
 int spm_debug_fail_allocations(int count);
+/* Bound of every device-side wait of the context's TMA transform passes, in
+ * seconds of the GPU's global timer (default 1 s, at most 60).  A wait that
+ * runs out sets the device error bit that the next synchronising call reports
+ * as SPM_ERR_DEVICE ("TMA pipeline wait timed out"); the pass stops and the
+ * context stays usable.  No reference counterpart. */
+int spm_set_wait_limit(spm_ctx *ctx, double seconds);
+/* Test switch for the bounded waits: the context's next `launches` TMA
+ * transform passes issue no tile loads, so their first waits run out with
+ * nothing in flight (0 switches it off).  The steps taken meanwhile run
+ * without graph replay.  No reference counterpart. */
+int spm_debug_skip_tma_loads(spm_ctx *ctx, int launches);
 /* Device blocks of up to 64 MB that destroyed contexts and pools freed are
  * kept for reuse (at most 2 GB per process), because cudaFree waits for the
  * whole device.  This returns them all to the driver; bytes = what was held. */

@@ -155,6 +155,7 @@ _SIGS = {
     "spm_time_steps": (C.c_int, [_P, C.c_int, C.POINTER(C.c_float)]),
     "spm_kernel_launches": (C.c_int, [_P, C.POINTER(C.c_longlong), C.c_int]),
     "spm_profile_pass": (C.c_int, [_P, C.c_int, _D, _D, C.POINTER(C.c_longlong)]),
+    "spm_profile_kernels": (C.c_int, [_P, C.c_int, C.c_char_p, C.c_size_t]),
     "spm_make_f_particle_dt_sole_noalloc": (C.c_int, [_P] * 10 + [C.c_int, C.c_int, C.c_int, _P]),
     "spm_pool_device_bytes": (C.c_int, [C.POINTER(SpmParams), C.c_int, C.POINTER(C.c_size_t),
                                         C.POINTER(C.c_size_t)]),
@@ -170,6 +171,8 @@ _SIGS = {
     "spm_pool_synchronize": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_uint)]),
     "spm_pool_stats": (C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
     "spm_debug_fail_allocations": (C.c_int, [C.c_int]),
+    "spm_set_wait_limit": (C.c_int, [_P, C.c_double]),
+    "spm_debug_skip_tma_loads": (C.c_int, [_P, C.c_int]),
     "spm_release_cached_memory": (C.c_int, [C.POINTER(C.c_size_t)]),
     "spm_server_config_default": (C.c_int, [C.POINTER(SpmServerConfig)]),
     "spm_server_create": (C.c_int, [C.POINTER(SpmServerConfig), C.POINTER(_P)]),

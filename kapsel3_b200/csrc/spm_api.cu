@@ -179,6 +179,7 @@ struct spm_ctx {
     FFTPlan<float>  *pp32 = &plan32;
     spm_pool        *pool = nullptr;  // pool this run belongs to (null for a lone run)
     int *        cells   = nullptr;
+    int *        lj_list = nullptr;  // LJ cell list: count[ncell], cell_of[np], bins[ncell][kLjBin]
     int *        sc_idx  = nullptr;  // stencil cache of the NS step: grid index per (particle, cell)
     double *     sc_w    = nullptr;  // ... and its profile weight
     int          ncells  = 0;
@@ -199,10 +200,16 @@ struct spm_ctx {
     double      *slip     = nullptr;
     double      *slip_eps = nullptr;
     int          slip_iters = 0;  // iterations of the last step's slip loop
-    // optional CUDA-event timing of the strided FFT passes inside real steps
-    bool                     prof_on = false;
-    std::vector<cudaEvent_t> prof_ev;
-    double                   prof_bytes = 0.0;
+    // optional CUDA-event timing of the step's kernels inside real steps:
+    // one record per launch (kernel family, algorithmic bytes, events on the
+    // launching stream)
+    struct ProfRec {
+        const char *name;
+        double      bytes;
+        cudaEvent_t a, b;
+    };
+    bool                 prof_on = false;
+    std::vector<ProfRec> prof;
     bool                     use_tma    = true;  // SPM_NO_TMA=1 selects the direct-load passes
     bool                     overlap    = true;  // SPM_NO_OVERLAP=1 keeps the particle work on the main stream
     bool                     zeta_dirty = false;  // zeta set by the host since the last NS step
@@ -263,6 +270,35 @@ struct spm_ctx {
         cudaError_t _le = cudaGetLastError();                                               \
         if (_le != cudaSuccess) return fail(SPM_ERR_CUDA, std::string("launch " #kern ": ") + \
                                                               cudaGetErrorString(_le));     \
+    } while (0)
+
+// Kernel timing inside real steps (spm_profile_kernels): prof_mark records
+// an event on the context's current stream before a launch, prof_done one
+// after it and files the pair under the kernel family with its algorithmic
+// bytes.  Both do nothing unless profiling is on.
+inline cudaEvent_t prof_mark(spm_ctx *c) {
+    if (!c->prof_on) return nullptr;
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    cudaEventRecord(e, c->st);
+    return e;
+}
+inline void prof_done(spm_ctx *c, cudaEvent_t a, const char *name, double bytes) {
+    if (!a) return;
+    cudaEvent_t b = nullptr;
+    if (cudaEventCreate(&b) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return;
+    }
+    cudaEventRecord(b, c->st);
+    c->prof.push_back({name, bytes, a, b});
+}
+// LAUNCH, timed under `name` with `bytes` algorithmic bytes when profiling.
+#define PLAUNCH(ctx, name, bytes, kern, grid, block, smem, ...)  \
+    do {                                                        \
+        cudaEvent_t _pa = prof_mark(ctx);                       \
+        LAUNCH(ctx, kern, grid, block, smem, __VA_ARGS__);      \
+        prof_done(ctx, _pa, name, (bytes));                     \
     } while (0)
 
 namespace {
@@ -445,6 +481,10 @@ void set_run_words(spm_ctx *c) {
     cudaMemcpy(c->rw, &h, sizeof(h), cudaMemcpyHostToDevice);
 }
 
+// Cells of the reference's LJ cell list (lc[d] = N[d] / 16 per axis).
+int  lj_ncell(const Phys &ph) { return ph.lc[0] * ph.lc[1] * ph.lc[2]; }
+bool lj_cell_list_applies(const Phys &ph) { return ph.lc[0] >= 1 && ph.lc[1] >= 1 && ph.lc[2] >= 1; }
+
 int check_device_error(spm_ctx *c) {
     unsigned int e = 0;
     SPM_CUDA_CHECK(cudaMemcpyAsync(&e, c->err, sizeof(e), cudaMemcpyDeviceToHost, c->st));
@@ -455,6 +495,15 @@ int check_device_error(spm_ctx *c) {
         if (e & SPM_DEVERR_PARTICLE_OUT_OF_BOX) m += " particle outside the periodic box;";
         if (e & SPM_DEVERR_LJ_CELL_OVERFLOW) m += " LJ cell overflow;";
         if (e & SPM_DEVERR_NAN) m += " non-finite value;";
+        if (e & SPM_DEVERR_SCRATCH_TOO_SMALL) m += " scratch buffer too small;";
+        if (e & SPM_DEVERR_TIMEOUT) m += " TMA pipeline wait timed out;";
+        const unsigned known = SPM_DEVERR_PARTICLE_OUT_OF_BOX | SPM_DEVERR_LJ_CELL_OVERFLOW | SPM_DEVERR_NAN |
+                               SPM_DEVERR_SCRATCH_TOO_SMALL | SPM_DEVERR_TIMEOUT;
+        if (e & ~known) m += " unknown error bits 0x" + [](unsigned v) {
+            char b[16];
+            std::snprintf(b, sizeof(b), "%x", v);
+            return std::string(b);
+        }(e & ~known) + ";";
         return fail(SPM_ERR_DEVICE, m);
     }
     return SPM_OK;
@@ -525,19 +574,10 @@ double pass_elems_rw(spm_ctx *c, int nf, int axis, const PassPrune &pr) {
 // algorithmic bytes of a pass: pass_elems_rw complex elements).
 template <typename T, int DIR>
 int fft_strided_pass(spm_ctx *c, int slot, int nf, int axis, PassPrune pr) {
-    if (c->prof_on) {
-        cudaEvent_t a, b;
-        SPM_CUDA_CHECK(cudaEventCreate(&a));
-        SPM_CUDA_CHECK(cudaEventCreate(&b));
-        SPM_CUDA_CHECK(cudaEventRecord(a, c->st));
-        SPM_CUDA_CHECK((strided_dispatch<T, DIR>(c, slot, nf, axis, pr)));
-        SPM_CUDA_CHECK(cudaEventRecord(b, c->st));
-        c->prof_ev.push_back(a);
-        c->prof_ev.push_back(b);
-        c->prof_bytes += pass_elems_rw<T>(c, nf, axis, pr) * sizeof(cplx<T>);
-    } else {
-        SPM_CUDA_CHECK((strided_dispatch<T, DIR>(c, slot, nf, axis, pr)));
-    }
+    cudaEvent_t a = prof_mark(c);
+    SPM_CUDA_CHECK((strided_dispatch<T, DIR>(c, slot, nf, axis, pr)));
+    prof_done(c, a, DIR > 0 ? "strided_pass_inverse" : "strided_pass_forward",
+              pass_elems_rw<T>(c, nf, axis, pr) * sizeof(cplx<T>));
     c->launches++;
     return SPM_OK;
 }
@@ -549,7 +589,7 @@ int fft_strided_pass(spm_ctx *c, int slot, int nf, int axis) {
 // kz_keep: inverse inputs kz >= kz_keep read as zero; kz_span: forward
 // outputs kz >= kz_span left unwritten (both: pruned transforms).
 template <typename T>
-int z_pass(spm_ctx *c, int slot, int nf, bool forward, int kz_keep = 1 << 30, int kz_span = 1 << 30) {
+int z_pass_launch(spm_ctx *c, int slot, int nf, bool forward, int kz_keep, int kz_span) {
     const T scale = (T)(1.0 / ((double)c->g.nx * c->g.ny * c->g.nz));
     auto    one   = [&](int s, int nfields, size_t stride) {
         return forward ? plan_of<T>(c).z_r2c(c->real<T>(s), c->cx<T>(s), nfields, 2 * stride, stride, c->st,
@@ -567,6 +607,17 @@ int z_pass(spm_ctx *c, int slot, int nf, bool forward, int kz_keep = 1 << 30, in
         c->launches++;
     }
     return SPM_OK;
+}
+template <typename T>
+int z_pass(spm_ctx *c, int slot, int nf, bool forward, int kz_keep = 1 << 30, int kz_span = 1 << 30) {
+    // algorithmic bytes: the real rows (NZ values) and the complex values
+    // read (kz < kz_keep) or written (kz < kz_span)
+    const double rows = (double)nf * c->fft_runs * c->g.nx * c->g.ny;
+    const double kz   = std::min(forward ? kz_span : kz_keep, c->g.hnz);
+    cudaEvent_t  pa   = prof_mark(c);
+    const int    rc   = z_pass_launch<T>(c, slot, nf, forward, kz_keep, kz_span);
+    prof_done(c, pa, forward ? "z_r2c" : "z_c2r", rows * (c->g.nz * sizeof(T) + kz * sizeof(cplx<T>)));
+    return rc;
 }
 template <typename T>
 int fft_fwd(spm_ctx *c, int slot, int nf) {
@@ -615,6 +666,23 @@ __global__ void k_zero3(double *uk_dc) {
     if (threadIdx.x < 3) uk_dc[threadIdx.x] = 0.0;
 }
 
+// Algorithmic bytes of a k-space kernel over the retained 2/3 box: `words`
+// complex values read or written per retained mode, for every batched run.
+template <typename T>
+double box_bytes(const spm_ctx *L, int words) {
+    return (double)L->fft_runs * (double)L->g.box_elems() * words * sizeof(cplx<T>);
+}
+// Algorithmic bytes of a stencil kernel over Np x NP_domain cells: the
+// cached grid index (4 B) and weight (8 B) of every cell plus the field
+// words it touches: kind 0 (phi scatter) a read-modify-write of phi; kind 1
+// (hydrodynamic force) reads of u (3) and phi; kind 2 (f scatter) reads of u
+// (3) and phi and read-modify-writes of the three f components.
+template <typename T>
+double stencil_bytes(const spm_ctx *c, int kind) {
+    const int words = kind == 0 ? 2 : kind == 1 ? 4 : 10;
+    return (double)c->ph.np * c->ncells * (12.0 + words * sizeof(T));
+}
+
 // ---------------------------------------------------------------------------
 // Building blocks of the step (templated on the field type).  The `_runs`
 // forms advance runs R[0..nr) that share one grid: per-run kernels go to each
@@ -631,8 +699,8 @@ int zeta_to_velocity(spm_ctx *L, int truncate) {
         return fft_inv_packed<T>(L, U0, 3);
     }
     int rc;
-    LAUNCH(L, (k_zeta_to_u<T, 1>), L->box_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
-           L->cx<T>(U1), L->cx<T>(U2), 1, L->fstride_c);
+    PLAUNCH(L, "k_zeta_to_u", box_bytes<T>(L, 5), (k_zeta_to_u<T, 1>), L->box_grid(), 256, 0, L->g, L->cx<T>(Z0),
+            L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0), L->cx<T>(U1), L->cx<T>(U2), 1, L->fstride_c);
     if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 0, prune_inverse(L->g, 0))) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 1, prune_inverse(L->g, 1))) != SPM_OK) return rc;
     return z_pass<T>(L, U0, 3, false, L->g.trn[2]);
@@ -643,18 +711,24 @@ template <typename T>
 int ns_solver(spm_ctx *L) {
     int rc;
     // zeta -> u_hat (truncated) -> inverse x, y passes
-    LAUNCH(L, (k_zeta_to_u<T, 1>), L->box_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0),
-           L->cx<T>(U1), L->cx<T>(U2), 1, L->fstride_c);
+    PLAUNCH(L, "k_zeta_to_u", box_bytes<T>(L, 5), (k_zeta_to_u<T, 1>), L->box_grid(), 256, 0, L->g, L->cx<T>(Z0),
+            L->cx<T>(Z1), L->uk_dc, L->cx<T>(U0), L->cx<T>(U1), L->cx<T>(U2), 1, L->fstride_c);
     if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 0, prune_inverse(L->g, 0))) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, +1>(L, U0, 3, 1, prune_inverse(L->g, 1))) != SPM_OK) return rc;
     // inverse z + products + forward z in one pass, then forward y, x passes
-    SPM_CUDA_CHECK(plan_of<T>(L).z_products(L->cx<T>(U0), L->slot_stride_c, L->fft_runs, L->fstride_c, L->st,
-                                            L->g.trn[2], L->g.kz_span()));
+    {
+        const double rows = (double)L->fft_runs * L->g.nx * L->g.ny;
+        cudaEvent_t  pa   = prof_mark(L);
+        SPM_CUDA_CHECK(plan_of<T>(L).z_products(L->cx<T>(U0), L->slot_stride_c, L->fft_runs, L->fstride_c, L->st,
+                                                L->g.trn[2], L->g.kz_span()));
+        prof_done(L, pa, "z_products", rows * (3.0 * L->g.trn[2] + 5.0 * L->g.kz_span()) * sizeof(cplx<T>));
+    }
     L->launches++;
     if ((rc = fft_strided_pass<T, -1>(L, U0, 5, 1, prune_forward(L->g, 1))) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, -1>(L, U0, 5, 0, prune_forward(L->g, 0))) != SPM_OK) return rc;
-    LAUNCH(L, (k_ns_update<T, 2>), L->box_grid(), 256, 0, L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->cx<T>(U0), L->cx<T>(U1),
-           L->cx<T>(U2), L->cx<T>(A0), L->cx<T>(A1), L->ph.nu, L->ph.dt, L->fstride_c, L->zl<T>(0), L->zl<T>(1));
+    PLAUNCH(L, "k_ns_update", box_bytes<T>(L, L->compensated() ? 13 : 9), (k_ns_update<T, 2>), L->box_grid(), 256, 0,
+            L->g, L->cx<T>(Z0), L->cx<T>(Z1), L->cx<T>(U0), L->cx<T>(U1), L->cx<T>(U2), L->cx<T>(A0), L->cx<T>(A1),
+            L->ph.nu, L->ph.dt, L->fstride_c, L->zl<T>(0), L->zl<T>(1));
     return SPM_OK;
 }
 
@@ -768,12 +842,37 @@ int rigidity_projection(spm_ctx *L) {
     if ((rc = z_pass<T>(L, UP0, 3, true, 1 << 30, L->g.kz_span())) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 1, prune_forward(L->g, 1))) != SPM_OK) return rc;
     if ((rc = fft_strided_pass<T, -1>(L, UP0, 3, 0, prune_forward(L->g, 0))) != SPM_OK) return rc;
-    LAUNCH(L, (k_project_add_curl<T, 2>), L->box_grid(), 256, 0, L->g, L->cx<T>(UP0), L->cx<T>(UP1), L->cx<T>(UP2),
-           L->cx<T>(Z0), L->cx<T>(Z1), L->uk_dc, L->fstride_c, L->zl<T>(0), L->zl<T>(1));
+    PLAUNCH(L, "k_project_add_curl", box_bytes<T>(L, L->compensated() ? 11 : 7), (k_project_add_curl<T, 2>),
+            L->box_grid(), 256, 0, L->g, L->cx<T>(UP0), L->cx<T>(UP1), L->cx<T>(UP2), L->cx<T>(Z0), L->cx<T>(Z1),
+            L->uk_dc, L->fstride_c, L->zl<T>(0), L->zl<T>(1));
     return SPM_OK;
 }
 
 int particle_blocks(spm_ctx *c) { return (c->ph.np + 127) / 128; }
+
+// The LJ forces of Force() (particle_solver.h:88-111) with the constant
+// body force: through the cell list (particles binned per 16-DX cell, one warp
+// per particle over the 27 neighbour cells) when the grid has at least one
+// such cell per axis, as the reference's cell list needs; else the scan over
+// all partners with the reference's pair multiplicity (p_forces).
+int lj_forces(spm_ctx *c, const Phys &ph) {
+    if (ph.np == 0) return SPM_OK;
+    if (!c->lj_list || !lj_cell_list_applies(ph)) {
+        PLAUNCH(c, "p_forces", 0.0, p_forces, (ph.np + 3) / 4, 128, 0, ph, c->ps, 0, 0.0);
+        return SPM_OK;
+    }
+    const int ncell   = lj_ncell(ph);
+    int      *count   = c->lj_list;
+    int      *cell_of = count + ncell;
+    int      *bins    = cell_of + ph.np;
+    if (ph.lj_on && ph.janus_prop != 3) {
+        SPM_CUDA_CHECK(cudaMemsetAsync(count, 0, (size_t)ncell * sizeof(int), c->st));
+        PLAUNCH(c, "p_cells_bin", 0.0, p_cells_bin, (ph.np + 127) / 128, 128, 0, ph, c->ps.x, count, cell_of, bins,
+                c->err);
+    }
+    PLAUNCH(c, "p_forces_cells", 0.0, p_forces_cells, (ph.np + 3) / 4, 128, 0, ph, c->ps, count, cell_of, bins);
+    return SPM_OK;
+}
 
 // Zeta uploaded by the host: truncate it once (the reference truncates zeta in
 // place at the start of NS_solver_slavedEuler; the step's retained-box
@@ -814,11 +913,11 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
             spm_ctx *c = R[r];
             if (c->ph.np == 0) continue;
             auto side_work = [&]() -> int {
-                LAUNCH(c, p_position, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev, 1);
+                PLAUNCH(c, "p_position", 0.0, p_position, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev, 1);
                 const dim3 sgrid((c->ncells + 127) / 128, c->ph.np);
-                LAUNCH(c, s_phi_scatter_cache<T>, sgrid, 128, 0, c->g, c->ph, c->ps.x, c->cells, c->ncells,
-                       c->real<T>(PHIS), c->err, c->sc_idx, c->sc_w);
-                LAUNCH(c, p_forces, (c->ph.np + 3) / 4, 128, 0, c->ph, c->ps, 0, 0.0);
+                PLAUNCH(c, "s_phi_scatter_cache", stencil_bytes<T>(c, 0), s_phi_scatter_cache<T>, sgrid, 128, 0, c->g,
+                        c->ph, c->ps.x, c->cells, c->ncells, c->real<T>(PHIS), c->err, c->sc_idx, c->sc_w);
+                SPM_TRY(lj_forces(c, c->ph));
                 return SPM_OK;
             };
             rc = side_work();
@@ -836,21 +935,21 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
     for (int r = 0; r < nr; r++) {
         spm_ctx *c = R[r];
         if (c->ph.np == 0) continue;
-        LAUNCH(c, s_hydro_force_cached<T>, c->ph.np, 256, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
-               c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS), c->real<T>(U0), c->real<T>(U1), c->real<T>(U2),
-               c->ps.f_hydro, c->ps.torque_hydro);
+        PLAUNCH(c, "s_hydro_force_cached", stencil_bytes<T>(c, 1), s_hydro_force_cached<T>, c->ph.np, 256, 0, c->g,
+                c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells, c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS),
+                c->real<T>(U0), c->real<T>(U1), c->real<T>(U2), c->ps.f_hydro, c->ps.torque_hydro);
         if (c->ph.janus_prop == SPM_JANUS_SQUIRMER) {
             SPM_TRY(slip_loop<T>(c));  // lone runs only; leaves the slip field in UP
         } else {
-            LAUNCH(c, p_velocity, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev);
+            PLAUNCH(c, "p_velocity", 0.0, p_velocity, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev);
         }
         // obstacles draw no noise (fluct.cxx:23)
         if (c->P.kbt > 0.0 && c->ph.janus_prop != SPM_JANUS_OBSTACLE)
             LAUNCH(c, p_thermostat, 1, kThermoThreads, 0, c->ph, c->ps, c->mt);
         const dim3 sgrid((c->ncells + 127) / 128, c->ph.np);
-        LAUNCH(c, s_f_scatter_cached<T>, sgrid, 128, 0, c->g, c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells,
-               c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS), c->real<T>(U0), c->real<T>(U1), c->real<T>(U2),
-               c->real<T>(UP0), c->real<T>(UP1), c->real<T>(UP2));
+        PLAUNCH(c, "s_f_scatter_cached", stencil_bytes<T>(c, 2), s_f_scatter_cached<T>, sgrid, 128, 0, c->g, c->ph,
+                c->ps.x, c->ps.v, c->ps.omega, c->cells, c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS),
+                c->real<T>(U0), c->real<T>(U1), c->real<T>(U2), c->real<T>(UP0), c->real<T>(UP1), c->real<T>(UP2));
     }
     if ((rc = rigidity_projection<T>(L)) != SPM_OK) return rc;
     LAUNCH(L, k_ts_advance, (nr + 127) / 128, 128, 0, L->rw, nr);
@@ -1136,6 +1235,7 @@ void destroy_ctx(spm_ctx *c) {
     if (c->owns_arena) dev_free(c->arena);
     if (c->owns_rw) dev_free(c->rw);
     dev_free(c->cells);
+    dev_free(c->lj_list);
     dev_free(c->sc_idx);
     dev_free(c->sc_w);
     dev_free(c->pbuf);
@@ -1255,7 +1355,9 @@ int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *
     if (dev_alloc((void **)&c->cells, cells.size() * sizeof(int)) != cudaSuccess ||
         dev_alloc((void **)&c->pbuf, (size_t)np * kPWords * sizeof(double)) != cudaSuccess ||
         dev_alloc((void **)&c->rec_stage, (size_t)std::max(np, 1) * SPM_PARTICLE_WORDS * sizeof(double)) != cudaSuccess ||
-        dev_alloc((void **)&c->mt, 625 * sizeof(unsigned int)) != cudaSuccess) {
+        dev_alloc((void **)&c->mt, 625 * sizeof(unsigned int)) != cudaSuccess ||
+        (lj_cell_list_applies(c->ph) &&
+         dev_alloc((void **)&c->lj_list, ((size_t)lj_ncell(c->ph) * (1 + kLjBin) + np) * sizeof(int)) != cudaSuccess)) {
         destroy_ctx(c);
         return fail(SPM_ERR_NOMEM, "small device buffers");
     }
@@ -1416,13 +1518,41 @@ int spm_initialize(spm_ctx *c, const double *particles_host) {
 
 int spm_step(spm_ctx *c, int nsteps) {
     if (!c || nsteps < 0) return fail(SPM_ERR_ARG, "bad argument");
+    // graph replay: lone Navier_Stokes runs (the slip loop of squirmers reads
+    // its convergence on the host), not while a test switch is armed
     const bool graph = c->use_graph && !c->pool && !c->prof_on && c->P.equation == SPM_EQ_NAVIER_STOKES &&
-                       c->P.janus_propulsion != SPM_JANUS_SQUIRMER;  // the slip loop reads its convergence on the host
+                       c->P.janus_propulsion != SPM_JANUS_SQUIRMER && c->pp64->skip_loads == 0 &&
+                       c->pp32->skip_loads == 0;
     for (int i = 0; i < nsteps; i++) {
         int rc = graph ? (c->fp64() ? step_graphed<double>(c) : step_graphed<float>(c))
                        : (c->fp64() ? step_impl<double>(c) : step_impl<float>(c));
         if (rc != SPM_OK) return rc;
     }
+    return SPM_OK;
+}
+
+// Drops the captured step graph (its kernels hold launch parameters that
+// changed); the next graphed step captures a new one.
+static int drop_step_graph(spm_ctx *c) {
+    if (!c->step_exec) return SPM_OK;
+    SPM_CUDA_CHECK(cudaStreamSynchronize(c->st));
+    cudaGraphExecDestroy(c->step_exec);
+    if (c->step_graph) cudaGraphDestroy(c->step_graph);
+    c->step_exec  = nullptr;
+    c->step_graph = nullptr;
+    return SPM_OK;
+}
+
+int spm_set_wait_limit(spm_ctx *c, double seconds) {
+    if (!c || !(seconds > 0.0) || seconds > 60.0) return fail(SPM_ERR_ARG, "wait limit must be in (0, 60] s");
+    const unsigned long long ns = (unsigned long long)(seconds * 1e9) > 0 ? (unsigned long long)(seconds * 1e9) : 1;
+    c->pp64->wait_ns = c->pp32->wait_ns = ns;
+    return drop_step_graph(c);
+}
+
+int spm_debug_skip_tma_loads(spm_ctx *c, int launches) {
+    if (!c || launches < 0) return fail(SPM_ERR_ARG, "bad argument");
+    c->pp64->skip_loads = c->pp32->skip_loads = launches;
     return SPM_OK;
 }
 
@@ -1513,8 +1643,18 @@ int spm_get_shear_state(spm_ctx *c, double *degree_oblique, double stress[8]) {
     return le_get_state(c, degree_oblique, stress);
 }
 
+// A device field array for the transforms: complex values (and so the base
+// and the field stride) 16-byte aligned, as the kernels' vector accesses and
+// tensor maps need.
+static bool fft_dev_aligned(const spm_ctx *c, const void *data, size_t field_stride) {
+    const size_t cbytes = c->fp64() ? 16 : 8;
+    return ((uintptr_t)data % 16) == 0 && (field_stride * cbytes) % 16 == 0;
+}
+
 int spm_fft_forward_dev(spm_ctx *c, void *data, int nfields, size_t field_stride) {
     if (!c || !data || nfields < 1) return fail(SPM_ERR_ARG, "bad argument");
+    if (!fft_dev_aligned(c, data, field_stride))
+        return fail(SPM_ERR_ARG, "field array and field stride must be 16-byte aligned");
     cudaError_t e = c->fp64() ? c->pp64->forward((double *)data, nfields, field_stride, c->st)
                               : c->pp32->forward((float *)data, nfields, field_stride, c->st);
     c->launches += 3;
@@ -1524,6 +1664,8 @@ int spm_fft_forward_dev(spm_ctx *c, void *data, int nfields, size_t field_stride
 
 int spm_fft_inverse_dev(spm_ctx *c, void *data, int nfields, size_t field_stride) {
     if (!c || !data || nfields < 1) return fail(SPM_ERR_ARG, "bad argument");
+    if (!fft_dev_aligned(c, data, field_stride))
+        return fail(SPM_ERR_ARG, "field array and field stride must be 16-byte aligned");
     cudaError_t e = c->fp64() ? c->pp64->inverse((cplx<double> *)data, nfields, field_stride, c->st)
                               : c->pp32->inverse((cplx<float> *)data, nfields, field_stride, c->st);
     c->launches += 3;
@@ -1553,26 +1695,93 @@ int spm_time_steps(spm_ctx *c, int nsteps, float *ms) {
     return check_device_error(c);
 }
 
+// nsteps steps with every profiled launch bracketed by CUDA events on its
+// own stream (direct launches, no graph replay); `prof` collects the records.
+static void profile_clear(spm_ctx *c) {
+    for (const auto &r : c->prof) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    c->prof.clear();
+}
+static int profile_steps(spm_ctx *c, int nsteps, float *total_ms) {
+    profile_clear(c);
+    cudaEvent_t t0, t1;
+    SPM_CUDA_CHECK(cudaEventCreate(&t0));
+    SPM_CUDA_CHECK(cudaEventCreate(&t1));
+    SPM_CUDA_CHECK(cudaEventRecord(t0, c->st));
+    c->prof_on = true;
+    int rc     = spm_step(c, nsteps);
+    c->prof_on = false;
+    cudaEventRecord(t1, c->st);
+    SPM_CUDA_CHECK(cudaStreamSynchronize(c->st));
+    SPM_CUDA_CHECK(cudaDeviceSynchronize());  // the side stream's records too
+    if (total_ms) cudaEventElapsedTime(total_ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return rc;
+}
+
 int spm_profile_pass(spm_ctx *c, int nsteps, double *avg_us, double *bytes_per_launch, long long *count) {
     if (!c || nsteps < 1 || !avg_us || !bytes_per_launch || !count) return fail(SPM_ERR_ARG, "bad argument");
-    c->prof_on    = true;
-    c->prof_bytes = 0.0;
-    int rc        = spm_step(c, nsteps);
-    c->prof_on    = false;
-    SPM_CUDA_CHECK(cudaStreamSynchronize(c->st));
-    double total = 0.0;
-    const size_t n = c->prof_ev.size() / 2;
-    for (size_t i = 0; i < n; i++) {
+    const int rc    = profile_steps(c, nsteps, nullptr);
+    double    total = 0.0, bytes = 0.0;
+    long long n     = 0;
+    for (const auto &r : c->prof) {
+        if (std::strncmp(r.name, "strided_pass", 12) != 0) continue;
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, c->prof_ev[2 * i], c->prof_ev[2 * i + 1]);
+        cudaEventElapsedTime(&ms, r.a, r.b);
         total += ms;
+        bytes += r.bytes;
+        n++;
     }
-    for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
-    c->prof_ev.clear();
+    profile_clear(c);
     if (rc != SPM_OK) return rc;
-    *count            = (long long)n;
+    *count            = n;
     *avg_us           = n ? 1000.0 * total / (double)n : 0.0;
-    *bytes_per_launch = n ? c->prof_bytes / (double)n : 0.0;
+    *bytes_per_launch = n ? bytes / (double)n : 0.0;
+    return check_device_error(c);
+}
+
+int spm_profile_kernels(spm_ctx *c, int nsteps, char *json, size_t cap) {
+    if (!c || nsteps < 1 || !json || cap < 64) return fail(SPM_ERR_ARG, "bad argument");
+    float     step_ms = 0.f;
+    const int rc      = profile_steps(c, nsteps, &step_ms);
+    struct Agg {
+        long long n     = 0;
+        double    ms    = 0.0;
+        double    bytes = 0.0;
+    };
+    std::vector<std::pair<std::string, Agg>> agg;
+    for (const auto &r : c->prof) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        auto it = std::find_if(agg.begin(), agg.end(), [&](const std::pair<std::string, Agg> &p) { return p.first == r.name; });
+        if (it == agg.end()) {
+            agg.push_back({r.name, Agg{}});
+            it = agg.end() - 1;
+        }
+        it->second.n++;
+        it->second.ms += ms;
+        it->second.bytes += r.bytes;
+    }
+    profile_clear(c);
+    if (rc != SPM_OK) return rc;
+    std::string out = "{\"steps\": " + std::to_string(nsteps) + ", \"step_ms_total\": " + std::to_string(step_ms) +
+                      ", \"kernels\": [";
+    for (size_t i = 0; i < agg.size(); i++) {
+        const Agg &a = agg[i].second;
+        char       b[320];
+        std::snprintf(b, sizeof(b),
+                      "%s{\"name\": \"%s\", \"launches\": %lld, \"us_total\": %.3f, \"us_per_launch\": %.3f, "
+                      "\"bytes_per_launch\": %.1f}",
+                      i ? ", " : "", agg[i].first.c_str(), a.n, 1000.0 * a.ms, 1000.0 * a.ms / (double)a.n,
+                      a.bytes / (double)a.n);
+        out += b;
+    }
+    out += "]}";
+    if (out.size() + 1 > cap) return fail(SPM_ERR_ARG, "profile buffer too small");
+    std::memcpy(json, out.c_str(), out.size() + 1);
     return check_device_error(c);
 }
 

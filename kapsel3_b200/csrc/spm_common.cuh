@@ -18,8 +18,10 @@
 
 namespace spm {
 
+// A complex value aligned to its full size, so that a value in shared or
+// global memory moves as one 8-byte (FP32) or 16-byte (FP64) access.
 template <typename T>
-struct cplx {
+struct alignas(2 * sizeof(T)) cplx {
     T re, im;
 };
 

@@ -9,9 +9,7 @@
 //            and kz=NZ/2 planes are discarded (c2r semantics)
 //
 // Three in-place passes over HBM, each a single kernel:
-//   Z pass: real rows (contiguous) <-> complex rows; length-NZ real transform
-//           done as an NZ/2-point complex four-step FFT in registers + shared
-//           memory, with the even/odd split post-/pre-processing.
+//   Z pass: real rows (contiguous) <-> complex rows (spm_zrow.cuh);
 //   Y pass, X pass: length-N complex transforms along a strided axis; a CTA
 //           owns W adjacent kz columns of N lines (W*16 B contiguous per
 //           line) and runs a four-step N = N1*N2 FFT: step 1 loads straight
@@ -23,6 +21,7 @@
 
 #include "spm_dft.cuh"
 #include "spm_tma.cuh"
+#include "spm_zrow.cuh"
 
 namespace spm {
 
@@ -129,12 +128,17 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
 // ahead of the four-step FFT, results go back with TMA stores from the same
 // buffer.  Columns >= hnz are outside the tensor: loads zero-fill them and
 // stores clip them.
+// Every wait on a ring buffer is bounded by wait_ns of the global timer.  A
+// CTA whose wait runs out records SPM_DEVERR_TIMEOUT, stops, waits (bounded
+// again) for the loads it has issued and not consumed, and returns.
+// skip_loads != 0 is a test switch: the CTAs issue no load at all, so every
+// first wait runs out with nothing in flight.
 // ---------------------------------------------------------------------------
 template <typename T, int N, int W, int DIR, int S>
 __global__ void __launch_bounds__(W *Split<N>::N1)
     fft_strided_tma_kernel(const __grid_constant__ CUtensorMap lmap, const __grid_constant__ CUtensorMap smap,
                            int axis, int n_outer, int ct_used, int ntiles, const cplx<T> *__restrict__ twN,
-                           unsigned int *err, PassPrune pr) {
+                           unsigned int *err, PassPrune pr, unsigned long long wait_ns, int skip_loads) {
     constexpr int  N1         = Split<N>::N1;
     constexpr int  N2         = Split<N>::N2;
     // lines per load / store box (lmap / smap): N, or two boxes of the
@@ -169,8 +173,12 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
         fence_mbar_init();
     }
     __syncthreads();
-    // tile t into ring buffer b: lines [0, hl) and, when pruned, [N - hl, N)
-    auto load_tile = [&](int t, int b) {
+    // tile t into ring buffer b: lines [0, hl) and, when pruned, [N - hl, N).
+    // last_issued (thread 0): the last iteration whose tile load was issued.
+    int  last_issued = -1;
+    auto load_tile   = [&](int t, int b) {
+        if (skip_loads) return;
+        last_issued = (t - (int)blockIdx.x) / (int)gridDim.x;
         int c0, c1, c2, c3;
         coords(t, c0, c1, c2, c3);
         cplx<T> *dst = buf + (size_t)b * N * W;
@@ -195,12 +203,16 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
         tw1[k1] = twN[(g * k1) & (N - 1)];
         if (DIR > 0) tw1[k1].im = -tw1[k1].im;
     }
-    int it = 0;
+    int  it      = 0;
+    bool stopped = false;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
         const int b  = it % S;
         cplx<T>  *B  = buf + (size_t)b * N * W;
-        const bool w = mbar_wait(&full[b], (unsigned)((it / S) & 1), err);
-        if (!__syncthreads_and(w)) break;
+        const bool w = mbar_wait(&full[b], (unsigned)((it / S) & 1), err, wait_ns);
+        if (!__syncthreads_and(w)) {
+            stopped = true;
+            break;
+        }
         // step 1: N2-point DFTs over n2 for n1 = g, in place (pruned inputs
         // read as zero)
         const bool col_in = (t % ct_used) * W + c < pr.col_keep;
@@ -255,375 +267,12 @@ __global__ void __launch_bounds__(W *Split<N>::N1)
             }
         }
     }
-    if (tid == 0) bulk_wait_all();
-}
-
-// ---------------------------------------------------------------------------
-// Z pass building blocks: one row of NZ = 2M reals <-> M+1 complex, handled
-// by P = Split<M>::N1 threads (t = 0..P-1) with a shared workspace row `s`.
-// Every thread of the CTA must call these together (they synchronise).
-//
-// r2c_row: ld(n) returns the packed pair (x[2n], x[2n+1]) for n < M;
-//          st(k, X) receives X[k] for k = 0..M.
-// c2r_row: ld(k) returns X[k] for k = 0..M (imaginary parts of X[0] and X[M]
-//          are discarded); st(n, z) receives z = (x[2n], x[2n+1]) * scale-
-//          normalised output.
-// ---------------------------------------------------------------------------
-// Workspace index of a z-row transform: one complex of padding after every
-// N1 values, so the step-2 reads of the four-step FFT (stride N1) hit
-// distinct shared-memory banks.  ws_len<M> complex per row.
-template <int M>
-__device__ __forceinline__ int wsi(int i) {
-    return i + i / Split<M>::N1;
-}
-// Row strides of the per-row shared buffers, in complex (pair) units: at
-// least `need`, and congruent to the P = N1 threads of a row modulo the pairs
-// per 128 bytes, so the rows that one shared-memory wavefront serves (a
-// half-warp of 8-byte or a quarter-warp of 16-byte accesses) fall on
-// disjoint banks.
-template <typename T, int M>
-constexpr int row_stride(int need) {
-    constexpr int mod = 128 / (int)sizeof(cplx<T>);
-    constexpr int p   = Split<M>::N1 % mod;
-    const int     r   = need % mod;
-    return need + ((p - r + mod) % mod);
-}
-template <typename T, int M>
-constexpr int ws_len() {
-    return row_stride<T, M>(M + 2 + (M + 1) / Split<M>::N1);
-}
-
-// The even/odd split of a length-2M real transform packed as M complex
-// values: X[k] from Z[k], Z[M-k] (forward) and Z'[k] from X[k], X[M-k]
-// (inverse, scaled by c).  w = e^{-2 pi i k / (2M)}.
-template <typename T>
-__device__ __forceinline__ cplx<T> r2c_split(const cplx<T> &zk, const cplx<T> &zmk, const cplx<T> &w) {
-    const T er  = (T)0.5 * (zk.re + zmk.re);
-    const T ei  = (T)0.5 * (zk.im - zmk.im);
-    const T orr = (T)0.5 * (zk.im + zmk.im);
-    const T oi  = (T)-0.5 * (zk.re - zmk.re);
-    return cplx<T>{er + (w.re * orr - w.im * oi), ei + (w.re * oi + w.im * orr)};
-}
-template <typename T>
-__device__ __forceinline__ cplx<T> c2r_split(const cplx<T> &xk, const cplx<T> &xmk, const cplx<T> &w, T c) {
-    const T er  = c * (xk.re + xmk.re);
-    const T ei  = c * (xk.im - xmk.im);
-    const T dr  = c * (xk.re - xmk.re);
-    const T di  = c * (xk.im + xmk.im);
-    const T orr = dr * w.re + di * w.im;
-    const T oi  = di * w.re - dr * w.im;
-    return cplx<T>{er - oi, ei + orr};
-}
-
-// r2c_row_m: as r2c_row, with ldm(m) returning the input of element
-// t + M1 m (m = 0..M2-1, a compile-time index after unrolling), so the row
-// may come from registers.
-template <typename T, int M, class LdM, class St>
-__device__ __forceinline__ void r2c_row_m(int t, LdM ldm, cplx<T> *s, const cplx<T> *__restrict__ twM,
-                                          const cplx<T> *__restrict__ twN, St st) {
-    constexpr int M1 = Split<M>::N1;
-    constexpr int M2 = Split<M>::N2;
-    constexpr int P  = M1;
-    cplx<T>       v[M2];
-#pragma unroll
-    for (int m = 0; m < M2; m++) v[m] = ldm(m);
-    dft_reg<T, M2, -1>(v);
-#pragma unroll
-    for (int k1 = 1; k1 < M2; k1++) v[k1] = cmul(v[k1], twM[(t * k1) & (M - 1)]);
-#pragma unroll
-    for (int k1 = 0; k1 < M2; k1++) s[wsi<M>(t + M1 * k1)] = v[k1];
-    __syncthreads();
-    cplx<T> z[M2 / M1][M1];
-#pragma unroll
-    for (int i = 0; i < M2 / M1; i++) {
-        const int k1 = t + M1 * i;
-#pragma unroll
-        for (int n1 = 0; n1 < M1; n1++) z[i][n1] = s[wsi<M>(n1 + M1 * k1)];
-        dft_reg<T, M1, -1>(z[i]);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < M2 / M1; i++) {
-        const int k1 = t + M1 * i;
-#pragma unroll
-        for (int k2 = 0; k2 < M1; k2++) s[wsi<M>(k1 + M2 * k2)] = z[i][k2];
-    }
-    __syncthreads();
-    // X[k] = E[k] + W_N^k O[k],  E = (Z[k] + conj Z[M-k]) / 2,
-    // O = -i (Z[k] - conj Z[M-k]) / 2,  k = 0..M.  A thread reads the pair
-    // Z[k], Z[M-k] (k = t + P i <= M/2) once and forms X[k] and X[M-k].
-    constexpr int H = M / 2;
-#pragma unroll
-    for (int i = 0; i <= H / P; i++) {
-        const int k = t + P * i;
-        if (k <= H) {
-            const cplx<T> zk  = s[wsi<M>(k)];
-            const cplx<T> zmk = s[wsi<M>((M - k) & (M - 1))];
-            st(k, r2c_split<T>(zk, zmk, twN[k]));  // twN: e^{-2 pi i k / (2M)}, k = 0..M
-            if (k != H) st(M - k, r2c_split<T>(zmk, zk, twN[M - k]));
-        }
-    }
-    __syncthreads();
-}
-
-template <typename T, int M, class Ld, class St>
-__device__ __forceinline__ void r2c_row(int t, Ld ld, cplx<T> *s, const cplx<T> *__restrict__ twM,
-                                        const cplx<T> *__restrict__ twN, St st) {
-    r2c_row_m<T, M>(t, [&](int m) { return ld(t + Split<M>::N1 * m); }, s, twM, twN, st);
-}
-
-// c2r_row_m: as c2r_row, with stm(m, z) receiving output element t + M1 m
-// (m = 0..M2-1, compile-time after unrolling), so the row may stay in
-// registers.
-template <typename T, int M, class Ld, class StM>
-__device__ __forceinline__ void c2r_row_m(int t, Ld ld, cplx<T> *s, const cplx<T> *__restrict__ twM,
-                                          const cplx<T> *__restrict__ twN, T scale, StM stm) {
-    constexpr int M1 = Split<M>::N1;
-    constexpr int M2 = Split<M>::N2;
-    constexpr int P  = M1;
-    // Z'[k] = E' + i O',  E' = c (X[k] + conj X[M-k]),
-    // O' = c (X[k] - conj X[M-k]) W_N^{-k},  k = 0..M-1.  A thread loads
-    // the pair X[k], X[M-k] (k = t + P i <= M/2; all loads first, in flight
-    // together) and writes Z'[k] and Z'[M-k]; the imaginary parts of X[0]
-    // and X[M] are discarded.
-    constexpr int H  = M / 2;
-    constexpr int NI = H / P + 1;
-    cplx<T>       xa[NI], xb[NI];
-#pragma unroll
-    for (int i = 0; i < NI; i++) {
-        const int k = t + P * i;
-        if (k <= H) {
-            xa[i] = ld(k);
-            xb[i] = k == H ? xa[i] : ld(M - k);
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < NI; i++) {
-        const int k = t + P * i;
-        if (k <= H) {
-            cplx<T> a = xa[i], b = xb[i];
-            if (k == 0) a.im = b.im = 0;
-            s[wsi<M>(k)] = c2r_split<T>(a, b, twN[k], scale);
-            if (k != 0 && k != H) s[wsi<M>(M - k)] = c2r_split<T>(b, a, twN[M - k], scale);
-        }
-    }
-    __syncthreads();
-    cplx<T> v[M2];
-#pragma unroll
-    for (int m = 0; m < M2; m++) v[m] = s[wsi<M>(t + M1 * m)];
-    dft_reg<T, M2, +1>(v);
-#pragma unroll
-    for (int k1 = 1; k1 < M2; k1++) {
-        cplx<T> w = twM[(t * k1) & (M - 1)];
-        w.im      = -w.im;
-        v[k1]     = cmul(v[k1], w);
-    }
-#pragma unroll
-    for (int k1 = 0; k1 < M2; k1++) s[wsi<M>(t + M1 * k1)] = v[k1];
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < M2 / M1; i++) {
-        const int k1 = t + M1 * i;
-        cplx<T>   u[M1];
-#pragma unroll
-        for (int n1 = 0; n1 < M1; n1++) u[n1] = s[wsi<M>(n1 + M1 * k1)];
-        dft_reg<T, M1, +1>(u);
-#pragma unroll
-        for (int k2 = 0; k2 < M1; k2++) stm(i + (M2 / M1) * k2, u[k2]);  // element k1 + M2 k2 = t + M1 m
-    }
-    __syncthreads();
-}
-
-template <typename T, int M, class Ld, class St>
-__device__ __forceinline__ void c2r_row(int t, Ld ld, cplx<T> *s, const cplx<T> *__restrict__ twM,
-                                        const cplx<T> *__restrict__ twN, T scale, St st) {
-    c2r_row_m<T, M>(t, ld, s, twM, twN, scale,
-                    [&](int m, const cplx<T> &z) { st(t + Split<M>::N1 * m, z); });
-}
-
-template <typename T>
-__device__ __forceinline__ cplx<T> load_pair(const T *row, int n) {
-    using V2   = typename vec2_of<T>::type;
-    const V2 p = reinterpret_cast<const V2 *>(row)[n];
-    return cplx<T>{p.x, p.y};
-}
-template <typename T>
-__device__ __forceinline__ void store_pair(T *row, int n, cplx<T> z) {
-    using V2 = typename vec2_of<T>::type;
-    V2 p;
-    p.x                             = z.re;
-    p.y                             = z.im;
-    reinterpret_cast<V2 *>(row)[n] = p;
-}
-
-// ---------------------------------------------------------------------------
-// Z pass, forward: real rows -> complex rows (in and out may alias).
-// in:  real row r at in + r*2*hnzp (2M reals used),   M = NZ/2
-// out: complex row r at out + r*hnzp (M+1 values, padding zeroed); outputs
-//      kz >= kz_span are not written (pruned transforms downstream read none)
-// ---------------------------------------------------------------------------
-template <typename T, int M, int R>
-__global__ void __launch_bounds__(R *Split<M>::N1)
-    fft_z_r2c_kernel(const T *in, cplx<T> *out, size_t field_stride_real, size_t field_stride_c, int nrows,
-                     int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, int kz_span) {
-    constexpr int P = Split<M>::N1;
-    __shared__ __align__(16) cplx<T> s[R][ws_len<T, M>()];
-    const int r   = threadIdx.x / P;
-    const int t   = threadIdx.x % P;
-    const int row = blockIdx.x * R + r;
-    const bool ok = row < nrows;
-    const T *rin  = in + (size_t)blockIdx.y * field_stride_real + (size_t)(ok ? row : 0) * 2 * hnzp;
-    cplx<T> *rout = out + (size_t)blockIdx.y * field_stride_c + (size_t)(ok ? row : 0) * hnzp;
-    r2c_row<T, M>(
-        t, [&](int n) { return ok ? load_pair<T>(rin, n) : cplx<T>{0, 0}; }, s[r], twM, twN,
-        [&](int k, cplx<T> X) {
-            if (ok && k < kz_span) rout[k] = X;
-        });
-    if (ok && kz_span > M)
-        for (int k = M + 1 + t; k < hnzp; k += P) rout[k] = cplx<T>{0, 0};
-}
-
-// ---------------------------------------------------------------------------
-// Z pass, inverse: complex rows -> real rows, output scaled by `scale`.
-// Inputs kz >= kz_keep are read as zero (pruned transforms; hnz: none).
-// ---------------------------------------------------------------------------
-template <typename T, int M, int R>
-__global__ void __launch_bounds__(R *Split<M>::N1)
-    fft_z_c2r_kernel(const cplx<T> *in, T *out, size_t field_stride_c, size_t field_stride_real, int nrows,
-                     int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale,
-                     int kz_keep) {
-    constexpr int P = Split<M>::N1;
-    __shared__ __align__(16) cplx<T> s[R][ws_len<T, M>()];
-    const int r   = threadIdx.x / P;
-    const int t   = threadIdx.x % P;
-    const int row = blockIdx.x * R + r;
-    const bool ok = row < nrows;
-    const cplx<T> *rin = in + (size_t)blockIdx.y * field_stride_c + (size_t)(ok ? row : 0) * hnzp;
-    T *rout            = out + (size_t)blockIdx.y * field_stride_real + (size_t)(ok ? row : 0) * 2 * hnzp;
-    c2r_row<T, M>(
-        t, [&](int k) { return (ok && k < kz_keep) ? rin[k] : cplx<T>{0, 0}; }, s[r], twM, twN, scale,
-        [&](int n, cplx<T> z) {
-            if (ok) store_pair<T>(rout, n, z);
-        });
-    if (ok && t == 0)
-        for (int k = 2 * M; k < 2 * hnzp; k++) rout[k] = (T)0;
-}
-
-// ---------------------------------------------------------------------------
-// Fused Z pass of the advection term (U2advection_k, operate_omega.cxx:12-55):
-// inverse z transform of the three velocity components, the five quadratic
-// products in registers/shared memory, forward z transform of the products.
-// io[0..2] hold u_hat (z-complex rows) on input; io[0..4] receive the
-// z-transformed products u2u3, u3u1, u1u2, (u2-u3)(u2+u3), (u3-u1)(u3+u1).
-// Inputs kz >= kz_keep are read as zero; outputs are written for kz <
-// kz_span only (the pruned passes downstream read no further).
-// ---------------------------------------------------------------------------
-template <typename T, int M, int R>
-__global__ void __launch_bounds__(R *Split<M>::N1)
-    fft_z_products_kernel(cplx<T> *io, size_t field_stride_c, size_t run_stride_c, int nrows, int hnzp,
-                          const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale, int kz_keep,
-                          int kz_span) {
-    constexpr int P     = Split<M>::N1;
-    constexpr int PITCH = 2 * row_stride<T, M>(M + 2);  // reals per staged row (>= 2 * hnzp)
-    io += (size_t)blockIdx.y * run_stride_c;  // run of a batched pool
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    T       *U  = reinterpret_cast<T *>(smem_raw);                 // [3][R][PITCH]
-    cplx<T> *ws = reinterpret_cast<cplx<T> *>(U + 3 * R * PITCH);   // [R][ws_len<M>]
-    const int r   = threadIdx.x / P;
-    const int t   = threadIdx.x % P;
-    const int row = blockIdx.x * R + r;
-    const bool ok = row < nrows;
-    const size_t roff = (size_t)(ok ? row : 0) * hnzp;
-    T *Ur[3] = {U + (0 * R + r) * PITCH, U + (1 * R + r) * PITCH, U + (2 * R + r) * PITCH};
-    // Inverse z of the three velocity rows: each thread loads its pairs
-    // X[k], X[M-k] straight from global memory (all in flight together) and
-    // the real row lands in U[d].
-#pragma unroll 1
-    for (int d = 0; d < 3; d++) {
-        const cplx<T> *rin = io + d * field_stride_c + roff;
-        T             *ur  = Ur[d];
-        c2r_row<T, M>(
-            t, [&](int k) { return (ok && k < kz_keep) ? rin[k] : cplx<T>{0, 0}; }, ws + r * ws_len<T, M>(), twM, twN,
-            scale, [&](int n, cplx<T> z) { store_pair<T>(ur, n, z); });
-    }
-#pragma unroll 1
-    for (int p = 0; p < 5; p++) {
-        cplx<T> *rout = io + p * field_stride_c + roff;
-        r2c_row<T, M>(
-            t,
-            [&](int n) {
-                const cplx<T> a = load_pair<T>(Ur[0], n), b = load_pair<T>(Ur[1], n), c = load_pair<T>(Ur[2], n);
-                const T       xs[2] = {a.re, a.im}, ys[2] = {b.re, b.im}, zs[2] = {c.re, c.im};
-                T             o[2];
-#pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    const T x = xs[e], y = ys[e], z = zs[e];
-                    o[e] = p == 0 ? y * z : p == 1 ? z * x : p == 2 ? x * y : p == 3 ? (y - z) * (y + z)
-                                                                                     : (z - x) * (z + x);
-                }
-                return cplx<T>{o[0], o[1]};
-            },
-            ws + r * ws_len<T, M>(), twM, twN,
-            [&](int k, cplx<T> X) {
-                if (ok && k < kz_span) rout[k] = X;
-            });
-        if (ok && kz_span > M)
-            for (int k = M + 1 + t; k < hnzp; k += P) rout[k] = cplx<T>{0, 0};
-    }
-}
-
-// ---------------------------------------------------------------------------
-// The same fused Z pass with the three velocity rows kept in registers: the
-// inverse transform leaves element t + M1 m of its row in slot m of thread
-// t, which is the slot the forward transform of a product reads it from, so
-// the products are formed in registers and only the transform workspace is
-// in shared memory (for FP32 rows: 3 x M2 complex values per thread).
-// ---------------------------------------------------------------------------
-template <typename T, int M, int R>
-__global__ void __launch_bounds__(R *Split<M>::N1)
-    fft_z_products_reg_kernel(cplx<T> *io, size_t field_stride_c, size_t run_stride_c, int nrows, int hnzp,
-                              const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale,
-                              int kz_keep, int kz_span) {
-    constexpr int P  = Split<M>::N1;
-    constexpr int M2 = Split<M>::N2;
-    __shared__ __align__(16) cplx<T> ws[R][ws_len<T, M>()];
-    io += (size_t)blockIdx.y * run_stride_c;  // run of a batched pool
-    const int    r    = threadIdx.x / P;
-    const int    t    = threadIdx.x % P;
-    const int    row  = blockIdx.x * R + r;
-    const bool   ok   = row < nrows;
-    const size_t roff = (size_t)(ok ? row : 0) * hnzp;
-    cplx<T>      u[3][M2];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-        const cplx<T> *rin = io + d * field_stride_c + roff;
-        c2r_row_m<T, M>(
-            t, [&](int k) { return (ok && k < kz_keep) ? rin[k] : cplx<T>{0, 0}; }, ws[r], twM, twN, scale,
-            [&](int m, const cplx<T> &z) { u[d][m] = z; });
-    }
-#pragma unroll 1
-    for (int p = 0; p < 5; p++) {
-        cplx<T> *rout = io + p * field_stride_c + roff;
-        r2c_row_m<T, M>(
-            t,
-            [&](int m) {
-                const T xs[2] = {u[0][m].re, u[0][m].im}, ys[2] = {u[1][m].re, u[1][m].im},
-                        zs[2] = {u[2][m].re, u[2][m].im};
-                T o[2];
-#pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    const T x = xs[e], y = ys[e], z = zs[e];
-                    o[e] = p == 0 ? y * z : p == 1 ? z * x : p == 2 ? x * y : p == 3 ? (y - z) * (y + z)
-                                                                                     : (z - x) * (z + x);
-                }
-                return cplx<T>{o[0], o[1]};
-            },
-            ws[r], twM, twN,
-            [&](int k, cplx<T> X) {
-                if (ok && k < kz_span) rout[k] = X;
-            });
-        if (ok && kz_span > M)
-            for (int k = M + 1 + t; k < hnzp; k += P) rout[k] = cplx<T>{0, 0};
+    if (tid == 0) {
+        // after a timeout: the loads issued for iterations it.. are still
+        // owed to this CTA's shared memory; wait for them (bounded) first
+        if (stopped)
+            for (int j = it; j <= last_issued; j++) mbar_wait(&full[j % S], (unsigned)((j / S) & 1), nullptr, wait_ns);
+        bulk_wait_all();
     }
 }
 

@@ -18,34 +18,19 @@ struct FFTPlan {
     cplx<T> *tw_zn = nullptr;  // e^{-2 pi i k/NZ}, k <= NZ/2
 
     static constexpr int W = sizeof(T) == 8 ? 16 : 32;  // kz columns per strided tile
-    // rows per Z-pass CTA: 16, fewer (a power of two) for long rows so a
-    // CTA's row workspaces stay within 46 KB of static shared memory
-    static constexpr int zrows(int m) {
-        return pow2_floor_16((int)(47104 / ((size_t)ws_len_of(m) * sizeof(cplx<T>))));
-    }
-    static constexpr int pow2_floor_16(int r) { return r >= 16 ? 16 : r >= 8 ? 8 : r >= 4 ? 4 : r >= 2 ? 2 : 1; }
-
-    // rows per CTA of the fused products kernel (three staged rows + workspace
-    // per row, kept within about 66 KB of dynamic shared memory)
-    static constexpr int prows(int m) {
-        return (int)(65536 / (8 * m * sizeof(T))) >= 16 ? 16 : (int)(65536 / (8 * m * sizeof(T)));
-    }
-    static constexpr size_t psmem(int m) {
-        return (size_t)prows(m) * (3 * 2 * stride_of(m, m + 2) * sizeof(T) + (size_t)ws_len_of(m) * sizeof(cplx<T>));
-    }
 
     static bool size_ok(int n) { return n >= 8 && n <= 512 && (n & (n - 1)) == 0; }
-    // ws_len<M>() for a runtime M (Split<M>::N1 of spm_dft.cuh)
-    static constexpr int ws_len_of(int m) {
-        const int n1 = m <= 8 ? 2 : m <= 32 ? 4 : m <= 128 ? 8 : 16;
-        return stride_of(m, m + 2 + (m + 1) / n1);
+
+    // The fused z pass of the advection term keeps the three velocity rows in
+    // registers for FP32 rows of up to 256 reals, else in shared memory (one
+    // warp of rows per CTA).
+    template <int MM>
+    static constexpr bool ureg() {
+        return sizeof(T) == 4 && MM <= 128;
     }
-    // row_stride<T, M>(need) of spm_fft.cuh for a runtime M
-    static constexpr int stride_of(int m, int need) {
-        const int n1  = m <= 8 ? 2 : m <= 32 ? 4 : m <= 128 ? 8 : 16;
-        const int mod = 128 / (int)sizeof(cplx<T>);
-        const int p = n1 % mod, r = need % mod;
-        return need + ((p - r + mod) % mod);
+    template <int MM>
+    static constexpr int prows() {
+        return ureg<MM>() ? zr_rows<T, MM>() : 32 / ZR<MM>::P;
     }
 
     // Fused inverse-z / advection products / forward-z pass over five slots.
@@ -54,19 +39,12 @@ struct FFTPlan {
         const int nrows = g.nx * g.ny;
         const T   scale = (T)(1.0 / ((double)g.nx * g.ny * g.nz));
         switch (g.nz / 2) {
-#define SPM_ZP(MM)                                                                                  \
-    case MM: {                                                                                      \
-        if (sizeof(T) == 4 && kRegProducts) {                                                       \
-            constexpr int RR = zrows(MM);                                                           \
-            fft_z_products_reg_kernel<T, MM, RR>                                                    \
-                <<<dim3((nrows + RR - 1) / RR, nruns), RR * Split<MM>::N1, 0, st>>>(                \
-                    io, fs_c, run_stride_c, nrows, g.hnzp, tw_zm, tw_zn, scale, kz_keep, kz_span);  \
-        } else {                                                                                    \
-            constexpr int RR = prows(MM);                                                           \
-            fft_z_products_kernel<T, MM, RR>                                                        \
-                <<<dim3((nrows + RR - 1) / RR, nruns), RR * Split<MM>::N1, psmem(MM), st>>>(        \
-                    io, fs_c, run_stride_c, nrows, g.hnzp, tw_zm, tw_zn, scale, kz_keep, kz_span);  \
-        }                                                                                           \
+#define SPM_ZP(MM)                                                                                              \
+    case MM: {                                                                                                  \
+        constexpr int RR = prows<MM>();                                                                         \
+        zr_products_kernel<T, MM, RR, ureg<MM>()>                                                               \
+            <<<dim3((nrows + RR - 1) / RR, nruns), RR * ZR<MM>::P, zr_products_smem<T, MM, RR, ureg<MM>()>(), st>>>( \
+                io, fs_c, run_stride_c, nrows, g.hnzp, tw_zm, tw_zn, scale, kz_keep, kz_span);                 \
     } break;
             SPM_ZP(4) SPM_ZP(8) SPM_ZP(16) SPM_ZP(32) SPM_ZP(64) SPM_ZP(128) SPM_ZP(256)
 #undef SPM_ZP
@@ -113,11 +91,11 @@ struct FFTPlan {
                       int kz_span = 1 << 30) const {
         const int nrows = g.nx * g.ny;
         switch (g.nz / 2) {
-#define SPM_ZR2C(MM)                                                                                   \
-    case MM: {                                                                                         \
-        constexpr int RR = zrows(MM);                                                                  \
-        fft_z_r2c_kernel<T, MM, RR><<<dim3((nrows + RR - 1) / RR, nfields), RR * Split<MM>::N1, 0, st>>>( \
-            in, out, fs_real, fs_c, nrows, g.hnzp, tw_zm, tw_zn, kz_span);                             \
+#define SPM_ZR2C(MM)                                                                                          \
+    case MM: {                                                                                                \
+        constexpr int RR = zr_rows<T, MM>();                                                                  \
+        zr_r2c_kernel<T, MM, RR><<<dim3((nrows + RR - 1) / RR, nfields), RR * ZR<MM>::P, 0, st>>>(            \
+            in, out, fs_real, fs_c, nrows, g.hnzp, tw_zm, tw_zn, kz_span);                                    \
     } break;
             SPM_ZR2C(4) SPM_ZR2C(8) SPM_ZR2C(16) SPM_ZR2C(32) SPM_ZR2C(64) SPM_ZR2C(128) SPM_ZR2C(256)
 #undef SPM_ZR2C
@@ -129,11 +107,11 @@ struct FFTPlan {
                       cudaStream_t st, int kz_keep = 1 << 30) const {
         const int nrows = g.nx * g.ny;
         switch (g.nz / 2) {
-#define SPM_ZC2R(MM)                                                                                   \
-    case MM: {                                                                                         \
-        constexpr int RR = zrows(MM);                                                                  \
-        fft_z_c2r_kernel<T, MM, RR><<<dim3((nrows + RR - 1) / RR, nfields), RR * Split<MM>::N1, 0, st>>>( \
-            in, out, fs_c, fs_real, nrows, g.hnzp, tw_zm, tw_zn, scale, kz_keep);                      \
+#define SPM_ZC2R(MM)                                                                                          \
+    case MM: {                                                                                                \
+        constexpr int RR = zr_rows<T, MM>();                                                                  \
+        zr_c2r_kernel<T, MM, RR><<<dim3((nrows + RR - 1) / RR, nfields), RR * ZR<MM>::P, 0, st>>>(            \
+            in, out, fs_c, fs_real, nrows, g.hnzp, tw_zm, tw_zn, scale, kz_keep);                             \
     } break;
             SPM_ZC2R(4) SPM_ZC2R(8) SPM_ZC2R(16) SPM_ZC2R(32) SPM_ZC2R(64) SPM_ZC2R(128) SPM_ZC2R(256)
 #undef SPM_ZC2R
@@ -146,9 +124,12 @@ struct FFTPlan {
     // (size or missing driver entry point); the caller then uses strided().
     static constexpr int W_T = sizeof(T) == 8 ? 16 : 32;
     static constexpr int S_T = 3;
-    // FP32 advection products with the velocity rows in registers
-    static constexpr bool kRegProducts = true;
     unsigned int *err = nullptr;  // device error word (set by the owner)
+    // bound of every TMA ring wait, global-timer nanoseconds
+    unsigned long long wait_ns = kWaitLimitNs;
+    // test switch: the next skip_loads TMA pass launches issue no loads, so
+    // their waits run out (see fft_strided_tma_kernel)
+    mutable int skip_loads = 0;
     int           ctas_per_sm = 1;
     int           sm_count    = 148;
 
@@ -176,12 +157,14 @@ struct FFTPlan {
             return cudaErrorNotSupported;
         const cplx<T> *tw   = axis == 1 ? tw_y : tw_x;
         const int      grid = std::min(ntiles, sm_count * ctas_per_sm);
+        const int      skip = skip_loads > 0 ? 1 : 0;
+        if (skip) skip_loads--;
         switch (n) {
 #define SPM_TMA(NN)                                                                                            \
     case NN:                                                                                                   \
         fft_strided_tma_kernel<T, NN, W_T, DIR, S_T>                                                           \
             <<<grid, W_T * Split<NN>::N1, (size_t)S_T * NN * W_T * sizeof(cplx<T>), st>>>(                     \
-                lmap, smap, axis, outer, ct_used, ntiles, tw, err, pr);                                        \
+                lmap, smap, axis, outer, ct_used, ntiles, tw, err, pr, wait_ns, skip);                         \
         break;
             SPM_TMA(8) SPM_TMA(16) SPM_TMA(32) SPM_TMA(64) SPM_TMA(128) SPM_TMA(256)
 #undef SPM_TMA
@@ -251,8 +234,9 @@ struct FFTPlan {
     }
     template <int MM>
     static cudaError_t attr_products() {
-        return cudaFuncSetAttribute(fft_z_products_kernel<T, MM, prows(MM)>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem(MM));
+        return cudaFuncSetAttribute(zr_products_kernel<T, MM, prows<MM>(), ureg<MM>()>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)zr_products_smem<T, MM, prows<MM>(), ureg<MM>()>());
     }
     static cudaError_t set_smem_attrs() {
         cudaError_t e = cudaSuccess;

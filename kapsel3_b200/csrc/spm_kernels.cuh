@@ -1083,6 +1083,116 @@ __global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Cell list of the Lennard-Jones forces (Calc_f_Lennard_Jones_shear_cap_
+// primitive_lnk, md_force.cxx:34-196): cells of Cell_length DX = 16 DX per
+// axis, lc[d] = N[d] / 16 of them (md_force.cxx:14, 56-61), a particle in the
+// cell (int)(x / 16 DX) of each axis (md_force.cxx:68-75).
+// Layout: count[ncell], cell_of[np], bins[ncell][kLjBin].  A cell holding
+// more than kLjBin particles keeps its count; its scans then go over all
+// particles with cell_of == cell instead of the bin.
+// ---------------------------------------------------------------------------
+constexpr int kLjBin = 32;
+
+__device__ __forceinline__ int lj_cell_axis(const Phys &ph, double x, int d, bool &bad) {
+    int m = (int)(x / ph.cell_len);
+    if (m < 0 || m >= ph.lc[d]) {
+        bad = true;
+        m   = m < 0 ? 0 : ph.lc[d] - 1;
+    }
+    return m;
+}
+
+// One thread per particle: its cell, and a slot in the cell's bin (count[]
+// zeroed before the launch).
+__global__ void p_cells_bin(Phys ph, const double *__restrict__ x, int *__restrict__ count,
+                            int *__restrict__ cell_of, int *__restrict__ bins, unsigned int *err) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ph.np) return;
+    bool      bad = false;
+    const int c   = (lj_cell_axis(ph, x[3 * n], 0, bad) * ph.lc[1] + lj_cell_axis(ph, x[3 * n + 1], 1, bad)) *
+                      ph.lc[2] +
+                  lj_cell_axis(ph, x[3 * n + 2], 2, bad);
+    if (bad && err) atomicOr(err, SPM_DEVERR_PARTICLE_OUT_OF_BOX);
+    cell_of[n]       = c;
+    const int slot   = atomicAdd(&count[c], 1);
+    if (slot < kLjBin) bins[(size_t)c * kLjBin + slot] = n;
+}
+
+// The next particle index above `last` in cell c (np when none): the bin's
+// entries, or every particle of the cell when the bin overflowed.  Visiting a
+// cell in increasing particle index keeps every sum in a fixed order.
+__device__ __forceinline__ int lj_next_in_cell(const Phys &ph, int c, int last, const int *__restrict__ count,
+                                               const int *__restrict__ cell_of, const int *__restrict__ bins) {
+    const int k    = count[c];
+    int       best = ph.np;
+    if (k <= kLjBin) {
+        for (int i = 0; i < k; i++) {
+            const int m = bins[(size_t)c * kLjBin + i];
+            if (m > last && m < best) best = m;
+        }
+    } else {
+        for (int m = last + 1; m < ph.np; m++)
+            if (cell_of[m] == c) return m;
+    }
+    return best;
+}
+
+// LJ pair forces from the cell list plus the constant body force (Force,
+// particle_solver.h:88-111).  One warp per particle n: lane l < 27 takes the
+// l-th neighbour cell of n's cell in the reference's scan order with its wrap
+// (-1 -> lc-1, lc -> 0, md_force.cxx:86-101), so with fewer than three cells
+// on an axis a neighbour cell comes up more than once and its pairs count as
+// often, as in the reference; a warp sum in a fixed order follows.  Every
+// pair term is the one the reference forms for i > j with Distance0(x_i,
+// x_j); lj_stress[n] receives particle n's share of sum f_x r_y over the
+// pairs where it is the higher index.  Pairs of two obstacles exert no force
+// (obstacle_chain, interaction.h:29-35; Janus particles are one species here).
+__global__ void p_forces_cells(Phys ph, PState s, const int *__restrict__ count, const int *__restrict__ cell_of,
+                               const int *__restrict__ bins) {
+    const int lane = threadIdx.x & 31;
+    const int n    = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (n >= ph.np) return;
+    double f[3]   = {0.0, 0.0, 0.0};
+    double stress = 0.0;
+    if (ph.lj_on && ph.janus_prop != 3 && lane < 27) {
+        const int mc[3] = {cell_of[n] / (ph.lc[1] * ph.lc[2]), (cell_of[n] / ph.lc[2]) % ph.lc[1],
+                           cell_of[n] % ph.lc[2]};
+        const int o[3]  = {lane / 9 - 1, (lane / 3) % 3 - 1, lane % 3 - 1};
+        int       cl[3];
+        for (int d = 0; d < 3; d++) {
+            int c = mc[d] + o[d];
+            if (c < 0) c = ph.lc[d] - 1;
+            if (c > ph.lc[d] - 1) c = 0;
+            cl[d] = c;
+        }
+        const int cell = (cl[0] * ph.lc[1] + cl[1]) * ph.lc[2] + cl[2];
+        for (int m = lj_next_in_cell(ph, cell, -1, count, cell_of, bins); m < ph.np;
+             m     = lj_next_in_cell(ph, cell, m, count, cell_of, bins)) {
+            if (m == n) continue;
+            const int    hi = n > m ? n : m, lo = n > m ? m : n;
+            double       rij[3];
+            const double rr = min_image(ph, s.x + 3 * hi, s.x + 3 * lo, rij);
+            if (!(rr < ph.lj_cutoff)) continue;
+            const double sg    = (n == hi) ? 1.0 : -1.0;
+            const double dmy_r = lj_f(rr, ph);
+            for (int d = 0; d < 3; d++) f[d] += -dmy_r * (sg * rij[d]);
+            if (n == hi) stress += (-dmy_r * rij[0]) * rij[1];
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        f[0] += __shfl_xor_sync(0xffffffffu, f[0], o);
+        f[1] += __shfl_xor_sync(0xffffffffu, f[1], o);
+        f[2] += __shfl_xor_sync(0xffffffffu, f[2], o);
+        stress += __shfl_xor_sync(0xffffffffu, stress, o);
+    }
+    if (lane == 0) {
+        for (int d = 0; d < 3; d++) s.fr[3 * n + d] += f[d] + ph.body_force[d];
+        s.lj_stress[n] = stress;
+    }
+}
+
 // MD_solver_velocity_Euler / _AB2_hydro (particle_solver.cxx:103-142,
 // 239-281) followed by reset_Forces (particle_solver.cxx:11-37).
 // Velocity / angular-velocity update of particle n (Euler at step 0, AB2

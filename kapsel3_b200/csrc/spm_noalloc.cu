@@ -14,8 +14,11 @@
 //   * FP64, grids of 8..64 points per axis (NX*NY*(NZ/2+1) complex values
 //     per field at most 64*64*33);
 //   * the first call on a device resolves the array's device address with
-//     cudaGetSymbolAddress and uploads the FFT twiddle tables; make that
-//     first call before any stream capture;
+//     cudaGetSymbolAddress and uploads the FFT twiddle tables of every
+//     supported size into it; make that first call before any stream
+//     capture.  Later calls issue only kernels and memsets on `stream`;
+//   * the transforms use the passes without device-side waits, so a call has
+//     no device error to report and stays asynchronous;
 //   * every call shares the one array: calls that overlap on the GPU (two
 //     streams, two host threads) race and give wrong results.
 #include <mutex>
@@ -31,11 +34,20 @@ namespace {
 
 constexpr int    kNoAllocMaxN     = 64;
 constexpr size_t kNoAllocField    = (size_t)kNoAllocMaxN * kNoAllocMaxN * (kNoAllocMaxN + 2);  // doubles
-constexpr size_t kNoAllocTwiddles = 4 * kNoAllocMaxN;                                        // complex
-constexpr size_t kNoAllocDoubles  = 3 * kNoAllocField + 2 * kNoAllocTwiddles + 2;
+// twiddle tables of the sizes n = 8, 16, 32, 64: for each n the length-n
+// table of the X and Y passes, then the z tables of NZ = n (n/2 and n/2 + 1
+// values), 2n + 1 complex values in all
+constexpr int    kNoAllocTwiddles = 2 * (8 + 16 + 32 + 64) + 4;                                // complex
+constexpr size_t kNoAllocDoubles  = 3 * kNoAllocField + 2 * (size_t)kNoAllocTwiddles;
 
-// The scratch: three padded FP64 fields, the twiddle tables and the device
-// error word of the TMA passes.
+// offset (complex values) of the tables of size n = 2^lg (lg = 3..6)
+constexpr int tw_offset(int lg) {
+    int o = 0;
+    for (int l = 3; l < lg; l++) o += 2 * (1 << l) + 1;
+    return o;
+}
+
+// The scratch: three padded FP64 fields and the twiddle tables.
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
 struct NoAllocDevice {
@@ -103,7 +115,8 @@ void fill_table(cplx<double> *dst, int n, int count) {
 }
 
 // Once per device, with that device current: resolve the scratch's device
-// address and configure the FFT kernels.  No allocation.
+// address, configure the FFT kernels and upload the twiddle tables of every
+// supported size (a synchronous copy into the array).  No allocation.
 int setup_device(int dev, NoAllocDevice *&out) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     NoAllocDevice              &d = g_dev[dev];
@@ -114,7 +127,18 @@ int setup_device(int dev, NoAllocDevice *&out) {
             return spm_internal_fail(SPM_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch) failed");
         if (FFTPlan<double>::configure_kernels() != cudaSuccess)
             return spm_internal_fail(SPM_ERR_CUDA, "FFT kernel configuration failed");
-        d.base  = static_cast<double *>(ptr);
+        static cplx<double> htw[kNoAllocTwiddles];
+        for (int lg = 3; lg <= 6; lg++) {
+            const int     n = 1 << lg;
+            cplx<double> *t = htw + tw_offset(lg);
+            fill_table(t, n, n);
+            fill_table(t + n, n / 2, n / 2);
+            fill_table(t + n + n / 2, n, n / 2 + 1);
+        }
+        double *base = static_cast<double *>(ptr);
+        if (cudaMemcpy(base + 3 * kNoAllocField, htw, sizeof(htw), cudaMemcpyHostToDevice) != cudaSuccess)
+            return spm_internal_fail(SPM_ERR_CUDA, "twiddle table upload failed");
+        d.base  = base;
         d.ready = true;
     }
     out = &d;
@@ -152,31 +176,22 @@ extern "C" int spm_make_f_particle_dt_sole_noalloc(const double *u0, const doubl
         g.wave[k] = 2.0 * 3.14159265358979323846 / (double)n3[k];  // DX = 1 grid units
     }
     g.dx = 1.0;
-    const size_t fc = g.field_elems_c();  // complex per field
-    double      *fields = d->base;
-    cplx<double> *tw    = reinterpret_cast<cplx<double> *>(d->base + 3 * kNoAllocField);
-    unsigned int *err   = reinterpret_cast<unsigned int *>(d->base + 3 * kNoAllocField + 2 * kNoAllocTwiddles);
+    const size_t  fc     = g.field_elems_c();  // complex per field
+    double       *fields = d->base;
+    cplx<double> *tw     = reinterpret_cast<cplx<double> *>(d->base + 3 * kNoAllocField);
+    auto          table  = [&](int n) { return tw + tw_offset(__builtin_ctz((unsigned)n)); };
 
-    // Twiddle tables of this call's sizes (four tables, 64 complex each), from
-    // a fixed host buffer; cleared fields (the padding of a row is never
-    // written by na_make_f and must read as zero).
-    cplx<double> htw[kNoAllocTwiddles];
-    fill_table(htw, g.nx, g.nx);
-    fill_table(htw + kNoAllocMaxN, g.ny, g.ny);
-    fill_table(htw + 2 * kNoAllocMaxN, g.nz / 2, g.nz / 2);
-    fill_table(htw + 3 * kNoAllocMaxN, g.nz, g.nz / 2 + 1);
-    if (cudaMemcpyAsync(tw, htw, sizeof(htw), cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemsetAsync(fields, 0, 3 * fc * sizeof(cplx<double>), st) != cudaSuccess ||
-        cudaMemsetAsync(err, 0, sizeof(unsigned int), st) != cudaSuccess)
+    // Cleared fields: the padding of a row is never written by na_make_f and
+    // must read as zero.
+    if (cudaMemsetAsync(fields, 0, 3 * fc * sizeof(cplx<double>), st) != cudaSuccess)
         return spm_internal_fail(SPM_ERR_CUDA, "spm_make_f_particle_dt_sole_noalloc: scratch set-up failed");
 
     FFTPlan<double> plan;
     plan.g     = g;
-    plan.tw_x  = tw;
-    plan.tw_y  = tw + kNoAllocMaxN;
-    plan.tw_zm = tw + 2 * kNoAllocMaxN;
-    plan.tw_zn = tw + 3 * kNoAllocMaxN;
-    plan.err   = err;
+    plan.tw_x  = table(g.nx);
+    plan.tw_y  = table(g.ny);
+    plan.tw_zm = table(g.nz) + g.nz;
+    plan.tw_zn = table(g.nz) + g.nz + g.nz / 2;
     int sms    = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     plan.sm_count = sms;
@@ -185,10 +200,7 @@ extern "C" int spm_make_f_particle_dt_sole_noalloc(const double *u0, const doubl
     cudaError_t e = cudaGetLastError();
     cplx<double> *fk = reinterpret_cast<cplx<double> *>(fields);
     auto strided = [&](int dir, int axis) {
-        cudaError_t r = dir < 0 ? plan.strided_tma<-1>(fk, 3, fc, axis, st) : plan.strided_tma<+1>(fk, 3, fc, axis, st);
-        if (r == cudaErrorNotSupported)
-            r = dir < 0 ? plan.strided<-1>(fk, 3, fc, axis, st) : plan.strided<+1>(fk, 3, fc, axis, st);
-        return r;
+        return dir < 0 ? plan.strided<-1>(fk, 3, fc, axis, st) : plan.strided<+1>(fk, 3, fc, axis, st);
     };
     if (e == cudaSuccess) e = plan.z_r2c(fields, fk, 3, 2 * fc, fc, st);
     if (e == cudaSuccess) e = strided(-1, 1);

@@ -3,9 +3,9 @@
 // driver entry point (no link-time dependency on libcuda).
 //
 // Only plain (non-multicast) tiled loads and stores are used, always on this
-// GPU's own memory.  Every wait on an mbarrier is bounded: after
-// kSpinLimit polls the waiting thread records SPM_DEVERR_TIMEOUT in the
-// device error word and gives up.
+// GPU's own memory.  Every wait on an mbarrier is bounded in time: once the
+// global nanosecond timer has advanced by the caller's limit the waiting
+// thread records SPM_DEVERR_TIMEOUT in the device error word and gives up.
 #pragma once
 
 #include <cuda.h>
@@ -14,8 +14,14 @@
 
 namespace spm {
 
-constexpr unsigned int SPM_DEVERR_TIMEOUT = 1u << 4;
-constexpr long long    kSpinLimit         = 1ll << 26;
+constexpr unsigned int       SPM_DEVERR_TIMEOUT = 1u << 4;
+constexpr unsigned long long kWaitLimitNs       = 1000000000ull;  // default bound of one wait: 1 s
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) {
     return (unsigned)__cvta_generic_to_shared(p);
@@ -32,10 +38,14 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
                  : "memory");
 }
 
-// Bounded wait for phase `parity` of an mbarrier.  Returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned int *err) {
-    const unsigned a = smem_addr(bar);
-    for (long long it = 0; it < kSpinLimit; it++) {
+// Wait for phase `parity` of an mbarrier for at most limit_ns nanoseconds of
+// the global timer.  Returns false on timeout (and records it in *err when
+// err is given).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned int *err,
+                                          unsigned long long limit_ns) {
+    const unsigned           a  = smem_addr(bar);
+    const unsigned long long t0 = global_ns();
+    for (;;) {
         unsigned done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -43,6 +53,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsign
             : "r"(a), "r"(parity)
             : "memory");
         if (done) return true;
+        if (global_ns() - t0 > limit_ns) break;
     }
     if (err) atomicOr(err, SPM_DEVERR_TIMEOUT);
     return false;

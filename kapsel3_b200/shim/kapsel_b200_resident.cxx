@@ -1,0 +1,93 @@
+// Device-resident time evolution inside the unmodified KAPSEL program.
+//
+// The reference's main loop advances the run through the function pointer
+// Time_evolution (sp_3d_ns.cxx:10, set to Time_evolution_hydro or
+// Time_evolution_hydro_OBL at sp_3d_ns.cxx:690-707, called at :954).  Once
+// the reference has finished its own initialisation (the initial projection,
+// sp_3d_ns.cxx:809-826), kapsel_b200_go_resident() points it at
+// resident_time_evolution below, which keeps zeta, uk_dc and the particles on
+// the GPU and advances them with spm_step.  The host copies are refreshed only
+// where the main loop reads them: before an output frame (ts % GTS == 0,
+// sp_3d_ns.cxx:863-874) and before the restart file written after the last
+// step (sp_3d_ns.cxx:974-982).
+//
+// Served: Navier_Stokes and Shear_Navier_Stokes_Lees_Edwards runs of one
+// particle species with spherical particles, not resumed.  For any other run
+// the pointer is left alone and the reference steps on the CPU.  In a
+// Lees-Edwards run the main loop's per-step stress print (Mean_shear_stress,
+// sp_3d_ns.h:247-339) reads CPU-side globals this path does not update;
+// spm_get_shear_state returns that line from the device.
+#include <vector>
+
+#include "kapsel_b200_common.h"
+
+extern void (*Time_evolution)(double **zeta, double uk_dc[DIM], double **f, Particle *p, CTime &jikan);
+extern double *phi;
+
+namespace {
+
+using kapsel_b200::check;
+
+spm_ctx            *g_run = nullptr;
+int                 g_eq  = SPM_EQ_NAVIER_STOKES;
+std::vector<double> g_rec;
+double              g_body_force[3] = {0.0, 0.0, 0.0};
+
+// Host copies of the state the main loop reads: zeta, uk_dc, the particles,
+// phi (output frames) and, for Lees-Edwards, degree_oblique.
+void download(double **zeta, double uk_dc[DIM], Particle *p) {
+    check(spm_get_zeta(g_run, zeta[0], zeta[1], uk_dc), "spm_get_zeta");
+    g_rec.assign((size_t)Particle_Number * SPM_PARTICLE_WORDS, 0.0);
+    check(spm_get_particles(g_run, g_rec.data()), "spm_get_particles");
+    kapsel_b200::unpack_records(g_rec.data(), p);
+    if (phi) check(spm_get_phi(g_run, phi), "spm_get_phi");
+    if (g_eq == SPM_EQ_LEES_EDWARDS) {
+        double stress[8];
+        check(spm_get_shear_state(g_run, &degree_oblique, stress), "spm_get_shear_state");
+    }
+}
+
+void resident_time_evolution(double **zeta, double uk_dc[DIM], double **f, Particle *p, CTime &jikan) {
+    (void)f;
+    if (!g_run) {  // the reference's state after its initial projection
+        spm_params prm = kapsel_b200::params_from_globals(g_eq);
+        for (int d = 0; d < DIM; d++) prm.body_force[d] = g_body_force[d];
+        check(spm_create(&prm, nullptr, &g_run), "spm_create");
+        check(spm_set_zeta(g_run, zeta[0], zeta[1], uk_dc), "spm_set_zeta");
+        check(spm_set_particles(g_run, kapsel_b200::records(p, g_rec)), "spm_set_particles");
+    }
+    if (jikan.dt_fluid != DT) {
+        fprintf(stderr, "kapsel_b200: dt changed during the run (%g != %g)\n", jikan.dt_fluid, DT);
+        exit_job(EXIT_FAILURE);
+    }
+    check(spm_step(g_run, 1), "spm_step");
+    const int next = jikan.ts + 1;
+    if (jikan.ts == MSTEP || (next <= MSTEP && next % GTS == 0)) download(zeta, uk_dc, p);
+}
+
+}  // namespace
+
+// A constant force on every particle, added where Force() adds gravity
+// (particle_solver.h:88-111); for a host that applies one on the CPU side
+// (the reference has no input for it at density 1).  Call before
+// kapsel_b200_go_resident.
+extern "C" void kapsel_b200_set_body_force(double fx, double fy, double fz) {
+    g_body_force[0] = fx;
+    g_body_force[1] = fy;
+    g_body_force[2] = fz;
+}
+
+// Called by the program once its initialisation is complete and before its
+// main loop (see the build's Show_output_parameter hook).
+extern "C" void kapsel_b200_go_resident() {
+    if (RESUMED || Component_Number != 1 || SW_PT != spherical_particle || SW_JANUS || SW_WALL != NO_WALL) return;
+    if (SW_EQ == Navier_Stokes) {
+        g_eq = SPM_EQ_NAVIER_STOKES;
+    } else if (SW_EQ == Shear_Navier_Stokes_Lees_Edwards) {
+        g_eq = SPM_EQ_LEES_EDWARDS;
+    } else {
+        return;
+    }
+    Time_evolution = resident_time_evolution;
+    fprintf(stderr, "# kapsel_b200: time evolution resident on the GPU (host copies at output frames)\n");
+}

@@ -24,40 +24,21 @@
 // (the _host entry points); header-inline reference code between the calls
 // (A2a_k / A_k2a FFTs, the particle integrators) keeps running on the CPU.
 // Keeping state resident across a whole step is the job of spm_step, which a
-// maintainer calls from Time_evolution_hydro itself (INTEGRATION.md).
+// maintainer calls from Time_evolution_hydro itself.
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
 
-#include "input.h"
-#include "macro.h"
-#include "variable.h"
-
-#include "kapsel_spm.h"
+#include "kapsel_b200_common.h"
 
 namespace {
 
+using kapsel_b200::check;
+
 spm_ctx            *g_ctx = nullptr;
 std::vector<double> g_rec;
-
-void check(int rc, const char *what) {
-    if (rc != SPM_OK) {
-        fprintf(stderr, "kapsel_b200: %s failed: %s\n", what, spm_last_error());
-        exit_job(EXIT_FAILURE);
-    }
-}
-
-int log2_exact(int n, const char *axis) {
-    int k = 0;
-    while ((1 << k) < n) k++;
-    if ((1 << k) != n) {
-        fprintf(stderr, "kapsel_b200: N%s = %d is not a power of two\n", axis, n);
-        exit_job(EXIT_FAILURE);
-    }
-    return k;
-}
 
 spm_ctx *ctx() {
     if (g_ctx) return g_ctx;
@@ -65,61 +46,12 @@ spm_ctx *ctx() {
         fprintf(stderr, "kapsel_b200: the GPU boundary serves Navier_Stokes runs with one particle species\n");
         exit_job(EXIT_FAILURE);
     }
-    if (spm_params_size() != sizeof(spm_params)) {
-        fprintf(stderr, "kapsel_b200: libkapsel_spm was built from another kapsel_spm.h (spm_params %zu bytes, "
-                        "this program %zu): rebuild the program\n",
-                spm_params_size(), sizeof(spm_params));
-        exit_job(EXIT_FAILURE);
-    }
-    spm_params p;
-    check(spm_params_default(&p), "spm_params_default");
-    p.npx         = log2_exact(NX, "X");
-    p.npy         = log2_exact(NY, "Y");
-    p.npz         = log2_exact(NZ, "Z");
-    p.dx          = DX;
-    p.rho         = RHO;
-    p.eta         = ETA;
-    p.kbt         = kBT;
-    p.alpha_v     = alpha_v;
-    p.alpha_o     = alpha_o;
-    p.equation    = SPM_EQ_NAVIER_STOKES;
-    p.n_particles = Particle_Number;
-    p.mass_ratio  = MASS_RATIOS[0];
-    p.a           = A;
-    p.a_xi        = A_XI;
-    p.epsilon     = EPSILON;
-    p.lj_powers   = LJ_powers;
-    p.lj_truncate = LJ_truncate;
-    p.rotation    = ROTATION;
-    for (int d = 0; d < DIM; d++) p.fix_cell[d] = FIX_CELLxyz[d];
-    p.dt        = DT;
-    p.precision = SPM_PREC_FP64;
+    spm_params p = kapsel_b200::params_from_globals(SPM_EQ_NAVIER_STOKES);
     check(spm_create(&p, nullptr, &g_ctx), "spm_create");
     return g_ctx;
 }
 
-// Particle (variable.h:27-77) -> SPM_PARTICLE_WORDS records.
-double *records(const Particle *p) {
-    g_rec.assign((size_t)Particle_Number * SPM_PARTICLE_WORDS, 0.0);
-    for (int n = 0; n < Particle_Number; n++) {
-        double         *r  = g_rec.data() + (size_t)n * SPM_PARTICLE_WORDS;
-        const Particle &q  = p[n];
-        const double   *a[] = {q.x, q.x_nopbc, q.v, q.v_old, q.omega, q.omega_old};
-        for (int i = 0; i < 6; i++)
-            for (int d = 0; d < 3; d++) r[3 * i + d] = a[i][d];
-        r[18] = q.q.s;
-        r[22] = q.q_old.s;
-        for (int d = 0; d < 3; d++) {
-            r[19 + d] = q.q.v[d];
-            r[23 + d] = q.q_old.v[d];
-        }
-        const double *b[] = {q.f_hydro, q.f_hydro_previous, q.torque_hydro, q.torque_hydro_previous, q.fr,
-                             q.fr_previous};
-        for (int i = 0; i < 6; i++)
-            for (int d = 0; d < 3; d++) r[26 + 3 * i + d] = b[i][d];
-    }
-    return g_rec.data();
-}
+double *records(const Particle *p) { return kapsel_b200::records(p, g_rec); }
 
 }  // namespace
 

@@ -30,29 +30,42 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
+# The reference source tree: the environment variable KAPSEL_REFERENCE_TREE,
+# else the tree the build of REF_DIR recorded in REF_DIR/REFERENCE_TREE.
+TREE_RECORD = os.path.join(REF_DIR, "REFERENCE_TREE")
+
+
+def reference_tree() -> Optional[str]:
+    p = os.environ.get("KAPSEL_REFERENCE_TREE")
+    if not p and os.path.exists(TREE_RECORD):
+        p = open(TREE_RECORD).read().strip()
+    return p if p and os.path.isdir(p) else None
 PARTICLE_FIELDS = [("x", 3), ("x_nopbc", 3), ("v", 3), ("v_old", 3), ("omega", 3), ("omega_old", 3),
                    ("q", 4), ("q_old", 4), ("f_hydro", 3), ("f_hydro_previous", 3),
                    ("torque_hydro", 3), ("torque_hydro_previous", 3), ("fr", 3), ("fr_previous", 3)]
 PARTICLE_WORDS = sum(n for _, n in PARTICLE_FIELDS)
 
 
-def ref_binary(omp: bool = False, gpu_shim: bool = False) -> Optional[str]:
-    """kapsel_ref (serial), kapsel_ref_omp (OpenMP) or kapsel_gpu (serial, with
+def ref_binary(omp: bool = False, gpu_shim: bool = False, gpu_resident: bool = False) -> Optional[str]:
+    """kapsel_ref (serial), kapsel_ref_omp (OpenMP), kapsel_gpu (serial, with
     the reference's boundary functions linked to the B200 library through
-    kapsel3_b200/shim)."""
-    name = "kapsel_gpu" if gpu_shim else ("kapsel_ref_omp" if omp else "kapsel_ref")
+    kapsel3_b200/shim) or kapsel_gpu_resident (OpenMP host part, its main loop
+    advanced on the GPU by kapsel3_b200/shim/kapsel_b200_resident.cxx)."""
+    name = ("kapsel_gpu_resident" if gpu_resident else "kapsel_gpu" if gpu_shim
+            else ("kapsel_ref_omp" if omp else "kapsel_ref"))
     p = os.path.join(REF_DIR, name)
     return p if os.access(p, os.X_OK) else None
 
 
-def available(omp: bool = False, gpu_shim: bool = False) -> bool:
-    return ref_binary(omp, gpu_shim) is not None
+def available(omp: bool = False, gpu_shim: bool = False, gpu_resident: bool = False) -> bool:
+    return ref_binary(omp, gpu_shim, gpu_resident) is not None
 
 
 def run_reference(keys_path: str, dump_path: Optional[str] = None, fields_every: int = 1,
                   body_force=(0.0, 0.0, 0.0), omp: bool = False, threads: Optional[int] = None,
-                  step_times_path: Optional[str] = None, timeout: float = 3600.0, gpu_shim: bool = False) -> str:
-    exe = ref_binary(omp, gpu_shim)
+                  step_times_path: Optional[str] = None, timeout: float = 3600.0, gpu_shim: bool = False,
+                  gpu_resident: bool = False) -> str:
+    exe = ref_binary(omp, gpu_shim, gpu_resident)
     if exe is None:
         raise FileNotFoundError("oracle/_ref is not built (make -C oracle/ref_build)")
     env = dict(os.environ)

@@ -7,8 +7,9 @@ may differ where three or more profiles overlap a cell).  Covered: FP64
 Navier_Stokes with the thermostat (MT19937 state), FP32-mixed (compensated
 zeta words), Lees-Edwards (degree_oblique and its device scalars) and
 Electrolyte (ion concentrations and Total_solute; AC field in time).  A
-checkpoint is refused by a context with other parameters, and a truncated
-file is refused."""
+checkpoint is refused by a context with other parameters (a Shear_Navier_Stokes
+state by a run with another sustained profile), and a truncated file is
+refused."""
 import os
 
 import numpy as np
@@ -16,7 +17,7 @@ import pytest
 
 from kapsel3_b200 import _native as N
 from kapsel3_b200.spm import SPMRun
-from kapsel3_b200.udf import EQ_EL, EQ_LE, SPMConfig, make_particles
+from kapsel3_b200.udf import EQ_EL, EQ_LE, EQ_SNS, SPMConfig, make_particles
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
@@ -93,3 +94,24 @@ def test_checkpoint_is_refused_by_another_run(gpu, tmp_path):
     with SPMRun(cfg, precision=prec) as b:
         with pytest.raises(N.SpmError, match="truncated"):
             b.load_state(short)
+
+
+def test_shear_checkpoint_keeps_its_profile(gpu, tmp_path):
+    """A Shear_Navier_Stokes state restores only into a run with the same
+    sustained profile: an AC state is refused by a DC run and by an AC run of
+    another frequency."""
+    ac = SPMConfig(npx=5, npy=5, npz=5, n_particles=2, a=4.0, a_xi=2.0, dt=0.05, equation=EQ_SNS, shear_rate=0.01,
+                   shear_ac=True, shear_frequency=0.2)
+    parts = make_particles(ac, seed=5)
+    path = os.path.join(tmp_path, "ac.ck")
+    with SPMRun(ac) as a:
+        a.initialize(parts)
+        a.step(2)
+        a.save_state(path)
+    with SPMRun(ac) as b:
+        b.load_state(path)
+    for other in (SPMConfig(**{**ac.__dict__, "shear_ac": False, "shear_frequency": 0.0}),
+                  SPMConfig(**{**ac.__dict__, "shear_frequency": 0.3})):
+        with SPMRun(other) as b:
+            with pytest.raises(N.SpmError):
+                b.load_state(path)

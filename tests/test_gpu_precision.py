@@ -4,11 +4,11 @@ C3: 256^3, 1000 colloids a=5, seeded state, no noise.  The FP32-mixed path
 (FP32 fields / FFT / projection / advection, zeta kept as a compensated
 FP32 pair, FP64 particle reductions, integrators and k = 0 mode) stays within
 1e-5 relative L2 of the FP64 GPU path in the velocity field, phi and particle
-x, v, omega at every 50th of 200 steps.
+x, v, omega at every 50th of 500 steps (the configuration's full length).
 
 C4: 128^3 Lees-Edwards, shear rate 1e-3, 400 colloids a=4: the mean apparent
-shear stress (Mean_shear_stress, sp_3d_ns.h:325) over 500 steps agrees within
-1e-5 relative."""
+shear stress (Mean_shear_stress, sp_3d_ns.h:325) over 2000 steps (the
+configuration's full length) agrees within 1e-5 relative."""
 import numpy as np
 import pytest
 
@@ -31,7 +31,7 @@ def test_c3_fp32_mixed_tracks_fp64(gpu):
     with SPMRun(cfg, precision=N.SPM_PREC_FP32_MIXED) as r32, SPMRun(cfg, precision=N.SPM_PREC_FP64) as r64:
         r32.initialize(parts)
         r64.initialize(parts)
-        for ts in range(50, 201, 50):
+        for ts in range(50, 501, 50):
             r32.step(50)
             r64.step(50)
             p32, p64 = r32.particles(), r64.particles()
@@ -49,7 +49,7 @@ def test_c4_lees_edwards_stress_fp32_mixed_vs_fp64(gpu):
         with SPMRun(cfg, precision=prec) as r:
             r.initialize(parts)
             app = []
-            for _ in range(500):
+            for _ in range(2000):
                 r.step(1)
                 app.append(r.shear_state()[1][7])
             means[prec] = float(np.mean(app))

@@ -49,6 +49,10 @@ CASES = {
                                  dict(seed=2, v_sd=1e-3, ro=True)),
     "noncubic_close_pairs": (SPMConfig(npx=5, npy=4, npz=6, n_particles=4, a=3.0, a_xi=2.0, dt=0.05, kbt=1e-5,
                                        body_force=(0.0, 2e-3, -1e-3)), dict(seed=5, v_sd=2e-3, ro=True)),
+    # z rows of 512 points: the longest rows the z transforms take (their
+    # velocity rows are kept in shared memory in both precisions)
+    "long_z_rows": (SPMConfig(npx=4, npy=4, npz=9, n_particles=2, a=3.0, a_xi=2.0, dt=0.05,
+                              body_force=(0.0, 0.0, 2e-3)), dict(seed=9, v_sd=1e-3, ro=True)),
 }
 
 
@@ -63,8 +67,9 @@ def test_fp64_step_matches_oracle(gpu, name):
             assert r[k] < TOL64, (name, r)
 
 
-def test_fp32_mixed_close_to_fp64(gpu):
-    cfg, init = CASES["two_spheres_body_force"]
+@pytest.mark.parametrize("name", ["two_spheres_body_force", "long_z_rows"])
+def test_fp32_mixed_close_to_fp64(gpu, name):
+    cfg, init = CASES[name]
     parts = make_particles(cfg, seed=init["seed"])
     res = run_pair(cfg, parts, nsteps=12, check_every=4, prec=N.SPM_PREC_FP32_MIXED)
     for r in res:

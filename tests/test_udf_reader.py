@@ -27,7 +27,7 @@ from kapsel3_b200.spm import config_from_udf, read_udf
 from kapsel3_b200.udf import EQ_LE, SPMConfig, make_particles, udf_keys, write_udf, write_udf_keys
 from oracle import ref_runner
 
-REFERENCE_TREE = os.environ.get("KAPSEL_REFERENCE_TREE", "/root/reference")
+REFERENCE_TREE = ref_runner.reference_tree() or ""
 
 
 def load(path, n, keys=False):

@@ -5,11 +5,13 @@ comes from their own pool or from another runtime, or their time loop must
 not call the allocator).  This entry point serves them: the caller passes
 device buffers for inputs and outputs and the call uses only a fixed device
 array built into the library.  The test calls it through the C ABI twice in
-a row, with different inputs, and compares each result with the existing
-context-based entry point spm_make_f_particle_dt_sole_host on the same
-inputs (FP64, 1e-11 relative).  It is collected last so that a run stopping
-at the first failure has already run every other test, and it works in a
-fresh process as well as after the other tests.
+a row, with different inputs, on the smallest grid (8 points per axis), a
+ragged one and the largest (64^3, whose three fields fill the fixed array),
+and compares each result with the existing context-based entry point
+spm_make_f_particle_dt_sole_host and with the oracle's Solenoidal_u of
+up - min(phi, 1) u (FP64, 1e-11 relative).  It is collected last so that a
+run stopping at the first failure has already run every other test, and it
+works in a fresh process as well as after the other tests.
 """
 import ctypes as C
 
@@ -18,7 +20,8 @@ import pytest
 
 from kapsel3_b200 import _native as N
 from kapsel3_b200.spm import SPMRun
-from kapsel3_b200.udf import SPMConfig, make_particles
+from kapsel3_b200.udf import SPMConfig
+from oracle.spm_oracle import OracleSPM
 
 pytestmark = pytest.mark.gpu
 
@@ -35,17 +38,25 @@ def _inputs(cfg, seed):
     return u, up, phi
 
 
-def test_noalloc_matches_context_entry_point(gpu):
+def _no_particles():
+    z = np.zeros((0, 3))
+    return {"x": z, "v": z, "omega": z, "q": np.zeros((0, 4))}
+
+
+@pytest.mark.parametrize("np3", [(3, 3, 3), (5, 4, 6), (6, 6, 6)])
+def test_noalloc_matches_context_entry_point_and_oracle(gpu, np3):
     import torch
 
-    cfg = SPMConfig(npx=5, npy=4, npz=6, n_particles=0, lj_truncate="NONE")
+    cfg = SPMConfig(npx=np3[0], npy=np3[1], npz=np3[2], n_particles=0, lj_truncate="NONE")
     nx, ny, nz = cfg.shape
     nzp = 2 * (nz // 2 + 1)
     L = N.lib()
+    oracle = OracleSPM(cfg, _no_particles())
     with SPMRun(cfg) as run:
         for call, seed in enumerate((101, 202)):
-            u, up, phi = _inputs(cfg, seed)
+            u, up, phi = _inputs(cfg, seed + sum(np3))
             want = run.Make_f_particle_dt_sole(u, up, phi)
+            ref = oracle.solenoidal_u(up - np.minimum(phi, 1.0) * u)
 
             def dev(a):
                 padded = np.zeros((nx, ny, nzp))
@@ -64,9 +75,11 @@ def test_noalloc_matches_context_entry_point(gpu):
             got = np.stack([t.cpu().numpy()[:, :, :nz] for t in fd])
             assert np.isfinite(got).all(), f"call {call}: output not fully written"
             assert _rel(got, want) < 1e-11, (call, _rel(got, want))
+            assert _rel(got, ref) < 1e-11, (call, _rel(got, ref))
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch(gpu):
     L = N.lib()
     assert L.spm_make_f_particle_dt_sole_noalloc(*[C.c_void_p(8)] * 10, 7, 5, 5, None) == 1
     assert b"8..64" in L.spm_last_error()
+    assert L.spm_make_f_particle_dt_sole_noalloc(*[C.c_void_p(8)] * 10, 5, 2, 5, None) == 1
