@@ -44,6 +44,9 @@ extern "C" {
 #define SPM_ERR_NO_DEVICE 5   /* no CUDA device visible */
 
 #define SPM_PARTICLE_WORDS 44
+/* Per rigid body: xGs[3], xGs without the periodic wrap[3], velocityGs[3],
+ * omegaGs[3] (space frame), Rigid_Masses, the diagonal of Rigid_Moments_body[3] */
+#define SPM_RIGID_WORDS 16
 
 #define SPM_EQ_NAVIER_STOKES 0  /* constitutive_eq.type = Navier_Stokes */
 #define SPM_EQ_LEES_EDWARDS 1   /* Shear_Navier_Stokes_Lees_Edwards */
@@ -123,6 +126,24 @@ typedef struct spm_params {
      * shear rate is shear_rate above; shear_ac = 0 DC, 1 AC with angular frequency shear_frequency */
     int    shear_ac;
     double shear_frequency;
+    /* Rigid bodies of spherical beads (object_type.type = rigid, object_type.rigid.Rigid_spec[s],
+     * input.cxx:1583-1700, 2468-2550; rigid.h).  rigid = 1: species s (n_species of them, one when
+     * n_species <= 1) holds rigid_count[s] bodies (Chain_number) of rigid_beads[s] beads
+     * (Beads_number); the n_particles records list the beads body after body, species 0 first, with
+     * coordinates as given (no periodic wrap, as the reference reads them).  The beads' MASS_RATIO is
+     * species_mass_ratio[s] (mass_ratio for one species).  rigid_free[s] = vx vy vz wx wy wz degrees
+     * of freedom, 1 free, 0 fixed (Rigid_motion "free" / "fix", switch.free_rigid); rigid_velocity[s]
+     * and rigid_omega[s] are the initial body velocity and body-frame angular velocity
+     * (Rigid_velocity, Rigid_omega).  Navier_Stokes runs with ROTATION ON, lone contexts (no pool). */
+    int    rigid;
+    int    rigid_beads[SPM_MAX_SPECIES];
+    int    rigid_count[SPM_MAX_SPECIES];
+    int    rigid_free[SPM_MAX_SPECIES][6];
+    double rigid_velocity[SPM_MAX_SPECIES][3];
+    double rigid_omega[SPM_MAX_SPECIES][3];
+    /* gravity.G along gravity.G_direction for rigid bodies: each body feels -G RHO V (MASS_RATIO - 1)
+     * along that axis, V its mass over its density (Add_f_gravity, md_force.cxx:317-322) */
+    double rigid_gravity[3];
 } spm_params;
 
 typedef struct spm_ctx spm_ctx;
@@ -173,6 +194,10 @@ int spm_step(spm_ctx *ctx, int nsteps);
 int spm_synchronize(spm_ctx *ctx);
 /* Copies state to / from host memory (blocking). */
 int spm_get_particles(spm_ctx *ctx, double *particles_host);
+/* Rigid bodies of a run (SW_PT == rigid): their number, and their state
+ * (SPM_RIGID_WORDS doubles per body; synchronising). */
+int spm_rigid_count(spm_ctx *ctx, int *n);
+int spm_get_rigid(spm_ctx *ctx, double *bodies);
 int spm_set_particles(spm_ctx *ctx, const double *particles_host);
 int spm_get_zeta(spm_ctx *ctx, double *zeta0, double *zeta1, double uk_dc[3]);
 int spm_set_zeta(spm_ctx *ctx, const double *zeta0, const double *zeta1, const double uk_dc[3]);

@@ -13,7 +13,13 @@ import re
 from . import build as _build
 
 SPM_OK = 0
+SPM_ERR_ARG = 1
+SPM_ERR_CUDA = 2
+SPM_ERR_NOMEM = 3
+SPM_ERR_DEVICE = 4
+SPM_ERR_NO_DEVICE = 5
 SPM_PARTICLE_WORDS = 44
+SPM_RIGID_WORDS = 16
 SPM_EQ_NAVIER_STOKES = 0
 SPM_EQ_LEES_EDWARDS = 1
 SPM_EQ_ELECTROLYTE = 2
@@ -65,6 +71,13 @@ class SpmParams(C.Structure):
         ("species_surface_charge", C.c_double * 4),
         ("shear_ac", C.c_int),
         ("shear_frequency", C.c_double),
+        ("rigid", C.c_int),
+        ("rigid_beads", C.c_int * 4),
+        ("rigid_count", C.c_int * 4),
+        ("rigid_free", (C.c_int * 6) * 4),
+        ("rigid_velocity", (C.c_double * 3) * 4),
+        ("rigid_omega", (C.c_double * 3) * 4),
+        ("rigid_gravity", C.c_double * 3),
     ]
 
 
@@ -156,6 +169,8 @@ _SIGS = {
     "spm_kernel_launches": (C.c_int, [_P, C.POINTER(C.c_longlong), C.c_int]),
     "spm_profile_pass": (C.c_int, [_P, C.c_int, _D, _D, C.POINTER(C.c_longlong)]),
     "spm_profile_kernels": (C.c_int, [_P, C.c_int, C.c_char_p, C.c_size_t]),
+    "spm_rigid_count": (C.c_int, [_P, C.POINTER(C.c_int)]),
+    "spm_get_rigid": (C.c_int, [_P, _D]),
     "spm_make_f_particle_dt_sole_noalloc": (C.c_int, [_P] * 10 + [C.c_int, C.c_int, C.c_int, _P]),
     "spm_pool_device_bytes": (C.c_int, [C.POINTER(SpmParams), C.c_int, C.POINTER(C.c_size_t),
                                         C.POINTER(C.c_size_t)]),

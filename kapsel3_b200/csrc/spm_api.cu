@@ -22,6 +22,7 @@
 #include "../../include/kapsel_spm.h"
 #include "spm_fft_plan.cuh"
 #include "spm_kernels.cuh"
+#include "spm_rigid.cuh"
 #include "spm_le.cuh"
 #include "spm_electrolyte.cuh"
 #include "spm_janus.cuh"
@@ -199,6 +200,12 @@ struct spm_ctx {
     // convergence value of the last slip iteration
     double      *slip     = nullptr;
     double      *slip_eps = nullptr;
+    // rigid bodies (spm_rigid.cuh): device state and the species' free degrees of freedom
+    RigidDev     rg{};
+    RigidFree    rfree{};
+    int         *rg_ibuf = nullptr;
+    double      *rg_dbuf = nullptr;
+    bool         rigid() const { return P.rigid != 0; }
     int          slip_iters = 0;  // iterations of the last step's slip loop
     // optional CUDA-event timing of the step's kernels inside real steps:
     // one record per launch (kernel family, algorithmic bytes, events on the
@@ -362,6 +369,27 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
         if (p.janus_axis == SPM_AXIS_NONE) return fail(SPM_ERR_ARG, "a SQUIRMER needs a janus_axis (X, Y or Z)");
         if (!(p.slip_vel > 0.0)) return fail(SPM_ERR_ARG, "a SQUIRMER needs janus_slip_vel (B1) > 0");
         if (p.slip_iter < 1 || !(p.slip_tol >= 0.0)) return fail(SPM_ERR_ARG, "SLIP_iter >= 1 and SLIP_tol >= 0");
+    }
+    // rigid bodies (object_type.rigid, input.cxx:1583-1700)
+    if (p.rigid) {
+        if (p.equation != SPM_EQ_NAVIER_STOKES) return fail(SPM_ERR_ARG, "rigid bodies are served in Navier_Stokes runs");
+        if (p.janus_propulsion != SPM_JANUS_OFF) return fail(SPM_ERR_ARG, "rigid bodies have no janus propulsion");
+        if (!p.rotation) return fail(SPM_ERR_ARG, "rigid bodies need ROTATION ON");
+        if (p.body_force[0] != 0.0 || p.body_force[1] != 0.0 || p.body_force[2] != 0.0)
+            return fail(SPM_ERR_ARG, "rigid bodies take no constant body force");
+        int beads = 0;
+        for (int s = 0; s < nsp; s++) {
+            if (p.rigid_beads[s] < 1 || p.rigid_count[s] < 0)
+                return fail(SPM_ERR_ARG, "rigid species need Beads_number >= 1 and Chain_number >= 0");
+            if (nsp > 1 && p.species_count[s] != p.rigid_beads[s] * p.rigid_count[s])
+                return fail(SPM_ERR_ARG, "species_count must be Beads_number * Chain_number for rigid species");
+            beads += p.rigid_beads[s] * p.rigid_count[s];
+        }
+        if (beads != p.n_particles) return fail(SPM_ERR_ARG, "the rigid bodies' beads must add up to n_particles");
+        if ((p.rigid_gravity[0] != 0.0) + (p.rigid_gravity[1] != 0.0) + (p.rigid_gravity[2] != 0.0) > 1)
+            return fail(SPM_ERR_ARG, "gravity acts along one axis (G_direction)");
+    } else if (p.rigid_gravity[0] != 0.0 || p.rigid_gravity[1] != 0.0 || p.rigid_gravity[2] != 0.0) {
+        return fail(SPM_ERR_ARG, "rigid_gravity is for rigid bodies; spherical particles take body_force");
     }
     g.nx  = 1 << p.npx;
     g.ny  = 1 << p.npy;
@@ -870,7 +898,8 @@ int lj_forces(spm_ctx *c, const Phys &ph) {
         PLAUNCH(c, "p_cells_bin", 0.0, p_cells_bin, (ph.np + 127) / 128, 128, 0, ph, c->ps.x, count, cell_of, bins,
                 c->err);
     }
-    PLAUNCH(c, "p_forces_cells", 0.0, p_forces_cells, (ph.np + 3) / 4, 128, 0, ph, c->ps, count, cell_of, bins);
+    PLAUNCH(c, "p_forces_cells", 0.0, p_forces_cells, (ph.np + 3) / 4, 128, 0, ph, c->ps, count, cell_of, bins,
+            c->rigid() ? c->rg.rid : nullptr, c->rigid() ? c->rg.f_lo : nullptr);
     return SPM_OK;
 }
 
@@ -913,7 +942,10 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
             spm_ctx *c = R[r];
             if (c->ph.np == 0) continue;
             auto side_work = [&]() -> int {
-                PLAUNCH(c, "p_position", 0.0, p_position, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev, 1);
+                if (c->rigid())
+                    PLAUNCH(c, "r_position", 0.0, r_position, c->rg.nb, 128, 0, c->ph, c->ps, c->rg, c->ts_dev);
+                else
+                    PLAUNCH(c, "p_position", 0.0, p_position, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev, 1);
                 const dim3 sgrid((c->ncells + 127) / 128, c->ph.np);
                 PLAUNCH(c, "s_phi_scatter_cache", stencil_bytes<T>(c, 0), s_phi_scatter_cache<T>, sgrid, 128, 0, c->g,
                         c->ph, c->ps.x, c->cells, c->ncells, c->real<T>(PHIS), c->err, c->sc_idx, c->sc_w);
@@ -938,14 +970,19 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
         PLAUNCH(c, "s_hydro_force_cached", stencil_bytes<T>(c, 1), s_hydro_force_cached<T>, c->ph.np, 256, 0, c->g,
                 c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells, c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS),
                 c->real<T>(U0), c->real<T>(U1), c->real<T>(U2), c->ps.f_hydro, c->ps.torque_hydro);
-        if (c->ph.janus_prop == SPM_JANUS_SQUIRMER) {
+        if (c->rigid()) {
+            LAUNCH(c, r_collect, c->rg.nb, 128, 0, c->ps, c->rg, c->rfree);
+            LAUNCH(c, r_velocity, c->rg.nb, 128, 0, c->ph, c->ps, c->rg, c->rfree, c->ts_dev);
+        } else if (c->ph.janus_prop == SPM_JANUS_SQUIRMER) {
             SPM_TRY(slip_loop<T>(c));  // lone runs only; leaves the slip field in UP
         } else {
             PLAUNCH(c, "p_velocity", 0.0, p_velocity, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev);
         }
         // obstacles draw no noise (fluct.cxx:23)
-        if (c->P.kbt > 0.0 && c->ph.janus_prop != SPM_JANUS_OBSTACLE)
-            LAUNCH(c, p_thermostat, 1, kThermoThreads, 0, c->ph, c->ps, c->mt);
+        if (c->P.kbt > 0.0 && c->ph.janus_prop != SPM_JANUS_OBSTACLE) {
+            LAUNCH(c, p_thermostat, 1, kThermoThreads, 0, c->ph, c->ps, c->mt, c->rigid() ? c->rg.noise : nullptr);
+            if (c->rigid()) LAUNCH(c, r_thermostat, c->rg.nb, 128, 0, c->ph, c->ps, c->rg, c->rfree);
+        }
         const dim3 sgrid((c->ncells + 127) / 128, c->ph.np);
         PLAUNCH(c, "s_f_scatter_cached", stencil_bytes<T>(c, 2), s_f_scatter_cached<T>, sgrid, 128, 0, c->g, c->ph,
                 c->ps.x, c->ps.v, c->ps.omega, c->cells, c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS),
@@ -1175,6 +1212,8 @@ int download_particles(spm_ctx *c, double *rec) {
     return SPM_OK;
 }
 
+#include "spm_rigid.inc"
+
 void avs_release(spm_ctx *c);
 
 // Electrolyte run constants from the parameters (Init_rho_ion,
@@ -1248,6 +1287,8 @@ void destroy_ctx(spm_ctx *c) {
     dev_free(c->el.partial);
     dev_free(c->slip);
     dev_free(c->slip_eps);
+    dev_free(c->rg_ibuf);
+    dev_free(c->rg_dbuf);
     if (c->side) cudaStreamDestroy(c->side);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
@@ -1371,6 +1412,10 @@ int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *
     }
     cudaMemcpy(c->cells, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemset(c->pbuf, 0, (size_t)np * kPWords * sizeof(double));
+    if (c->rigid() && (rc = rigid_alloc(c)) != SPM_OK) {
+        destroy_ctx(c);
+        return rc;
+    }
     unsigned int mt[625];
     mt_init(p.mt_seed, mt);
     cudaMemcpy(c->mt, mt, sizeof(mt), cudaMemcpyHostToDevice);
@@ -1507,7 +1552,13 @@ int spm_destroy(spm_ctx *c) {
 int spm_initialize(spm_ctx *c, const double *particles_host) {
     if (!c) return fail(SPM_ERR_ARG, "null context");
     if (c->ph.np > 0 && !particles_host) return fail(SPM_ERR_ARG, "particle records required");
-    int rc = upload_particles(c, particles_host, true);
+    int rc;
+    if (c->rigid()) {  // bodies set up from the beads as given (Init_Particle's rigid branch)
+        std::vector<double> rec(particles_host, particles_host + (size_t)c->ph.np * SPM_PARTICLE_WORDS);
+        rc = c->fp64() ? rigid_setup<double>(c, rec) : rigid_setup<float>(c, rec);
+    } else {
+        rc = upload_particles(c, particles_host, true);
+    }
     if (rc != SPM_OK) return rc;
     le_reset(c->le);
     rc = c->fp64() ? initialize_impl<double>(c) : initialize_impl<float>(c);
@@ -1567,6 +1618,19 @@ int spm_get_particles(spm_ctx *c, double *rec) {
     int rc = spm_synchronize(c);
     if (rc != SPM_OK) return rc;
     return download_particles(c, rec);
+}
+
+int spm_rigid_count(spm_ctx *c, int *n) {
+    if (!c || !n) return fail(SPM_ERR_ARG, "bad argument");
+    *n = c->rigid() ? c->rg.nb : 0;
+    return SPM_OK;
+}
+
+int spm_get_rigid(spm_ctx *c, double *bodies) {
+    if (!c || !c->rigid() || (!bodies && c->rg.nb > 0)) return fail(SPM_ERR_ARG, "bad argument (no rigid bodies)");
+    int rc = spm_synchronize(c);
+    if (rc != SPM_OK) return rc;
+    return rigid_download(c, bodies);
 }
 
 int spm_set_particles(spm_ctx *c, const double *rec) {

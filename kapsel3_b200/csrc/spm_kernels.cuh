@@ -1148,12 +1148,16 @@ __device__ __forceinline__ int lj_next_in_cell(const Phys &ph, int c, int last, 
 // x_j); lj_stress[n] receives particle n's share of sum f_x r_y over the
 // pairs where it is the higher index.  Pairs of two obstacles exert no force
 // (obstacle_chain, interaction.h:29-35; Janus particles are one species here).
+// Beads of rigid bodies (rid != null): pairs within one body are skipped
+// (rigid_chain, interaction.h:18-24), and f_lo[n] receives the force on n
+// from the pairs where n is the lower index (the bodies' torques need it).
 __global__ void p_forces_cells(Phys ph, PState s, const int *__restrict__ count, const int *__restrict__ cell_of,
-                               const int *__restrict__ bins) {
+                               const int *__restrict__ bins, const int *__restrict__ rid, double *__restrict__ f_lo) {
     const int lane = threadIdx.x & 31;
     const int n    = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (n >= ph.np) return;
     double f[3]   = {0.0, 0.0, 0.0};
+    double fl[3]  = {0.0, 0.0, 0.0};
     double stress = 0.0;
     if (ph.lj_on && ph.janus_prop != 3 && lane < 27) {
         const int mc[3] = {cell_of[n] / (ph.lc[1] * ph.lc[2]), (cell_of[n] / ph.lc[2]) % ph.lc[1],
@@ -1169,7 +1173,7 @@ __global__ void p_forces_cells(Phys ph, PState s, const int *__restrict__ count,
         const int cell = (cl[0] * ph.lc[1] + cl[1]) * ph.lc[2] + cl[2];
         for (int m = lj_next_in_cell(ph, cell, -1, count, cell_of, bins); m < ph.np;
              m     = lj_next_in_cell(ph, cell, m, count, cell_of, bins)) {
-            if (m == n) continue;
+            if (m == n || (rid && rid[m] == rid[n])) continue;
             const int    hi = n > m ? n : m, lo = n > m ? m : n;
             double       rij[3];
             const double rr = min_image(ph, s.x + 3 * hi, s.x + 3 * lo, rij);
@@ -1177,7 +1181,11 @@ __global__ void p_forces_cells(Phys ph, PState s, const int *__restrict__ count,
             const double sg    = (n == hi) ? 1.0 : -1.0;
             const double dmy_r = lj_f(rr, ph);
             for (int d = 0; d < 3; d++) f[d] += -dmy_r * (sg * rij[d]);
-            if (n == hi) stress += (-dmy_r * rij[0]) * rij[1];
+            if (n == hi) {
+                stress += (-dmy_r * rij[0]) * rij[1];
+            } else {
+                for (int d = 0; d < 3; d++) fl[d] += -dmy_r * (sg * rij[d]);
+            }
         }
     }
 #pragma unroll
@@ -1186,10 +1194,17 @@ __global__ void p_forces_cells(Phys ph, PState s, const int *__restrict__ count,
         f[1] += __shfl_xor_sync(0xffffffffu, f[1], o);
         f[2] += __shfl_xor_sync(0xffffffffu, f[2], o);
         stress += __shfl_xor_sync(0xffffffffu, stress, o);
+        if (f_lo) {
+            fl[0] += __shfl_xor_sync(0xffffffffu, fl[0], o);
+            fl[1] += __shfl_xor_sync(0xffffffffu, fl[1], o);
+            fl[2] += __shfl_xor_sync(0xffffffffu, fl[2], o);
+        }
     }
     if (lane == 0) {
         for (int d = 0; d < 3; d++) s.fr[3 * n + d] += f[d] + ph.body_force[d];
         s.lj_stress[n] = stress;
+        if (f_lo)
+            for (int d = 0; d < 3; d++) f_lo[3 * n + d] = fl[d];
     }
 }
 
@@ -1342,7 +1357,10 @@ __device__ __forceinline__ unsigned int mt_twist_word(const unsigned int *mt, in
     if (y & 1u) v ^= 0x9908b0dfu;
     return v;
 }
-__global__ void __launch_bounds__(kThermoThreads) p_thermostat(Phys ph, PState s, unsigned int *mt_g) {
+// noise != null (rigid bodies): the six normals of particle n go to
+// noise[6 n ..], nothing is applied (r_thermostat applies them per body).
+__global__ void __launch_bounds__(kThermoThreads) p_thermostat(Phys ph, PState s, unsigned int *mt_g,
+                                                               double *noise) {
     __shared__ unsigned int mt[624];
     __shared__ double       uni[624 + 1];  // the carried uniform, then this round's outputs
     __shared__ int          wsum[kThermoThreads / 32];
@@ -1407,7 +1425,9 @@ __global__ void __launch_bounds__(kThermoThreads) p_thermostat(Phys ph, PState s
             const int    n = before / 3, k = before % 3;
             for (int e = 0; e < 2; e++) {
                 const int q = 2 * k + e;  // normal index of particle n
-                if (q < 3)
+                if (noise)
+                    noise[6 * n + q] = g[e];
+                else if (q < 3)
                     s.v[3 * n + q] += g[e] * ph.noise_v * ph.imass_s[spec_of(ph, n)];
                 else if (ph.rotation)
                     s.omega[3 * n + q - 3] += g[e] * ph.noise_o * ph.imoi_s[spec_of(ph, n)];

@@ -23,25 +23,26 @@
 namespace spm {
 
 // The even/odd split of a length-2M real transform packed as M complex
-// values: X[k] from Z[k], Z[M-k] (forward) and Z'[k] from X[k], X[M-k]
-// (inverse, scaled by c).  w = e^{-2 pi i k / (2M)}.
+// values, w = e^{-2 pi i k / (2M)}:
+//   forward  X[k] = E + w O,  E = (Z[k] + conj Z[M-k]) / 2,
+//            O = -i (Z[k] - conj Z[M-k]) / 2; hw = w / 2 is passed;
+//   inverse  Z'[k] = c (X[k] + conj X[M-k]) + i c (X[k] - conj X[M-k]) conj(w),
+//            the output scaled by c; cw = c w is passed.
+// Folding the factors 1/2 and c into the twiddle leaves ten floating-point
+// operations per value.
 template <typename T>
-__device__ __forceinline__ cplx<T> r2c_split(const cplx<T> &zk, const cplx<T> &zmk, const cplx<T> &w) {
-    const T er  = (T)0.5 * (zk.re + zmk.re);
-    const T ei  = (T)0.5 * (zk.im - zmk.im);
-    const T orr = (T)0.5 * (zk.im + zmk.im);
-    const T oi  = (T)-0.5 * (zk.re - zmk.re);
-    return cplx<T>{er + (w.re * orr - w.im * oi), ei + (w.re * oi + w.im * orr)};
+__device__ __forceinline__ cplx<T> r2c_split(const cplx<T> &zk, const cplx<T> &zmk, const cplx<T> &hw) {
+    const T sr = zk.re + zmk.re, di = zk.im - zmk.im;
+    const T si = zk.im + zmk.im, dr = zk.re - zmk.re;
+    return cplx<T>{(T)0.5 * sr + (hw.re * si + hw.im * dr), (T)0.5 * di + (hw.im * si - hw.re * dr)};
 }
 template <typename T>
-__device__ __forceinline__ cplx<T> c2r_split(const cplx<T> &xk, const cplx<T> &xmk, const cplx<T> &w, T c) {
-    const T er  = c * (xk.re + xmk.re);
-    const T ei  = c * (xk.im - xmk.im);
-    const T dr  = c * (xk.re - xmk.re);
-    const T di  = c * (xk.im + xmk.im);
-    const T orr = dr * w.re + di * w.im;
-    const T oi  = di * w.re - dr * w.im;
-    return cplx<T>{er - oi, ei + orr};
+__device__ __forceinline__ cplx<T> c2r_split(const cplx<T> &xk, const cplx<T> &xmk, const cplx<T> &cw, T c) {
+    const T sr = xk.re + xmk.re, di = xk.im - xmk.im;
+    const T dr = xk.re - xmk.re, si = xk.im + xmk.im;
+    const T orr = dr * cw.re + si * cw.im;
+    const T oi  = si * cw.re - dr * cw.im;
+    return cplx<T>{c * sr - oi, c * di + orr};
 }
 
 template <int M>
@@ -188,8 +189,8 @@ __device__ __forceinline__ void zr_c2r(int t, const int (&a)[2], const cplx<T> (
         for (int j = 0; j < J; j++) {
             cplx<T> xk = kv[r][j], xm = zr_mirror<T, J>(kv, xn, t0, r, j);
             if (r == 0 && j == 0 && t0) xk.im = xm.im = 0;
-            cplx<T> w = wb[r];
-            twiddle_mul<T, 2 * J, -1>(w, j);  // e^{-2 pi i (a + Q j) / (2M)}
+            cplx<T> w = cplx<T>{scale * wb[r].re, scale * wb[r].im};
+            twiddle_mul<T, 2 * J, -1>(w, j);  // c e^{-2 pi i (a + Q j) / (2M)}
             zp[r][j] = c2r_split<T>(xk, xm, w, scale);
         }
     // step 1: J-point DFTs over j, twiddle e^{+2 pi i a b / M}, to shared
@@ -252,8 +253,8 @@ __device__ __forceinline__ void zr_r2c(int t, const int (&a)[2], const cplx<T> (
 #pragma unroll
         for (int j = 0; j < J; j++) {
             const cplx<T> zm = zr_mirror<T, J>(z, z0, t0, r, j);
-            cplx<T>       w  = wb[r];
-            twiddle_mul<T, 2 * J, -1>(w, j);
+            cplx<T>       w  = cplx<T>{(T)0.5 * wb[r].re, (T)0.5 * wb[r].im};
+            twiddle_mul<T, 2 * J, -1>(w, j);  // e^{-2 pi i (a + Q j) / (2M)} / 2
             kv[r][j] = r2c_split<T>(z[r][j], zm, w);
         }
     xn = cplx<T>{z0.re - z0.im, (T)0};  // X[M] (used by t = 0 only)

@@ -19,7 +19,7 @@ from typing import Dict, Optional, Tuple
 import numpy as np
 
 from . import _native as N
-from .udf import EQ_EL, EQ_LE, EQ_NS, EQ_SNS, SPMConfig
+from .udf import EQ_EL, EQ_LE, EQ_NS, EQ_SNS, SPMConfig, read_udf_keys
 
 RECORD = [("x", 3), ("x_nopbc", 3), ("v", 3), ("v_old", 3), ("omega", 3), ("omega_old", 3),
           ("q", 4), ("q_old", 4), ("f_hydro", 3), ("f_hydro_previous", 3),
@@ -95,6 +95,25 @@ def params_from_config(cfg: SPMConfig, precision: int = N.SPM_PREC_FP64,
         p.n_species = len(cfg.species)
         for i, (cnt, mr, q) in enumerate(cfg.species):
             p.species_count[i], p.species_mass_ratio[i], p.species_surface_charge[i] = int(cnt), float(mr), float(q)
+    if cfg.rigid:
+        p.rigid = 1
+        if len(cfg.rigid) > 1:
+            p.n_species = len(cfg.rigid)
+        for i, (beads, count, mr, motion, vel, om) in enumerate(cfg.rigid):
+            p.rigid_beads[i], p.rigid_count[i] = int(beads), int(count)
+            if len(cfg.rigid) > 1:
+                p.species_count[i], p.species_mass_ratio[i] = int(beads) * int(count), float(mr)
+            for d in range(6):
+                p.rigid_free[i][d] = 1 if motion == "free" else 0
+            for d in range(3):
+                p.rigid_velocity[i][d], p.rigid_omega[i][d] = float(vel[d]), float(om[d])
+        p.mass_ratio = float(cfg.rigid[0][2])
+        for d in range(3):
+            p.rigid_gravity[d] = float(cfg.rigid_gravity[d])
+        for sid, vflags, wflags in cfg.rigid_dof:
+            for d in range(3):
+                p.rigid_free[sid][d] = 1 if vflags[d] else 0
+                p.rigid_free[sid][3 + d] = 1 if wflags[d] else 0
     return p
 
 
@@ -113,13 +132,16 @@ def config_from_udf(path: str) -> Tuple[SPMConfig, Dict[str, np.ndarray]]:
     """Run parameters and initial particles of a UDF input file, as
     Gourmet_file_io and Init_Particle read them (user_specify or
     uniform_random placement; user_specify, random or space_align
-    orientation)."""
+    orientation).  A path ending in .keys is read as a key file
+    ("udf.path = value" lines, kapsel3_b200.udf.write_udf_keys)."""
     L = N.lib()
     p = N.SpmParams()
-    N.check(L.spm_params_from_udf(path.encode(), C.byref(p), None, 0), "spm_params_from_udf")
+    keys = path.endswith(".keys")
+    parse = L.spm_params_from_udf_keys if keys else L.spm_params_from_udf
+    N.check(parse(path.encode(), C.byref(p), None, 0), "spm_params_from_udf")
     rec = np.zeros((max(p.n_particles, 1), N.SPM_PARTICLE_WORDS))
-    N.check(L.spm_params_from_udf(path.encode(), C.byref(p), N.dptr(rec), p.n_particles), "spm_params_from_udf")
-    kv = read_udf(path)
+    N.check(parse(path.encode(), C.byref(p), N.dptr(rec), p.n_particles), "spm_params_from_udf")
+    kv = read_udf_keys(path) if keys else read_udf(path)
     cfg = SPMConfig(
         npx=p.npx, npy=p.npy, npz=p.npz, dx=p.dx, rho=p.rho, eta=p.eta, kbt=p.kbt,
         alpha_v=p.alpha_v, alpha_o=p.alpha_o,
@@ -141,7 +163,17 @@ def config_from_udf(path: str) -> Tuple[SPMConfig, Dict[str, np.ndarray]]:
         slip_mode=p.slip_mode, rotlet_c1=p.rotlet_c1, rotlet_c2=p.rotlet_c2, slip_tol=p.slip_tol,
         slip_iter=p.slip_iter,
         species=tuple((p.species_count[i], p.species_mass_ratio[i], p.species_surface_charge[i])
-                      for i in range(p.n_species)) if p.n_species > 1 else ())
+                      for i in range(p.n_species)) if p.n_species > 1 and not p.rigid else ())
+    if p.rigid:  # Rigid_spec[] and switch.free_rigid as the library parsed them
+        nsp = max(p.n_species, 1)
+        mr = [p.species_mass_ratio[s] if nsp > 1 else p.mass_ratio for s in range(nsp)]
+        cfg.rigid = tuple((p.rigid_beads[s], p.rigid_count[s], mr[s],
+                           kv[f"object_type.rigid.Rigid_spec[{s}].Rigid_motion"],
+                           tuple(p.rigid_velocity[s]), tuple(p.rigid_omega[s])) for s in range(nsp))
+        if kv.get("switch.free_rigid.type") == "YES":
+            cfg.rigid_dof = tuple((s, tuple(bool(p.rigid_free[s][d]) for d in range(3)),
+                                   tuple(bool(p.rigid_free[s][3 + d]) for d in range(3))) for s in range(nsp))
+        cfg.rigid_gravity = tuple(p.rigid_gravity)
     return cfg, unpack_particles(rec[:p.n_particles])
 
 
@@ -214,6 +246,17 @@ class SPMRun:
 
     def synchronize(self):
         N.check(self.L.spm_synchronize(self.h), "spm_synchronize")
+
+    def rigid_bodies(self) -> Dict[str, np.ndarray]:
+        """The rigid bodies' state: xG, xG_nopbc, vG, wG ([nb, 3]), mass [nb]
+        and the body-frame principal moments Ibody [nb, 3]."""
+        n = C.c_int()
+        N.check(self.L.spm_rigid_count(self.h, C.byref(n)), "spm_rigid_count")
+        out = np.zeros((max(n.value, 1), N.SPM_RIGID_WORDS))
+        N.check(self.L.spm_get_rigid(self.h, N.dptr(out)), "spm_get_rigid")
+        out = out[:n.value]
+        return dict(xg=out[:, 0:3], xg_nopbc=out[:, 3:6], vg=out[:, 6:9], wg=out[:, 9:12], mass=out[:, 12],
+                    ibody=out[:, 13:16])
 
     def time_steps(self, n: int) -> float:
         ms = C.c_float()

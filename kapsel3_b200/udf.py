@@ -87,6 +87,14 @@ class SPMConfig:
     # counts adding up to n_particles (species 0 first); empty: one species (n_particles, mass_ratio,
     # surface_charge)
     species: tuple = ()
+    # Rigid bodies (object_type.type = rigid, Rigid_spec[0..]): one entry per rigid species,
+    # (Beads_number, Chain_number, MASS_RATIO, Rigid_motion "free"/"fix", Rigid_velocity (3),
+    # Rigid_omega (3)); n_particles is then the sum of Beads_number * Chain_number.  rigid_dof
+    # overrides the degrees of freedom (switch.free_rigid): ((spec_id, (vx, vy, vz), (wx, wy, wz)), ...)
+    # with booleans.
+    rigid: tuple = ()
+    rigid_dof: tuple = ()
+    rigid_gravity: tuple = (0.0, 0.0, 0.0)  # gravity.G placed on the axis of gravity.G_direction
 
     # ------------------------------------------------------------------
     @property
@@ -170,6 +178,59 @@ def make_particles(cfg: SPMConfig, seed: int, v_sd: float = 0.0,
     return dict(x=x, v=v, q=q, omega=omega)
 
 
+def make_rigid_bodies(cfg: SPMConfig, seed: int, spacing_factor: float = 1.2, min_dist_factor: float = 1.05,
+                      straddle: bool = False, max_tries: int = 20000) -> Dict[str, np.ndarray]:
+    """Seeded bead positions of cfg.rigid's bodies, species after species and
+    body after body (the order of Rigid_spec[] and Particle_RigidID): each
+    body is a random walk of beads spacing_factor * A apart whose turns keep
+    its inertia tensor free of equal eigenvalues.  The coordinates are not
+    wrapped into the box (a body may reach over its edge, and with `straddle`
+    the first body does), as user_specify inputs give them.  Beads of
+    different bodies stay min_dist_factor * SIGMA apart (periodic images
+    included).  Velocities and orientations are zero and the identity: the
+    bodies' motion comes from Rigid_velocity / Rigid_omega."""
+    rng = np.random.default_rng(seed)
+    d = cfg.derived()
+    L = np.array([d["LX"], d["LY"], d["LZ"]])
+    step = spacing_factor * cfg.a
+    rmin = min_dist_factor * d["SIGMA"]
+    bodies = []
+    tries = 0
+    for beads, count, *_ in cfg.rigid:
+        for _ in range(int(count)):
+            while True:
+                tries += 1
+                if tries > max_tries:
+                    raise ValueError(f"cannot place the rigid bodies in {cfg.shape}")
+                pos = [rng.random(3) * L]
+                if straddle and not bodies:
+                    pos = [L * np.array([0.98, 0.5, 0.5])]
+                u = rng.normal(size=3)
+                u /= np.linalg.norm(u)
+                for k in range(1, int(beads)):
+                    # turn by 50-80 degrees about a random axis from the previous direction
+                    w = np.cross(u, rng.normal(size=3))
+                    w /= np.linalg.norm(w)
+                    t = np.deg2rad(rng.uniform(50.0, 80.0))
+                    u = np.cos(t) * u + np.sin(t) * w
+                    pos.append(pos[-1] + step * u)
+                body = np.array(pos)
+                ok = True
+                for other in bodies:
+                    dd = body[:, None, :] - other[None, :, :]
+                    dd -= np.rint(dd / L) * L
+                    if np.sqrt((dd ** 2).sum(-1)).min() <= rmin:
+                        ok = False
+                        break
+                if ok:
+                    bodies.append(body)
+                    break
+    x = np.concatenate(bodies) if bodies else np.zeros((0, 3))
+    n = len(x)
+    return dict(x=x, v=np.zeros((n, 3)), q=np.tile(np.array([1.0, 0.0, 0.0, 0.0]), (n, 1)),
+                omega=np.zeros((n, 3)))
+
+
 def _fmt(v) -> str:
     if isinstance(v, bool):
         return "ON" if v else "OFF"
@@ -227,7 +288,25 @@ def udf_keys(cfg: SPMConfig, particles: Dict[str, np.ndarray],
         k[f"{base}.External_field.{ft}.Shear_rate"] = _fmt(float(cfg.shear_rate))
         if cfg.shear_ac:
             k[f"{base}.External_field.AC.Frequency"] = _fmt(float(cfg.shear_frequency))
-    k["object_type.type"] = "spherical_particle"
+    k["object_type.type"] = "rigid" if cfg.rigid else "spherical_particle"
+    for i, (beads, count, mr, motion, vel, om) in enumerate(cfg.rigid):
+        ri = f"object_type.rigid.Rigid_spec[{i}]"
+        k[f"{ri}.Beads_number"] = str(int(beads))
+        k[f"{ri}.Chain_number"] = str(int(count))
+        k[f"{ri}.MASS_RATIO"] = _fmt(float(mr))
+        k[f"{ri}.Surface_charge"] = _fmt(0.0)
+        k[f"{ri}.Rigid_motion"] = motion
+        for c, v, w in zip("xyz", vel, om):
+            k[f"{ri}.Rigid_velocity.{c}"] = _fmt(float(v))
+            k[f"{ri}.Rigid_omega.{c}"] = _fmt(float(w))
+    if cfg.rigid:
+        k["switch.free_rigid.type"] = "YES" if cfg.rigid_dof else "NO"
+        for i, (sid, vflags, wflags) in enumerate(cfg.rigid_dof):
+            di = f"switch.free_rigid.YES.DOF[{i}]"
+            k[f"{di}.spec_id"] = str(int(sid))
+            for c, fv, fw in zip("xyz", vflags, wflags):
+                k[f"{di}.vel.{c}"] = "YES" if fv else "NO"
+                k[f"{di}.omega.{c}"] = "YES" if fw else "NO"
     ps = "object_type.spherical_particle.Particle_spec[0]"
     spec = cfg.species if len(cfg.species) > 1 else ((cfg.n_particles, cfg.mass_ratio, cfg.surface_charge),)
     for i, (cnt, mr, q) in enumerate(spec):
@@ -257,6 +336,10 @@ def udf_keys(cfg: SPMConfig, particles: Dict[str, np.ndarray],
     has_bf = any(f != 0.0 for f in cfg.body_force)
     k["gravity.G"] = "1.0" if has_bf else "0.0"
     k["gravity.G_direction"] = "-X"
+    if cfg.rigid and any(g != 0.0 for g in cfg.rigid_gravity):  # real gravity on the bodies
+        d = next(i for i, g in enumerate(cfg.rigid_gravity) if g != 0.0)
+        k["gravity.G"] = _fmt(float(cfg.rigid_gravity[d]))
+        k["gravity.G_direction"] = "-" + "XYZ"[d]
     k["EPSILON"] = _fmt(float(cfg.epsilon))
     k["LJ_powers"] = cfg.lj_powers
     k["mesh.NPX"], k["mesh.NPY"], k["mesh.NPZ"] = str(cfg.npx), str(cfg.npy), str(cfg.npz)

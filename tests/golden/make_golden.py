@@ -25,7 +25,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from kapsel3_b200.udf import EQ_LE, SPMConfig, make_particles, write_udf_keys  # noqa: E402
+from kapsel3_b200.udf import EQ_LE, SPMConfig, make_particles, make_rigid_bodies, write_udf_keys  # noqa: E402
+from kapsel3_b200.spm import config_from_udf, read_udf  # noqa: E402
 from oracle import ref_runner  # noqa: E402
 
 CASES = {
@@ -62,6 +63,38 @@ CASES = {
         cfg=dict(npx=5, npy=5, npz=5, n_particles=3, a=3.0, a_xi=2.0, dt=0.05, equation=EQ_LE, shear_rate=0.6,
                  num_snap=40),
         init=dict(seed=17, v_sd=1e-3, random_orientation=False), field_steps=(40,)),
+    # rigid bodies (object_type rigid): two 4-bead bodies moving with a fixed
+    # velocity and angular velocity (Rigid_motion fix), the first one across
+    # the x edge of the box
+    "rigid_32_fixed_motion": dict(
+        cfg=dict(npx=5, npy=5, npz=5, n_particles=8, a=3.0, a_xi=2.0, dt=0.05, num_snap=40,
+                 rigid=((4, 2, 1.0, "fix", (2e-3, -1e-3, 0.0), (0.0, 3e-3, 1e-3)),)),
+        init=dict(seed=21, straddle=True), field_steps=(40,)),
+    # free 3-bead bodies, MASS_RATIO 1.5, under gravity along -y
+    "rigid_32_free_gravity": dict(
+        cfg=dict(npx=5, npy=5, npz=5, n_particles=6, a=3.0, a_xi=2.0, dt=0.05, num_snap=60,
+                 rigid=((3, 2, 1.5, "free", (0.0, 0.0, 0.0), (0.0, 0.0, 0.0)),), rigid_gravity=(0.0, 1e-3, 0.0)),
+        init=dict(seed=22), field_steps=(60,)),
+    # two species, non-cubic grid: free 3-bead bodies with two degrees of
+    # freedom switched off (switch.free_rigid) and a fixed 4-bead body of
+    # MASS_RATIO 2, thermostat on
+    "rigid_species_dof_thermostat": dict(
+        cfg=dict(npx=5, npy=5, npz=6, n_particles=10, a=3.0, a_xi=2.0, dt=0.05, kbt=1e-5, num_snap=40,
+                 rigid=((3, 2, 1.0, "free", (0.0, 0.0, 0.0), (0.0, 0.0, 0.0)),
+                        (4, 1, 2.0, "fix", (1e-3, 0.0, 0.0), (0.0, 0.0, 2e-3))),
+                 rigid_dof=((0, (True, True, False), (False, True, True)),)),
+        init=dict(seed=23), field_steps=(40,)),
+    # the reference's own example inputs, shortened to a few dozen steps with
+    # every step kept: Examples/12/a2_N65_Rer02.udf (65 one-bead bodies of
+    # MASS_RATIO 1.5 spinning at a fixed body-frame rate, gravity along -z,
+    # the x rotation switched off by switch.free_rigid; its flat wall and
+    # Quincke switches, outside the step, turned off) and Examples/10/
+    # input_rigid_free1.udf (a free 65-bead body sedimenting along -y on a
+    # 64 x 128 x 64 grid)
+    "example12_65_spinning_bodies": dict(example="Examples/12/a2_N65_Rer02.udf", num_snap=30, field_steps=(30,),
+                                         overrides={"switch.wall.type": "NONE", "switch.quincke.type": "OFF"}),
+    "example10_rigid_free_sedimenting": dict(example="Examples/10/input_rigid_free1.udf", num_snap=20,
+                                             field_steps=(20,), zeta=False),
 }
 
 
@@ -78,9 +111,23 @@ def retained_modes(cfg: SPMConfig, zeta: np.ndarray) -> np.ndarray:
 
 
 def make_case(name, spec):
-    cfg = SPMConfig(**spec["cfg"])
-    init = dict(spec["init"])
-    parts = make_particles(cfg, **init)
+    if "example" in spec:
+        tree = ref_runner.reference_tree()
+        if tree is None:
+            raise SystemExit("the reference sources are needed for " + spec["example"])
+        kv = read_udf(os.path.join(tree, spec["example"]))
+        kv.update(spec.get("overrides", {}))
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "example.keys")
+            with open(path, "w") as f:
+                f.writelines(f"{k} = {v}\n" for k, v in kv.items())
+            cfg, parts = config_from_udf(path)
+        cfg.gts, cfg.num_snap = 1, spec["num_snap"]
+        init = dict(example=spec["example"], overrides=spec.get("overrides", {}))
+    else:
+        cfg = SPMConfig(**spec["cfg"])
+        init = dict(spec["init"])
+        parts = make_rigid_bodies(cfg, **init) if cfg.rigid else make_particles(cfg, **init)
     if "tweak" in spec:
         t = spec["tweak"]
         parts["x"][t["index"]] = t["x"]

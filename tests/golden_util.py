@@ -16,14 +16,23 @@ def fixture_names():
     return sorted(os.path.splitext(os.path.basename(p))[0] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
 
 
+def _config(name):
+    return json.loads(str(np.load(os.path.join(GOLDEN, name + ".npz"))["config_json"]))
+
+
 def small_fixture_names(max_points=64 ** 3):
-    """Fixtures on grids the numpy oracle steps in well under a second."""
+    """Fixtures of spherical particles on grids the numpy oracle steps in
+    well under a second (the oracle has no rigid bodies)."""
     out = []
     for n in fixture_names():
-        c = json.loads(str(np.load(os.path.join(GOLDEN, n + ".npz"))["config_json"]))
-        if (1 << c["npx"]) * (1 << c["npy"]) * (1 << c["npz"]) <= max_points:
+        c = _config(n)
+        if (1 << c["npx"]) * (1 << c["npy"]) * (1 << c["npz"]) <= max_points and not c.get("rigid"):
             out.append(n)
     return out
+
+
+def rigid_fixture_names():
+    return [n for n in fixture_names() if _config(n).get("rigid")]
 
 
 def load(name):

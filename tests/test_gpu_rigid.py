@@ -1,0 +1,121 @@
+"""Rigid bodies on the GPU beyond the per-step fixture comparison (every
+rigid fixture is also stepped by tests/test_gpu_golden.py):
+
+* the body state a run reports (spm_get_rigid) against its beads: every
+  bead carries its body's angular velocity, the beads keep their distances,
+  and a body's centre takes the Adams-Bashforth step of its velocities;
+* the FP32-mixed field path against FP64 on a rigid fixture;
+* checkpoint / restart of a rigid run (the bodies' state, their previous
+  forces and the MT19937 state of the rigid thermostat);
+* a fixed body keeps the velocity it was given and the angular velocity
+  its body-frame Rigid_omega had in space at the start (Rigid_motion fix;
+  init_set_vGs, rigid.h:248-251)."""
+import os
+
+import numpy as np
+import pytest
+
+from kapsel3_b200 import _native as N
+from kapsel3_b200.spm import SPMRun
+from tests.golden_util import load, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _first(cfg):
+    first = [0]
+    for beads, count, *_ in cfg.rigid:
+        for _ in range(int(count)):
+            first.append(first[-1] + int(beads))
+    return first
+
+
+def _rotate(q, v):
+    """q v q* for a unit quaternion q = (s, x, y, z)."""
+    s, u = q[0], np.asarray(q[1:])
+    return v + 2.0 * s * np.cross(u, v) + 2.0 * np.cross(u, np.cross(u, v))
+
+
+@pytest.mark.parametrize("name", ["rigid_species_dof_thermostat", "example10_rigid_free_sedimenting"])
+def test_body_state_matches_its_beads(gpu, name):
+    cfg, parts, z = load(name)
+    first = _first(cfg)
+    with SPMRun(cfg) as run:
+        run.initialize(parts)
+        b0 = run.rigid_bodies()
+        p0 = run.particles()
+        run.step(8)
+        b8 = run.rigid_bodies()
+        run.step(1)
+        b9 = run.rigid_bodies()
+        run.step(1)
+        b1 = run.rigid_bodies()
+        p1 = run.particles()
+    nb = len(first) - 1
+    assert b1["xg"].shape == (nb, 3) and b1["mass"].shape == (nb,)
+    for b in range(nb):
+        sl = slice(first[b], first[b + 1])
+        if cfg.kbt == 0.0:  # the rigid thermostat leaves the beads' angular velocities behind (fluct.cxx:40-95)
+            assert (p1["omega"][sl] == b1["wg"][b]).all()
+        d0 = np.linalg.norm(p0["x_nopbc"][sl, None] - p0["x_nopbc"][None, sl], axis=-1)
+        d1 = np.linalg.norm(p1["x_nopbc"][sl, None] - p1["x_nopbc"][None, sl], axis=-1)
+        assert np.abs(d1 - d0).max() < 1e-10
+        # the centre without the wrap takes the second-order Adams-Bashforth step (solver_Rigid_Position)
+        moved = b1["xg_nopbc"][b] - b9["xg_nopbc"][b]
+        want = 0.5 * cfg.dt * (3.0 * b9["vg"][b] - b8["vg"][b])
+        assert np.abs(moved - want).max() <= 1e-9 * np.abs(want).max() + 1e-15
+        assert b1["mass"][b] == b0["mass"][b] > 0
+
+
+def test_fp32_mixed_rigid_follows_fp64(gpu):
+    cfg, parts, z = load("rigid_32_free_gravity")
+    out = {}
+    for prec in (N.SPM_PREC_FP64, N.SPM_PREC_FP32_MIXED):
+        with SPMRun(cfg, precision=prec) as run:
+            run.initialize(parts)
+            run.step(60)
+            out[prec] = run.particles()
+    for k in ("x", "v", "omega"):
+        assert rel(out[N.SPM_PREC_FP32_MIXED][k], out[N.SPM_PREC_FP64][k]) < 1e-4, k
+    # and FP64 is the reference's trajectory
+    assert rel(out[N.SPM_PREC_FP64]["v"], z["traj_v"][60]) < 1e-10
+
+
+def test_rigid_checkpoint_continues_like_the_original(gpu, tmp_path):
+    cfg, parts, z = load("rigid_species_dof_thermostat")
+    path = os.path.join(tmp_path, "rigid.ck")
+    with SPMRun(cfg) as a:
+        a.initialize(parts)
+        a.step(7)
+        a.save_state(path)
+        a.step(6)
+        pa, ba = a.particles(), a.rigid_bodies()
+    with SPMRun(cfg) as b:
+        b.load_state(path)
+        assert b.time()[0] == 7
+        b.step(6)
+        pb, bb = b.particles(), b.rigid_bodies()
+    for k in ("x", "v", "omega", "q"):
+        assert rel(pb[k], pa[k]) < 1e-12, k
+    for k in ("xg", "vg", "wg"):
+        assert rel(bb[k], ba[k]) < 1e-12, k
+    assert rel(pb["v"], z["traj_v"][13]) < 1e-10
+
+
+def test_fixed_body_keeps_its_motion(gpu):
+    cfg, parts, z = load("rigid_32_fixed_motion")
+    vel = np.array(cfg.rigid[0][4])
+    w_body = np.array(cfg.rigid[0][5])
+    first = _first(cfg)
+    with SPMRun(cfg) as run:
+        run.initialize(parts)
+        q0 = run.particles()["q"]
+        for _ in range(4):
+            run.step(10)
+            bodies = run.rigid_bodies()
+            for b in range(len(first) - 1):
+                assert np.abs(bodies["vg"][b] - vel).max() < 1e-15
+                # the body-frame angular velocity turned to space once, by the initial orientation
+                # (init_set_vGs, rigid.h:248-251), and kept there
+                w = _rotate(q0[first[b]], w_body)
+                assert np.abs(bodies["wg"][b] - w).max() < 1e-12 * np.linalg.norm(w_body)

@@ -28,6 +28,8 @@ from kapsel3_b200.udf import EQ_LE, SPMConfig, make_particles, udf_keys, write_u
 from oracle import ref_runner
 
 REFERENCE_TREE = ref_runner.reference_tree() or ""
+OUTSIDE_SWITCHES = (("switch.pin.type", "NO"), ("switch.wall.type", "NONE"), ("switch.quincke.type", "OFF"),
+                    ("switch.multipole.type", "OFF"))
 
 
 def load(path, n, keys=False):
@@ -252,7 +254,7 @@ def _reference_inputs():
 
 @pytest.mark.skipif(not _reference_inputs(), reason="reference tree not present")
 def test_every_reference_example_parses_and_in_scope_ones_load():
-    loaded = 0
+    loaded = loaded_rigid = 0
     for f in _reference_inputs():
         kv = read_udf(f)
         assert kv["constitutive_eq.type"] and kv["object_type.type"], f
@@ -263,16 +265,23 @@ def test_every_reference_example_parses_and_in_scope_ones_load():
         janus = spherical and kv[ps + "janus_propulsion"] != "OFF"
         eq_ok = kv["constitutive_eq.type"] in ("Navier_Stokes", "Shear_Navier_Stokes") or (
             kv["constitutive_eq.type"] in (EQ_LE, "Electrolyte") and not janus)
-        in_scope = eq_ok and spherical
+        rigid = kv["object_type.type"] == "rigid"
+        # pinning, flat walls, Quincke rotation and multipoles are refused when switched on
+        switches_off = all(kv.get(k, off) == off for k, off in OUTSIDE_SWITCHES)
+        in_scope = eq_ok and (spherical or rigid) and switches_off
         assert (rc == 0) == in_scope, (f, N.lib().spm_last_error())
         if rc == 0:
             loaded += 1
             assert (p.npx, p.npy, p.npz) == tuple(int(kv[f"mesh.NP{a}"]) for a in "XYZ")
+            if rigid:
+                loaded_rigid += 1
+                _check_rigid_keys(kv, p)
             counts = []
             while f"object_type.spherical_particle.Particle_spec[{len(counts)}].Particle_number" in kv:
                 counts.append(int(kv[f"object_type.spherical_particle.Particle_spec[{len(counts)}].Particle_number"]))
-            assert p.n_particles == sum(counts)
-            if len(counts) > 1:
+            if not rigid:
+                assert p.n_particles == sum(counts)
+            if len(counts) > 1 and not rigid:
                 assert p.n_species == len(counts) and list(p.species_count)[:len(counts)] == counts
                 for i in range(len(counts)):
                     sp = f"object_type.spherical_particle.Particle_spec[{i}]."
@@ -309,7 +318,39 @@ def test_every_reference_example_parses_and_in_scope_ones_load():
                 # DT = factor / (NU * KMAX2), KMAX2 from the 2/3-rule wavenumbers
                 k2 = sum((2 * math.pi / ((1 << n) * p.dx) * (((1 << n) + 2) // 3)) ** 2 for n in (p.npx, p.npy, p.npz))
                 assert p.dt == pytest.approx(float(kv["time_increment.auto.factor"]) / (p.eta / p.rho * k2), rel=1e-14)
-    assert loaded >= 4
+    assert loaded >= 4 and loaded_rigid >= 6
+
+
+def _check_rigid_keys(kv, p):
+    """Rigid_spec[] (input.cxx:1583-1700), switch.free_rigid (input.cxx:1961-2008) and the rigid gravity
+    (md_force.cxx:317-322) as the parser stores them."""
+    spec = "object_type.rigid.Rigid_spec[{}]."
+    nsp = 0
+    while spec.format(nsp) + "Beads_number" in kv:
+        nsp += 1
+    assert p.rigid == 1 and p.n_species == (nsp if nsp > 1 else 0)
+    total = 0
+    for s in range(nsp):
+        sp = spec.format(s)
+        beads, count = int(kv[sp + "Beads_number"]), int(kv[sp + "Chain_number"])
+        assert (p.rigid_beads[s], p.rigid_count[s]) == (beads, count)
+        total += beads * count
+        free = [kv[sp + "Rigid_motion"] == "free"] * 6
+        dof = 0
+        while kv.get("switch.free_rigid.type") == "YES" and f"switch.free_rigid.YES.DOF[{dof}].spec_id" in kv:
+            t = f"switch.free_rigid.YES.DOF[{dof}]."
+            if int(kv[t + "spec_id"]) == s:
+                free = [kv[t + k + "." + a] == "YES" for k in ("vel", "omega") for a in "xyz"]
+            dof += 1
+        assert [bool(x) for x in p.rigid_free[s]] == free
+        for d, a in enumerate("xyz"):
+            assert p.rigid_velocity[s][d] == float(kv[sp + "Rigid_velocity." + a])
+            assert p.rigid_omega[s][d] == float(kv[sp + "Rigid_omega." + a])
+    assert p.n_particles == total
+    g = [0.0] * 3
+    if float(kv["gravity.G"]) != 0.0:
+        g["XYZ".index(kv["gravity.G_direction"][1])] = float(kv["gravity.G"])
+    assert list(p.rigid_gravity) == g
 
 
 def test_janus_config_round_trip(tmp_path):
