@@ -49,6 +49,40 @@ __host__ __device__ __forceinline__ cplx<T> csub(cplx<T> a, cplx<T> b) {
     return {a.re - b.re, a.im - b.im};
 }
 
+// FP32 complex addition and subtraction as one paired instruction
+// (add/sub.rn.f32x2 of sm_100): each lane rounds as the scalar operation
+// does, with half the floating-point instructions in the transforms'
+// butterflies.  (A product feeding the sum is no longer contracted into a
+// fused multiply-add, so a result may differ from the scalar code's in the
+// last bit.)
+#if !defined(SPM_NO_F32X2)
+#define SPM_F32X2_ASM(op)                                                                         \
+    unsigned long long ua, ub, ur;                                                                \
+    asm("mov.b64 %0, {%1, %2};" : "=l"(ua) : "f"(a.re), "f"(a.im));                               \
+    asm("mov.b64 %0, {%1, %2};" : "=l"(ub) : "f"(b.re), "f"(b.im));                               \
+    asm(op " %0, %1, %2;" : "=l"(ur) : "l"(ua), "l"(ub));                                         \
+    cplx<float> r;                                                                                \
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.re), "=f"(r.im) : "l"(ur));                              \
+    return r;
+template <>
+__host__ __device__ __forceinline__ cplx<float> cadd<float>(cplx<float> a, cplx<float> b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    SPM_F32X2_ASM("add.rn.f32x2")
+#else
+    return {a.re + b.re, a.im + b.im};
+#endif
+}
+template <>
+__host__ __device__ __forceinline__ cplx<float> csub<float>(cplx<float> a, cplx<float> b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    SPM_F32X2_ASM("sub.rn.f32x2")
+#else
+    return {a.re - b.re, a.im - b.im};
+#endif
+}
+#undef SPM_F32X2_ASM
+#endif
+
 // Grid geometry shared by every kernel.
 struct Grid {
     int nx, ny, nz;
