@@ -428,6 +428,8 @@ def serving_leg(rank, world, n_runs, barrier, max_over_ranks):
                             "max": float(lat.max()) if len(lat) else None},
         "pool_step_device_ms": {"p50": st["pool_step_device_p50_ms"], "p99": st["pool_step_device_p99_ms"]},
         "max_resident_runs": st["max_active"], "graph_captures": st["graph_captures"],
+        "worker_phase_max_ms": {k: round(st[k + "_max_ms"], 3)
+                                for k in ("pool_create", "admit", "pool_destroy", "launch", "finish")},
         "peak_device_gb": st["peak_bytes"] / 1e9, "wall_s": res["wall_s"],
         "fp64_rel_velocity_error": errs,
         "latency_definition": "host time between consecutive step completions of a run (first: from admission)",

@@ -374,9 +374,10 @@ int spm_set_wait_limit(spm_ctx *ctx, double seconds);
  * nothing in flight (0 switches it off).  The steps taken meanwhile run
  * without graph replay.  No reference counterpart. */
 int spm_debug_skip_tma_loads(spm_ctx *ctx, int launches);
-/* Device blocks of up to 64 MB that destroyed contexts and pools freed are
- * kept for reuse (at most 2 GB per process), because cudaFree waits for the
- * whole device.  This returns them all to the driver; bytes = what was held. */
+/* Device memory of contexts and pools comes from a stream-ordered memory pool
+ * per device that keeps freed blocks mapped for reuse, because cudaFree waits
+ * for the whole device and unmaps (up to 0.8 s for a pool arena on B200).
+ * This returns the unused part to the driver; bytes = what was held unused. */
 int spm_release_cached_memory(size_t *bytes);
 
 /* ---- serving loop (no reference counterpart) -----------------------------
@@ -412,6 +413,13 @@ typedef struct spm_server_stats {
     double    busy_s;           /* first admission to last retirement */
     double    step_latency_p50_ms, step_latency_p99_ms, step_latency_max_ms;
     double    pool_step_device_p50_ms, pool_step_device_p99_ms;
+    /* longest single host phase of the worker (ms): creating a pool, admitting
+     * one run into a pool (arena growth and the run's initialisation included),
+     * destroying a pool, launching one pool step (graph capture included when
+     * the pool's membership changed), accounting one finished pool step
+     * (result downloads included).  While the worker is in one of these, no
+     * other pool's finished step is accounted, so they bound step latency. */
+    double    pool_create_max_ms, admit_max_ms, pool_destroy_max_ms, launch_max_ms, finish_max_ms;
 } spm_server_stats;
 
 int spm_server_config_default(spm_server_config *cfg);

@@ -106,6 +106,8 @@ class SpmServerStats(C.Structure):
         ("step_latency_p50_ms", C.c_double), ("step_latency_p99_ms", C.c_double),
         ("step_latency_max_ms", C.c_double),
         ("pool_step_device_p50_ms", C.c_double), ("pool_step_device_p99_ms", C.c_double),
+        ("pool_create_max_ms", C.c_double), ("admit_max_ms", C.c_double), ("pool_destroy_max_ms", C.c_double),
+        ("launch_max_ms", C.c_double), ("finish_max_ms", C.c_double),
     ]
 
 

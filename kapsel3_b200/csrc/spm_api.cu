@@ -46,30 +46,51 @@ namespace {
 // tests; spm_debug_fail_allocations).
 std::atomic<int> g_fail_allocs{0};
 
-// Small device blocks freed by contexts are kept for reuse instead of being
-// returned with cudaFree, which waits for the whole device: a serving loop
-// that retires and admits runs continuously would otherwise stall every
-// pool in flight at each retirement.  Blocks up to kCacheBlock bytes (sizes
-// rounded up to an eighth of their octave) are kept per device, at most
-// kCacheTotal bytes in all; a block is only cached after its owner's stream
-// was synchronised (destroy_ctx, pool release), so no work still uses it.
-constexpr size_t kCacheBlock = (size_t)64 << 20;
-constexpr size_t kCacheTotal = (size_t)2 << 30;
-struct BlockCache {
-    std::mutex                                           mu;
-    std::unordered_map<void *, std::pair<size_t, int>>   live;  // block -> (bytes, device)
-    std::multimap<std::pair<int, size_t>, void *>        idle;  // (device, bytes) -> block
-    size_t                                               idle_bytes = 0;
+// Device memory comes from a stream-ordered memory pool per device whose
+// release threshold is unbounded: a freed block goes back to the pool, still
+// mapped, and the next allocation reuses it.  cudaFree of a large block waits
+// for the whole device and then unmaps it; on B200 a pool arena's cudaFree
+// took up to 0.8 s inside a serving loop, a stall for every run in flight.
+// Allocations are ordered on the pool's own stream and completed before
+// dev_alloc returns, so any stream may use the block; a block is freed only
+// after its owner's stream was synchronised (destroy_ctx, pool growth), so no
+// work still uses it when the pool hands it out again.
+struct DevMemPool {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t  st   = nullptr;
 };
-BlockCache &block_cache() {
-    static BlockCache c;
-    return c;
+struct DevMem {
+    std::mutex                        mu;
+    std::unordered_map<int, DevMemPool> pools;  // device -> pool
+    std::unordered_map<void *, int>     live;   // block -> device
+};
+DevMem &dev_mem() {
+    static DevMem m;
+    return m;
 }
-size_t round_block(size_t b) {
-    if (b <= 4096) return 4096;
-    int lg = 63 - __builtin_clzll((unsigned long long)b);
-    const size_t granule = (size_t)1 << (lg - 3);
-    return (b + granule - 1) / granule * granule;
+// The pool of device `dev` (created on first use; caller holds mu).
+cudaError_t dev_pool(DevMem &m, int dev, DevMemPool **out) {
+    auto it = m.pools.find(dev);
+    if (it != m.pools.end()) {
+        *out = &it->second;
+        return cudaSuccess;
+    }
+    cudaMemPoolProps props{};
+    props.allocType     = cudaMemAllocationTypePinned;
+    props.handleTypes   = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id   = dev;
+    DevMemPool dp;
+    cudaError_t e = cudaMemPoolCreate(&dp.pool, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = ~0ull;
+    if ((e = cudaMemPoolSetAttribute(dp.pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&dp.st, cudaStreamNonBlocking)) != cudaSuccess) {
+        cudaMemPoolDestroy(dp.pool);
+        return e;
+    }
+    *out = &(m.pools[dev] = dp);
+    return cudaSuccess;
 }
 
 cudaError_t dev_alloc(void **p, size_t bytes) {
@@ -80,43 +101,25 @@ cudaError_t dev_alloc(void **p, size_t bytes) {
         }
     int dev = 0;
     cudaGetDevice(&dev);
-    const size_t rb = bytes <= kCacheBlock ? round_block(bytes) : bytes;
-    BlockCache  &bc = block_cache();
-    {
-        std::lock_guard<std::mutex> lk(bc.mu);
-        auto it = bc.idle.find({dev, rb});
-        if (it != bc.idle.end()) {
-            *p = it->second;
-            bc.idle.erase(it);
-            bc.idle_bytes -= rb;
-            bc.live[*p] = {rb, dev};
-            return cudaSuccess;
-        }
-    }
-    cudaError_t e = cudaMalloc(p, rb);
+    DevMem                     &m = dev_mem();
+    std::lock_guard<std::mutex> lk(m.mu);
+    DevMemPool                 *dp = nullptr;
+    cudaError_t                 e  = dev_pool(m, dev, &dp);
     if (e != cudaSuccess) return e;
-    std::lock_guard<std::mutex> lk(bc.mu);
-    bc.live[*p] = {rb, dev};
+    if ((e = cudaMallocFromPoolAsync(p, bytes, dp->pool, dp->st)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(dp->st)) != cudaSuccess) return e;
+    m.live[*p] = dev;
     return cudaSuccess;
 }
 void dev_free(void *p) {
     if (!p) return;
-    BlockCache &bc = block_cache();
-    {
-        std::lock_guard<std::mutex> lk(bc.mu);
-        auto it = bc.live.find(p);
-        if (it != bc.live.end()) {
-            const size_t b = it->second.first;
-            const int    d = it->second.second;
-            bc.live.erase(it);
-            if (b <= kCacheBlock && bc.idle_bytes + b <= kCacheTotal) {
-                bc.idle.insert({{d, b}, p});
-                bc.idle_bytes += b;
-                return;
-            }
-        }
-    }
-    cudaFree(p);
+    DevMem                     &m = dev_mem();
+    std::lock_guard<std::mutex> lk(m.mu);
+    auto it = m.live.find(p);
+    if (it == m.live.end()) return;
+    auto pit = m.pools.find(it->second);
+    if (pit != m.pools.end()) cudaFreeAsync(p, pit->second.st);
+    m.live.erase(it);
 }
 }  // namespace
 

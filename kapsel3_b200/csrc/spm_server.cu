@@ -102,7 +102,14 @@ struct spm_server {
     long long run_steps = 0, captures = 0;
     int       max_active = 0;
     double    t_first_admit = 0.0, t_last_done = 0.0;
+    // longest host phases of the worker (ms)
+    double    create_max = 0, admit_max = 0, destroy_max = 0, launch_max = 0, finish_max = 0;
     std::string worker_error;
+    void phase(double &mx, double t0) {
+        const double ms = (now_s() - t0) * 1e3;
+        std::lock_guard<std::mutex> lk(mu);
+        mx = std::max(mx, ms);
+    }
 
     void set_state(Request *q, int state, int status, const std::string &msg) {
         q->state   = state;
@@ -119,6 +126,7 @@ struct spm_server {
     void loop();
     bool admit_some();
     void finish_pool_steps(PoolEntry *pe);
+    void finish_pool_steps_impl(PoolEntry *pe);
     void retire(PoolEntry *pe, Request *q, int state, int status, const std::string &msg);
     void launch(PoolEntry *pe);
 };
@@ -145,6 +153,11 @@ void spm_server::retire(PoolEntry *pe, Request *q, int state, int status, const 
 // Accounts the steps a pool just finished: per-step latency samples, errors,
 // retirement of runs that reached their step count or were cancelled.
 void spm_server::finish_pool_steps(PoolEntry *pe) {
+    const double t_phase = now_s();
+    finish_pool_steps_impl(pe);
+    phase(finish_max, t_phase);
+}
+void spm_server::finish_pool_steps_impl(PoolEntry *pe) {
     const int n = (int)pe->members.size();
     std::vector<unsigned int> errs(n, 0u);
     float       dev_ms = 0.f;
@@ -198,7 +211,9 @@ void spm_server::launch(PoolEntry *pe) {
     int k = cfg.steps_per_launch > 0 ? cfg.steps_per_launch : 1;
     for (Request *q : pe->members) k = std::min(k, q->nsteps - q->steps_done);
     if (k <= 0) k = 1;
-    const int rc = spm_pool_step(pe->pool, k, cfg.use_graph);
+    const double t_phase = now_s();
+    const int    rc      = spm_pool_step(pe->pool, k, cfg.use_graph);
+    phase(launch_max, t_phase);
     if (rc != SPM_OK) {
         const std::string msg = std::string("pool step launch: ") + spm_last_error();
         std::vector<Request *> snapshot = pe->members;
@@ -257,8 +272,10 @@ bool spm_server::admit_some() {
         // create the pool if needed
         int rc = SPM_OK;
         if (!target) {
-            spm_pool *pl = nullptr;
+            spm_pool    *pl = nullptr;
+            const double t_phase = now_s();
             rc           = spm_pool_create(&q->p, grow_to, nullptr, &pl);
+            phase(create_max, t_phase);
             if (rc == SPM_OK) {
                 auto pe   = std::make_unique<PoolEntry>();
                 pe->key   = q->p;
@@ -274,7 +291,9 @@ bool spm_server::admit_some() {
         if (rc == SPM_OK) {
             int cap_before = 0, cap_after = 0;
             spm_pool_size(target->pool, nullptr, &cap_before);
+            const double t_phase = now_s();
             rc = spm_pool_admit(target->pool, &q->p, q->particles.empty() ? nullptr : q->particles.data(), &run);
+            phase(admit_max, t_phase);
             spm_pool_size(target->pool, nullptr, &cap_after);
             if (cap_after != cap_before) {
                 std::lock_guard<std::mutex> lk(mu);
@@ -364,7 +383,9 @@ void spm_server::loop() {
                 long long k = 0;
                 int       cnt = 0;
                 spm_pool_stats(pe->pool, &k, &cnt);
+                const double t_phase = now_s();
                 spm_pool_destroy(pe->pool);
+                phase(destroy_max, t_phase);
                 std::lock_guard<std::mutex> lk(mu);
                 captures += cnt;
                 used -= pe->arena;
@@ -592,6 +613,11 @@ int spm_server_get_stats(spm_server *s, spm_server_stats *st) {
     st->step_latency_max_ms = s->lat_ms.empty() ? 0.0 : *std::max_element(s->lat_ms.begin(), s->lat_ms.end());
     st->pool_step_device_p50_ms = percentile(s->pool_dev_ms, 0.50);
     st->pool_step_device_p99_ms = percentile(s->pool_dev_ms, 0.99);
+    st->pool_create_max_ms      = s->create_max;
+    st->admit_max_ms            = s->admit_max;
+    st->pool_destroy_max_ms     = s->destroy_max;
+    st->launch_max_ms           = s->launch_max;
+    st->finish_max_ms           = s->finish_max;
     return SPM_OK;
 }
 

@@ -161,7 +161,7 @@ class Server:
     """The native request loop (spm_server_*)."""
 
     def __init__(self, budget_bytes: int = 150 << 30, use_graph: bool = True, pool_capacity: int = 8,
-                 steps_per_launch: int = 1, device: int = 0):
+                 steps_per_launch: int = 1, device: int = 0, pool_idle_s: Optional[float] = None):
         self.L = N.lib()
         cfg = N.SpmServerConfig()
         N.check(self.L.spm_server_config_default(C.byref(cfg)), "spm_server_config_default")
@@ -170,6 +170,8 @@ class Server:
         cfg.pool_initial_capacity = pool_capacity
         cfg.steps_per_launch = steps_per_launch
         cfg.device = device
+        if pool_idle_s is not None:
+            cfg.pool_idle_s = pool_idle_s
         h = C.c_void_p()
         N.check(self.L.spm_server_create(C.byref(cfg), C.byref(h)), "spm_server_create")
         self.h = h

@@ -10,6 +10,8 @@ within 1e-6 relative velocity error, and FP32-mixed against FP64 within 1e-5.
 
 Fault tests inject every failure on the host (bad requests, budget, cancel,
 a failing device allocation); none faults or hangs the GPU."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -195,3 +197,25 @@ def test_serving_stream_small(gpu):
     assert all(r["state"] == N.SPM_REQ_DONE for r in res["results"])
     assert res["stats"]["run_steps"] == 12 * 20
     assert len(res["latencies"]) == 12 * 20
+
+
+def test_retired_memory_returns_to_the_pool_without_a_stall(gpu):
+    """Pools and runs take their device memory from the library's stream-ordered
+    memory pool: destroying a pool while another steps does not wait for the
+    device (the worker's longest pool destruction stays at milliseconds), the
+    freed blocks are handed out again, and spm_release_cached_memory returns
+    the unused part to the driver with the library still usable."""
+    w = serving_workload(n_runs=16, rate_per_s=200.0, sides=(32, 64), np_max=20, nsteps=30, seed=11)
+    from kapsel3_b200.serve import run_stream
+    with Server(pool_idle_s=0.0) as srv:
+        res = run_stream(srv, w["requests"])
+    st = res["stats"]
+    assert all(r["state"] == N.SPM_REQ_DONE for r in res["results"])
+    assert st["pool_destroy_max_ms"] < 100.0, st
+    held = C.c_size_t()
+    N.check(N.lib().spm_release_cached_memory(C.byref(held)), "spm_release_cached_memory")
+    cfg1 = SPMConfig(npx=5, npy=5, npz=5, n_particles=2, a=4.0, a_xi=2.0, dt=0.05)
+    with SPMRun(cfg1) as run:
+        run.initialize(make_particles(cfg1, seed=1))
+        run.step(2)
+        assert np.isfinite(run.particles()["v"]).all()
