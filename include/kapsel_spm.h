@@ -226,6 +226,25 @@ int spm_get_concentration(spm_ctx *ctx, int species, double *conc_k);
  * this library's own (binary, host byte order). */
 int spm_save_state(spm_ctx *ctx, const char *path);
 int spm_load_state(spm_ctx *ctx, const char *path);
+/* The reference's own restart files, so that a run moves between the
+ * reference program and this library in both directions.
+ * spm_load_restart = Force_restore_parameters (resume.cxx:507-588): reads the
+ * section resume.CONTINUE.Saved_Data of a restart file (a UDF file, or a key
+ * file of "udf.path = value" lines) into an initialised context: zeta of every
+ * mode, uk_dc, the particles (orientations normalised as Read_Particle_udf
+ * does, :757-869), jikan and degree_oblique, and an Electrolyte run's k-space
+ * concentrations.  The file's jikan.ts is the reference's index of the step
+ * just completed; the context then counts jikan.ts + 1 steps.  The reference's
+ * resumed program takes one step of its initial state before it restores (the
+ * first pass of its main loop, sp_3d_ns.cxx:856-1005), which advances its
+ * thermostat's generator; a caller that must follow it exactly does the same
+ * (kapsel3_b200.spm.resume_run).
+ * spm_save_restart = Save_Restart_udf (resume.cxx:10-74, 381-506): writes a key
+ * file with the keys of input_path (the run's input, UDF or key file; NULL for
+ * the resume section alone), resume.Calculation = CONTINUE and the section
+ * above for the context's state.  Rigid bodies and squirmers are refused. */
+int spm_load_restart(spm_ctx *ctx, const char *path);
+int spm_save_restart(spm_ctx *ctx, const char *input_path, const char *path);
 /* ---- output in the reference's legacy AVS format -----------------------
  * (output.AVS = ON, FileType = BINARY; Init_avs / Output_avs,
  * avs_output.cxx:45-143, 261-285; Init_avs_p / Output_avs_p,

@@ -148,6 +148,8 @@ _SIGS = {
     "spm_get_concentration": (C.c_int, [_P, C.c_int, _D]),
     "spm_save_state": (C.c_int, [_P, C.c_char_p]),
     "spm_load_state": (C.c_int, [_P, C.c_char_p]),
+    "spm_load_restart": (C.c_int, [_P, C.c_char_p]),
+    "spm_save_restart": (C.c_int, [_P, C.c_char_p, C.c_char_p]),
     "spm_avs_open": (C.c_int, [_P, C.c_char_p, C.c_char_p, C.c_int]),
     "spm_avs_frame": (C.c_int, [_P]),
     "spm_avs_flush": (C.c_int, [_P]),

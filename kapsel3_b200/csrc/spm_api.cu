@@ -1866,3 +1866,4 @@ int spm_kernel_launches(spm_ctx *c, long long *count, int reset) {
 #include "spm_pool.inc"
 #include "spm_checkpoint.inc"
 #include "spm_output.inc"
+#include "spm_restart.inc"

@@ -320,6 +320,17 @@ class SPMRun:
         """Restores a checkpoint written by a run with the same parameters."""
         N.check(self.L.spm_load_state(self.h, path.encode()), "spm_load_state")
 
+    def load_restart(self, path: str):
+        """Restores the saved section of a restart file of the reference
+        program (spm_load_restart; UDF or key file)."""
+        N.check(self.L.spm_load_restart(self.h, path.encode()), "spm_load_restart")
+
+    def save_restart(self, path: str, input_path: Optional[str] = None):
+        """Writes a restart key file the reference program resumes from
+        (spm_save_restart): the keys of `input_path`, then the saved state."""
+        N.check(self.L.spm_save_restart(self.h, input_path.encode() if input_path else None, path.encode()),
+                "spm_save_restart")
+
     def avs_open(self, out_dir: str, out_name: str, num_snap: int):
         """Legacy AVS output of this run (spm_avs_open): headers now, one
         frame per avs_frame() call."""
@@ -428,6 +439,29 @@ class SPMRun:
                                    else pack_particles(particles, self.cfg.n_particles), dtype=float).copy()
         N.check(self.L.spm_calc_f_lennard_jones_host(self.h, N.dptr(rec)), "Calc_f_Lennard_Jones")
         return rec
+
+
+def resume_run(path: str, precision: int = N.SPM_PREC_FP64, mt_seed: int = 0,
+               config: Optional[SPMConfig] = None) -> "SPMRun":
+    """A run resumed from a restart file of the reference program (UDF file,
+    or a key file ending in .keys), as its main loop resumes one
+    (sp_3d_ns.cxx:856-1005): the run is set up from the file's parameters and
+    initial particles, takes one step (the reference's first pass, whose
+    result the restore overwrites; it draws that step's thermostat noise),
+    and then restores the saved section (Force_restore_parameters).
+    `config` replaces the file's parameters where the file cannot hold them
+    all (a constant body force has no UDF key)."""
+    cfg, parts = config_from_udf(path)
+    cfg = config or cfg
+    run = SPMRun(cfg, precision=precision, mt_seed=mt_seed)
+    try:
+        run.initialize(parts)
+        run.step(1)
+        run.load_restart(path)
+    except Exception:
+        run.close()
+        raise
+    return run
 
 
 def device_count() -> int:

@@ -478,6 +478,16 @@ def udf_text(keys: Dict[str, str]) -> tuple:
     return "\n".join(schema) + "\n", "\n".join(data) + "\n"
 
 
+def write_udf_from_keys(path: str, keys: Dict[str, str]) -> None:
+    """Writes a key map (e.g. a restart key file of spm_save_restart, read
+    with read_udf_keys) as a self-describing UDF file."""
+    schema, data = udf_text(keys)
+    with open(path, "w") as f:
+        f.write("// written by kapsel3_b200.udf.write_udf_from_keys\n")
+        f.write(schema)
+        f.write(data)
+
+
 def write_udf(path: str, cfg: SPMConfig, particles: Dict[str, np.ndarray],
               out_dir: Optional[str] = None, define_path: Optional[str] = None) -> None:
     """Writes the run as a UDF input file (the paths of `udf_keys`).  With

@@ -8,7 +8,11 @@
 // lines keyed by the same UDF paths that the reference asks for through
 // `UDFManager::get` (e.g. `mesh.NPX = 5`,
 // `object_type.spherical_particle.Particle_spec[0].Particle_number = 2`).
-// `put` records values in memory only; `write` and `newRecord` do nothing.
+// `put` records values in memory; `write` writes them to the file named at
+// construction as the same key lines (the restart file of Save_Restart_udf,
+// resume.cxx:10-74, can then be read back as an input), and after
+// `newRecord` (Output_udf, output.cxx:268-375) every record's keys are
+// written with the prefix `record[<n>].`.
 // A `get` of a missing key prints the key to stderr and returns false (the
 // reference probes optional keys this way, input.cxx:667-675); the key files
 // used here are checked to produce no such line for a required key.
@@ -21,6 +25,7 @@
 #include <map>
 #include <sstream>
 #include <string>
+#include <vector>
 
 class Location {
   public:
@@ -43,8 +48,8 @@ class Location {
 class UDFManager {
   public:
     explicit UDFManager(const std::string &file) { load(file); }
-    UDFManager(const std::string &file, const std::string & /*def*/, bool /*flag*/) { (void)file; }
-    UDFManager(const std::string &file, const std::string & /*def*/, int /*flag*/) { (void)file; }
+    UDFManager(const std::string &file, const std::string & /*def*/, bool /*flag*/) : out_(file) {}
+    UDFManager(const std::string &file, const std::string & /*def*/, int /*flag*/) : out_(file) {}
     ~UDFManager() {}
 
     template <typename T>
@@ -90,8 +95,30 @@ class UDFManager {
         }
         return n;
     }
-    void        write() {}
-    void        newRecord() {}
+    void write() {
+        if (out_.empty()) return;
+        FILE *f = std::fopen(out_.c_str(), "w");
+        if (!f) {
+            std::fprintf(stderr, "udf stand-in: cannot write '%s'\n", out_.c_str());
+            return;
+        }
+        if (records_.empty()) {
+            for (std::map<std::string, std::string>::const_iterator it = kv_.begin(); it != kv_.end(); ++it)
+                std::fprintf(f, "%s = %s\n", it->first.c_str(), it->second.c_str());
+        } else {
+            records_.push_back(kv_);
+            for (size_t r = 1; r < records_.size(); r++)
+                for (std::map<std::string, std::string>::const_iterator it = records_[r].begin();
+                     it != records_[r].end(); ++it)
+                    std::fprintf(f, "record[%zu].%s = %s\n", r - 1, it->first.c_str(), it->second.c_str());
+            records_.pop_back();
+        }
+        std::fclose(f);
+    }
+    void newRecord() {
+        records_.push_back(kv_);
+        kv_.clear();
+    }
     std::string getEngineName() { return "kapsel"; }
     std::string getEngineVersion() { return "v3"; }
 
@@ -117,7 +144,9 @@ class UDFManager {
         std::string::size_type e = s.find_last_not_of(" \t\r\n");
         return s.substr(b, e - b + 1);
     }
-    std::map<std::string, std::string> kv_;
+    std::map<std::string, std::string>              kv_;
+    std::string                                     out_;
+    std::vector<std::map<std::string, std::string> > records_;
 };
 
 #endif
