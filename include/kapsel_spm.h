@@ -244,6 +244,15 @@ int spm_load_state(spm_ctx *ctx, const char *path);
  * the resume section alone), resume.Calculation = CONTINUE and the section
  * above for the context's state.  Rigid bodies and squirmers are refused. */
 int spm_load_restart(spm_ctx *ctx, const char *path);
+/* Per-frame particle records of the reference's UDF output (output.UDF = ON;
+ * Output_udf, output.cxx:268-375): spm_udf_out_record appends one record of
+ * the context's current state (E, t = the completed steps, and per particle
+ * R, R_raw, v, q, omega and the previous step's f_hydro, torque_hydro, f_r,
+ * torque_r, f_slip, torque_slip; rigid runs add RigidParticles[]) to the file
+ * opened by spm_udf_out_open, as "record[<n>].<udf.path> = <value>" lines. */
+int spm_udf_out_open(spm_ctx *ctx, const char *path);
+int spm_udf_out_record(spm_ctx *ctx);
+int spm_udf_out_close(spm_ctx *ctx);
 int spm_save_restart(spm_ctx *ctx, const char *input_path, const char *path);
 /* ---- output in the reference's legacy AVS format -----------------------
  * (output.AVS = ON, FileType = BINARY; Init_avs / Output_avs,

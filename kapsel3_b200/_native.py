@@ -149,6 +149,9 @@ _SIGS = {
     "spm_save_state": (C.c_int, [_P, C.c_char_p]),
     "spm_load_state": (C.c_int, [_P, C.c_char_p]),
     "spm_load_restart": (C.c_int, [_P, C.c_char_p]),
+    "spm_udf_out_open": (C.c_int, [_P, C.c_char_p]),
+    "spm_udf_out_record": (C.c_int, [_P]),
+    "spm_udf_out_close": (C.c_int, [_P]),
     "spm_save_restart": (C.c_int, [_P, C.c_char_p, C.c_char_p]),
     "spm_avs_open": (C.c_int, [_P, C.c_char_p, C.c_char_p, C.c_int]),
     "spm_avs_frame": (C.c_int, [_P]),

@@ -156,6 +156,7 @@ int slots_for(const spm_params &p) {
 
 struct spm_pool;
 struct AvsOut;
+struct UdfOut;
 
 struct spm_ctx {
     spm_params   P{};
@@ -225,6 +226,7 @@ struct spm_ctx {
     bool                     zeta_dirty = false;  // zeta set by the host since the last NS step
     int                      nslots     = NSLOT;  // field slots of this run (slots_for)
     AvsOut                  *avs        = nullptr;  // AVS field/particle output (spm_avs_open)
+    UdfOut                  *udf_out    = nullptr;  // UDF particle records (spm_udf_out_open)
     // one Navier_Stokes step of a lone run captured as a CUDA graph and
     // replayed by spm_step (SPM_NO_GRAPH=1 keeps the direct launches)
     bool                     use_graph    = true;
@@ -1218,6 +1220,7 @@ int download_particles(spm_ctx *c, double *rec) {
 #include "spm_rigid.inc"
 
 void avs_release(spm_ctx *c);
+void udf_out_release(spm_ctx *c);
 
 // Electrolyte run constants from the parameters (Init_rho_ion,
 // operate_electrolyte.cxx:667-720, 490-520; Elementary_charge = 1,
@@ -1269,6 +1272,7 @@ void el_init_state(ELState &el, const spm_params &p) {
 void destroy_ctx(spm_ctx *c) {
     if (!c) return;
     avs_release(c);
+    udf_out_release(c);
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->step_exec) cudaGraphExecDestroy(c->step_exec);
     if (c->step_graph) cudaGraphDestroy(c->step_graph);
@@ -1867,3 +1871,4 @@ int spm_kernel_launches(spm_ctx *c, long long *count, int reset) {
 #include "spm_checkpoint.inc"
 #include "spm_output.inc"
 #include "spm_restart.inc"
+#include "spm_udf_out.inc"

@@ -331,6 +331,17 @@ class SPMRun:
         N.check(self.L.spm_save_restart(self.h, input_path.encode() if input_path else None, path.encode()),
                 "spm_save_restart")
 
+    def udf_out_open(self, path: str):
+        """Opens the per-frame UDF particle records (spm_udf_out_open)."""
+        N.check(self.L.spm_udf_out_open(self.h, path.encode()), "spm_udf_out_open")
+
+    def udf_out_record(self):
+        """Appends one record of the current state (Output_udf)."""
+        N.check(self.L.spm_udf_out_record(self.h), "spm_udf_out_record")
+
+    def udf_out_close(self):
+        N.check(self.L.spm_udf_out_close(self.h), "spm_udf_out_close")
+
     def avs_open(self, out_dir: str, out_name: str, num_snap: int):
         """Legacy AVS output of this run (spm_avs_open): headers now, one
         frame per avs_frame() call."""

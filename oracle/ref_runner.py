@@ -64,10 +64,13 @@ def available(omp: bool = False, gpu_shim: bool = False, gpu_resident: bool = Fa
 def run_reference(keys_path: str, dump_path: Optional[str] = None, fields_every: int = 1,
                   body_force=(0.0, 0.0, 0.0), omp: bool = False, threads: Optional[int] = None,
                   step_times_path: Optional[str] = None, timeout: float = 3600.0, gpu_shim: bool = False,
-                  gpu_resident: bool = False, restart_path: Optional[str] = None) -> str:
+                  gpu_resident: bool = False, restart_path: Optional[str] = None,
+                  out_udf_path: Optional[str] = None) -> str:
     """Runs the reference program on a key file; with restart_path, its
     restart file (written at the end of every run, Save_Restart_udf) goes
-    there as a key file that a later run can take as its input."""
+    there as a key file that a later run can take as its input; with
+    out_udf_path, its output UDF (the Output_udf records of a run with
+    output.UDF = ON) goes there as record[n].<path> key lines."""
     exe = ref_binary(omp, gpu_shim, gpu_resident)
     if exe is None:
         raise FileNotFoundError("oracle/_ref is not built (make -C oracle/ref_build)")
@@ -82,7 +85,8 @@ def run_reference(keys_path: str, dump_path: Optional[str] = None, fields_every:
     if threads is not None:
         env["OMP_NUM_THREADS"] = str(threads)
     wd = tempfile.mkdtemp(prefix="kapsel_ref_")
-    cmd = [exe, f"-I{keys_path}", f"-O{wd}/out.udf", f"-D{wd}/def.udf", f"-R{restart_path or wd + '/res.udf'}"]
+    cmd = [exe, f"-I{keys_path}", f"-O{out_udf_path or wd + '/out.udf'}", f"-D{wd}/def.udf",
+           f"-R{restart_path or wd + '/res.udf'}"]
     open(f"{wd}/def.udf", "w").close()
     r = subprocess.run(cmd, env=env, cwd=wd, capture_output=True, text=True, timeout=timeout)
     if r.returncode != 0:

@@ -41,9 +41,20 @@ def _fields(path, cfg):
     return np.fromfile(path, dtype=np.float32).reshape(10, nz, ny, nx)
 
 
+LE_CASE = SPMConfig(npx=5, npy=5, npz=4, n_particles=3, a=3.5, a_xi=2.0, dt=0.05, gts=2, num_snap=3,
+                    equation=EQ_LE, shear_rate=0.5, kbt=1e-5)
+
+
 @pytest.mark.skipif(not os.access(AVS_REF, os.X_OK), reason="oracle/_ref/kapsel_ref_avs is not built")
-def test_avs_files_match_the_reference_program(gpu, tmp_path):
-    cfg = SPMConfig(npx=5, npy=4, npz=6, n_particles=3, a=4.0, a_xi=2.0, dt=0.05, gts=2, num_snap=2)
+@pytest.mark.parametrize("equation", ["navier_stokes", "lees_edwards"])
+def test_avs_files_match_the_reference_program(gpu, tmp_path, equation):
+    """Lees-Edwards frames take u and the stress from the oblique grid and
+    components to Cartesian ones, u with the mean flow of Shear_rate_eff
+    (U_oblique2u, Stress_oblique2Stress; output.cxx:133-146)."""
+    if equation == "lees_edwards":
+        cfg = LE_CASE
+    else:
+        cfg = SPMConfig(npx=5, npy=4, npz=6, n_particles=3, a=4.0, a_xi=2.0, dt=0.05, gts=2, num_snap=2)
     parts = make_particles(cfg, seed=3, v_sd=1e-3, random_orientation=True)
     keys = str(tmp_path / "in.keys")
     write_udf_keys(keys, cfg, parts, out_dir=str(tmp_path / "ref"))
@@ -82,8 +93,3 @@ def test_avs_fp32_run_and_errors(gpu, tmp_path):
         run.initialize(parts)
         with pytest.raises(N.SpmError, match="spm_avs_open was not called"):
             run.avs_frame()
-    le = SPMConfig(npx=5, npy=5, npz=5, n_particles=2, a=4.0, equation=EQ_LE, shear_rate=0.1)
-    with SPMRun(le) as run:
-        run.initialize(make_particles(le, seed=4))
-        with pytest.raises(N.SpmError, match="Lees-Edwards"):
-            run.avs_open(str(tmp_path / "le"), "frame", 1)
