@@ -211,7 +211,12 @@ int spm_get_time(spm_ctx *ctx, int *ts, double *time);
  * line of Mean_shear_stress (sp_3d_ns.h:296-339): stress[0..7] =
  * {Shear_rate_eff, strain, lj, hydro_old, hydro_new, reynolds, fluid,
  * apparent}.  For a Lees-Edwards run spm_get_velocity returns the oblique
- * (contravariant) velocity on the sheared grid. */
+ * (contravariant) velocity on the sheared grid.  A Shear_Navier_Stokes run
+ * gives its line (Update_strain, sp_3d_ns.h:205-214; Mean_shear_stress,
+ * :319-340): degree_oblique = 0, stress[0..5] = {the instantaneous shear
+ * rate, the strain since initialisation, the shear stress -stress_yx, the
+ * viscosity -stress_yx / rate, the inertia stress (AC), -stress_yx + inertia
+ * (AC)}. */
 int spm_get_shear_state(spm_ctx *ctx, double *degree_oblique, double stress[8]);
 /* Electrolyte runs: the k-space concentration of ion species `species`
  * (0: the counterion of a saltfree run or the positive ion; 1: the negative

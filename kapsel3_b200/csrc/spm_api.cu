@@ -26,6 +26,7 @@
 #include "spm_le.cuh"
 #include "spm_electrolyte.cuh"
 #include "spm_janus.cuh"
+#include "spm_sns.cuh"
 
 using namespace spm;
 
@@ -204,6 +205,8 @@ struct spm_ctx {
     // convergence value of the last slip iteration
     double      *slip     = nullptr;
     double      *slip_eps = nullptr;
+    // Shear_Navier_Stokes runs: the diagnostics' words and row sums (spm_sns.cuh)
+    double      *sns      = nullptr;
     // rigid bodies (spm_rigid.cuh): device state and the species' free degrees of freedom
     RigidDev     rg{};
     RigidFree    rfree{};
@@ -844,7 +847,7 @@ int shear_sustain(spm_ctx *c) {
     const double t   = (double)c->ts * c->ph.dt;
     const double amp = c->P.shear_ac ? cos(c->P.shear_frequency * t) : 1.0;
     LAUNCH(c, r_shear_sustain<T>, c->grid_blocks(), 256, 0, c->g, c->real<T>(U0), c->P.shear_ac, c->P.shear_rate,
-           c->ph.L[1], amp);
+           c->ph.L[1], amp, c->sns ? c->real<T>(A0) : (T *)nullptr);
     SPM_TRY(fft_fwd<T>(c, U0, 3));
     LAUNCH(c, k_u_to_zeta<T>, c->grid_blocks(), 256, 0, c->g, c->cx<T>(U0), c->cx<T>(U1), c->cx<T>(U2),
            c->cx<T>(Z0), c->cx<T>(Z1), c->uk_dc);
@@ -853,6 +856,45 @@ int shear_sustain(spm_ctx *c) {
         SPM_CUDA_CHECK(cudaMemsetAsync(c->real<T>(ZL0), 0, c->field_bytes(), c->st));
         SPM_CUDA_CHECK(cudaMemsetAsync(c->real<T>(ZL1), 0, c->field_bytes(), c->st));
     }
+    return SPM_OK;
+}
+
+// The Shear_Navier_Stokes diagnostics of the step (spm_sns.cuh), after the
+// rigidity force f is scattered into UP and before its projection: the
+// density of the particles' current positions into A1, the row sums of
+// u + f (U0 + UP0), fs rho (A0 holds the step's sustaining force) and
+// rho (u + f), then the rate, strain and stresses.
+template <typename T>
+int shear_diagnostics(spm_ctx *c) {
+    SPM_CUDA_CHECK(cudaMemsetAsync(c->real<T>(A1), 0, c->field_bytes(), c->st));
+    if (c->ph.np > 0) {
+        RhoWeights w{};
+        const int  nsp = std::max(c->P.n_species, 1);
+        for (int s = 0; s < 4; s++) {
+            const double mr = s < nsp ? (nsp > 1 ? c->P.species_mass_ratio[s] : c->P.mass_ratio) : 1.0;
+            w.drho[s]       = mr * c->P.rho - c->P.rho;
+        }
+        const dim3 sgrid((c->ncells + 127) / 128, c->ph.np);
+        LAUNCH(c, s_rho_scatter<T>, sgrid, 128, 0, c->g, c->ph, c->ps.x, c->cells, c->ncells, c->real<T>(A1), w);
+    }
+    double *rows = c->sns + kSnsWords;
+    LAUNCH(c, r_sns_rows<T>, c->g.ny, 256, 0, c->g, c->real<T>(U0), c->real<T>(UP0), c->real<T>(A0), c->real<T>(A1),
+           c->P.rho, rows, 0);
+    LAUNCH(c, k_sns_finish, 1, 512, 0, c->g, rows, c->sns, c->ph.dt, 0);
+    return SPM_OK;
+}
+
+// AC: the inertia stress from u_x of the step's new zeta (U0 is free at the
+// end of the step; A1 still holds the density).
+template <typename T>
+int shear_inertia(spm_ctx *c) {
+    LAUNCH(c, (k_zeta_to_u<T, 0>), c->pw_grid(), 256, 0, c->g, c->cx<T>(Z0), c->cx<T>(Z1), c->uk_dc, c->cx<T>(U0),
+           c->cx<T>(U1), c->cx<T>(U2), 0, c->fstride_c);
+    SPM_TRY(fft_inv_packed<T>(c, U0, 1));
+    double *rows = c->sns + kSnsWords;
+    LAUNCH(c, r_sns_rows<T>, c->g.ny, 256, 0, c->g, c->real<T>(U0), c->real<T>(U0), c->real<T>(A0), c->real<T>(A1),
+           c->P.rho, rows, 1);
+    LAUNCH(c, k_sns_finish, 1, 512, 0, c->g, rows, c->sns, c->ph.dt, 1);
     return SPM_OK;
 }
 
@@ -993,7 +1035,9 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
                 c->ps.x, c->ps.v, c->ps.omega, c->cells, c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS),
                 c->real<T>(U0), c->real<T>(U1), c->real<T>(U2), c->real<T>(UP0), c->real<T>(UP1), c->real<T>(UP2));
     }
+    if (L->sns) SPM_TRY(shear_diagnostics<T>(L));  // lone Shear_Navier_Stokes runs
     if ((rc = rigidity_projection<T>(L)) != SPM_OK) return rc;
+    if (L->sns && L->P.shear_ac) SPM_TRY(shear_inertia<T>(L));
     LAUNCH(L, k_ts_advance, (nr + 127) / 128, 128, 0, L->rw, nr);
     for (int r = 0; r < nr; r++) {
         R[r]->ts++;
@@ -1018,6 +1062,7 @@ int initialize_impl(spm_ctx *c) {
     if ((rc = zeta_to_velocity<T>(c, 1)) != SPM_OK) return rc;
     if ((rc = rigidity_projection<T>(c)) != SPM_OK) return rc;
     LAUNCH(c, k_zero3, 1, 32, 0, c->uk_dc);
+    if (c->sns) SPM_CUDA_CHECK(cudaMemsetAsync(c->sns, 0, kSnsWords * sizeof(double), c->st));
     // shear runs start with v_x = omega_z = 0 (init_particle.cxx:768-781)
     if ((c->le.enabled || c->P.equation == SPM_EQ_SHEAR_NAVIER_STOKES) && c->ph.np > 0)
         LAUNCH(c, p_le_zero_vx, particle_blocks(c), 128, 0, c->ph, c->ps);
@@ -1294,6 +1339,7 @@ void destroy_ctx(spm_ctx *c) {
     dev_free(c->el.partial);
     dev_free(c->slip);
     dev_free(c->slip_eps);
+    dev_free(c->sns);
     dev_free(c->rg_ibuf);
     dev_free(c->rg_dbuf);
     if (c->side) cudaStreamDestroy(c->side);
@@ -1450,6 +1496,11 @@ int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *
     c->ps.mdf                   = c->ps.torque_r_previous + (size_t)np * 3;
     c->ps.lj_stress             = c->ps.mdf + (size_t)np * 3;
     le_init(c->le, c->g, c->ph, p);
+    if (p.equation == SPM_EQ_SHEAR_NAVIER_STOKES && pool_cap == 0 && !lead &&
+        dev_alloc((void **)&c->sns, ((size_t)kSnsWords + 3 * (size_t)c->g.ny) * sizeof(double)) != cudaSuccess) {
+        destroy_ctx(c);
+        return fail(SPM_ERR_NOMEM, "shear diagnostics buffer");
+    }
     if (p.janus_propulsion == SPM_JANUS_SQUIRMER) {
         if (dev_alloc((void **)&c->slip, (size_t)std::max(np, 1) * kSlipWords * sizeof(double)) != cudaSuccess ||
             dev_alloc((void **)&c->slip_eps, sizeof(double)) != cudaSuccess) {
@@ -1711,6 +1762,16 @@ int spm_get_shear_state(spm_ctx *c, double *degree_oblique, double stress[8]) {
     if (!c) return fail(SPM_ERR_ARG, "null context");
     int rc = spm_synchronize(c);
     if (rc != SPM_OK) return rc;
+    if (c->sns) {
+        double w[kSnsWords];
+        SPM_CUDA_CHECK(cudaMemcpy(w, c->sns, sizeof(w), cudaMemcpyDeviceToHost));
+        if (degree_oblique) *degree_oblique = 0.0;
+        if (stress) {
+            const int map[8] = {kSnsRate, kSnsStrain, kSnsStress, kSnsVisc, kSnsInertia, kSnsApparent, -1, -1};
+            for (int i = 0; i < 8; i++) stress[i] = map[i] >= 0 ? w[map[i]] : 0.0;
+        }
+        return SPM_OK;
+    }
     return le_get_state(c, degree_oblique, stress);
 }
 

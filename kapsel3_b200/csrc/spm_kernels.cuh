@@ -62,14 +62,18 @@ struct Phys {
 // u_x = zigzag(j) cos(omega t) everywhere, zigzag = -rate j DX for j < LY/4,
 // rate (LY - j DX) in the last quarter, rate (j DX - LY/2) between.
 template <typename T>
-__global__ void r_shear_sustain(Grid g, T *__restrict__ u0, int ac, double rate, double ly, double amp) {
+// fs (optional) receives the change made to u_x, the reference's Shear_force
+// (fluid_solver.cxx:71-72, 112), zero off the planes under DC.
+__global__ void r_shear_sustain(Grid g, T *__restrict__ u0, int ac, double rate, double ly, double amp,
+                                T *__restrict__ fs) {
     const size_t rowlen = 2 * (size_t)g.hnzp;
     const size_t n      = (size_t)g.nx * g.ny * rowlen;
     const double qly = ly / 4., hly = ly / 2.;
     const int    j1 = g.ny / 4, j2 = 3 * g.ny / 4;
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
         if ((int)(idx % rowlen) >= g.nz) continue;
-        const int j = (int)((idx / rowlen) % (size_t)g.ny);
+        const int j   = (int)((idx / rowlen) % (size_t)g.ny);
+        const T   old = u0[idx];
         if (!ac) {
             if (j == j1) u0[idx] = (T)(-(rate * qly * g.dx));
             if (j == j2) u0[idx] = (T)(rate * qly * g.dx);
@@ -78,6 +82,7 @@ __global__ void r_shear_sustain(Grid g, T *__restrict__ u0, int ac, double rate,
             const double v = q == 0 ? -rate * j * g.dx : (q == 3 ? rate * ly - rate * j * g.dx : -rate * hly + rate * j * g.dx);
             u0[idx]        = (T)(v * amp);
         }
+        if (fs) fs[idx] = u0[idx] - old;
     }
 }
 
