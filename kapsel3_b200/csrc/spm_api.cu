@@ -380,7 +380,8 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
     }
     // rigid bodies (object_type.rigid, input.cxx:1583-1700)
     if (p.rigid) {
-        if (p.equation != SPM_EQ_NAVIER_STOKES) return fail(SPM_ERR_ARG, "rigid bodies are served in Navier_Stokes runs");
+        if (p.equation != SPM_EQ_NAVIER_STOKES && p.equation != SPM_EQ_SHEAR_NAVIER_STOKES)
+            return fail(SPM_ERR_ARG, "rigid bodies are served in Navier_Stokes and Shear_Navier_Stokes runs");
         if (p.janus_propulsion != SPM_JANUS_OFF) return fail(SPM_ERR_ARG, "rigid bodies have no janus propulsion");
         if (!p.rotation) return fail(SPM_ERR_ARG, "rigid bodies need ROTATION ON");
         if (p.body_force[0] != 0.0 || p.body_force[1] != 0.0 || p.body_force[2] != 0.0)

@@ -119,3 +119,48 @@ def test_fixed_body_keeps_its_motion(gpu):
                 # (init_set_vGs, rigid.h:248-251), and kept there
                 w = _rotate(q0[first[b]], w_body)
                 assert np.abs(bodies["wg"][b] - w).max() < 1e-12 * np.linalg.norm(w_body)
+
+
+@pytest.mark.skipif(not __import__("oracle.ref_runner", fromlist=["x"]).available(),
+                    reason="reference program not built (oracle/_ref)")
+@pytest.mark.parametrize("ac", [False, True])
+def test_rigid_bodies_under_sustained_shear_match_the_reference(gpu, ac, tmp_path):
+    """Rigid bodies in a Shear_Navier_Stokes box (as the reference's
+    Examples/08/s001_t000_rigid.udf): the reference program's particles and
+    zeta after every step within 1e-10, and its stress line."""
+    import dataclasses
+
+    from kapsel3_b200.udf import EQ_SNS, make_rigid_bodies, write_udf_keys
+    from oracle import ref_runner
+
+    cfg, _, _ = load("rigid_32_free_gravity")
+    cfg = dataclasses.replace(cfg, equation=EQ_SNS, shear_rate=0.03, shear_ac=ac, shear_frequency=0.4,
+                              rigid_gravity=(0.0, 0.0, 0.0), gts=1, num_snap=6)
+    parts = make_rigid_bodies(cfg, seed=31)
+    keys, dump = str(tmp_path / "in.keys"), str(tmp_path / "d.bin")
+    write_udf_keys(keys, cfg, parts, out_dir=str(tmp_path / "avs"))
+    err = ref_runner.run_reference(keys, dump, fields_every=1, timeout=600)
+    frames = ref_runner.read_dump(dump)["frames"]
+    width = 6 if ac else 5
+    lines = []
+    for line in err.splitlines():
+        f = line.split()
+        if len(f) == width and not line.startswith("#"):
+            try:
+                lines.append([float(v) for v in f])
+            except ValueError:
+                pass
+    with SPMRun(cfg) as run:
+        run.initialize(parts)
+        for fr in frames:
+            if fr["ts"] > 0:
+                run.step(1)
+                deg, st = run.shear_state()
+                ours = [run.time()[1], st[0], st[1], st[2]] + ([st[4], st[5]] if ac else [st[3]])
+                for a, b in zip(ours, lines[fr["ts"] - 1]):
+                    assert abs(a - b) <= 6e-8 * abs(b) + 1e-14, (fr["ts"], ours, lines[fr["ts"] - 1])
+            p = run.particles()
+            for k in ("x", "v", "omega", "q"):
+                assert rel(p[k], fr[k]) < 1e-10, (fr["ts"], k, rel(p[k], fr[k]))
+            z, _ = run.zeta()
+            assert rel(z, fr["zeta"]) < 1e-10, (fr["ts"], "zeta")

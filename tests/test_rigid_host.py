@@ -134,8 +134,9 @@ def _rigid_examples():
 def test_reference_rigid_examples_pass_the_checks():
     """Every rigid example input of the reference parses unless it switches
     on a force outside the step (Examples/12: a flat wall and Quincke
-    rotation); the Navier_Stokes ones pass the library's checks (gravity
-    included), the sheared ones are refused with a message."""
+    rotation); the Navier_Stokes and Shear_Navier_Stokes ones pass the
+    library's checks (gravity included), the Lees-Edwards one is refused
+    with a message."""
     ns = 0
     for f in _rigid_examples():
         p = N.SpmParams()
@@ -146,9 +147,9 @@ def test_reference_rigid_examples_pass_the_checks():
             continue
         assert N.lib().spm_params_from_udf(f.encode(), C.byref(p), None, 0) == 0, f
         rc, nbytes = _bytes(p)
-        if p.equation == N.SPM_EQ_NAVIER_STOKES:
+        if p.equation in (N.SPM_EQ_NAVIER_STOKES, N.SPM_EQ_SHEAR_NAVIER_STOKES):
             assert rc == 0 and nbytes > 0, (f, N.lib().spm_last_error())
             ns += 1
         else:
             assert rc == N.SPM_ERR_ARG and b"Navier_Stokes runs" in N.lib().spm_last_error(), f
-    assert ns >= 5
+    assert ns >= 6
