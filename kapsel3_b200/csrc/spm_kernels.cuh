@@ -343,13 +343,15 @@ __global__ void r_advection_products(Grid g, T *__restrict__ u0, T *__restrict__
 // ---------------------------------------------------------------------------
 template <typename T, int BOX>
 __global__ void k_ns_update(Grid g, cplx<T> *__restrict__ z0p, cplx<T> *__restrict__ z1p,
-                            const cplx<T> *__restrict__ p_u2u3, const cplx<T> *__restrict__ p_u3u1,
-                            const cplx<T> *__restrict__ p_u1u2, const cplx<T> *__restrict__ p_a0,
+                            cplx<T> *__restrict__ p_u2u3, cplx<T> *__restrict__ p_u3u1,
+                            cplx<T> *__restrict__ p_u1u2, const cplx<T> *__restrict__ p_a0,
                             const cplx<T> *__restrict__ p_a1, double nu, double dt, size_t run_stride_c,
-                            cplx<T> *__restrict__ zl0, cplx<T> *__restrict__ zl1) {
+                            cplx<T> *__restrict__ zl0, cplx<T> *__restrict__ zl1,
+                            const RunWords *__restrict__ rw) {
     const size_t ro = blockIdx.y * run_stride_c;
     z0p += ro, z1p += ro, p_u2u3 += ro, p_u3u1 += ro, p_u1u2 += ro, p_a0 += ro, p_a1 += ro;
     if (zl0) zl0 += ro, zl1 += ro;
+    if (rw) rw += blockIdx.y;
     for_modes<BOX>(g, [&](size_t idx, const KPoint &p, bool valid) {
         if (!valid) return;
         if (!p.keep) {
@@ -398,6 +400,20 @@ __global__ void k_ns_update(Grid g, cplx<T> *__restrict__ z0p, cplx<T> *__restri
         }
         z0p[idx] = z0;
         z1p[idx] = z1;
+        if (rw) {
+            // Zeta_k2u_k of the new zeta (k_zeta_to_u of the retained box) into the
+            // three product slots this mode has just consumed; k = 0 takes uk_dc
+            // with the FIX_CELL components zeroed, as k_fix_cell then leaves it
+            cplx<T> om[3], u[3] = {{0, 0}, {0, 0}, {0, 0}};
+            zeta_to_omega<T>(p, z0, z1, om);
+            const T ik2 = ik2_of<T>(p);
+            i_cross<T>((T)p.kx * ik2, (T)p.ky * ik2, (T)p.kz * ik2, om, u);
+            if (idx == 0)
+                for (int d = 0; d < 3; d++) u[d].re = (rw->fix_mask & (1 << d)) ? (T)0 : (T)rw->uk_dc[d];
+            p_u2u3[idx] = u[0];
+            p_u3u1[idx] = u[1];
+            p_u1u2[idx] = u[2];
+        }
     });
 }
 

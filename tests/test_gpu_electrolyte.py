@@ -109,8 +109,26 @@ def test_electrolyte_parameter_checks(gpu):
                       "Poisson_Boltzmann"), (dict(salt=True, valency=(1.0, 1.0)), "salt")):
         with pytest.raises(N.SpmError, match=msg):
             SPMRun(SPMConfig(**{**base, **bad}), precision=N.SPM_PREC_FP64)
-    with pytest.raises(N.SpmError, match="FP64"):
-        SPMRun(SPMConfig(**base), precision=N.SPM_PREC_FP32_MIXED)
+
+
+@pytest.mark.parametrize("name", ["salt_ac", "pb_counterions_dc"])
+def test_electrolyte_fp32_mixed_close_to_fp64(gpu, name):
+    """FP32 fields and transforms (plain FP32 zeta and concentrations) with
+    FP64 particle work and sums: velocities, the flow and the ion
+    concentrations within 1e-5 of the FP64 run after a few dozen steps."""
+    cfg = CASES[name]
+    parts = make_particles(cfg, seed=41, v_sd=1e-3, random_orientation=True)
+    out = {}
+    for prec in (N.SPM_PREC_FP64, N.SPM_PREC_FP32_MIXED):
+        with SPMRun(cfg, precision=prec) as run:
+            run.initialize(parts)
+            run.step(30)
+            out[prec] = (run.particles()["v"], run.velocity(), [run.concentration(n) for n in range(2 if cfg.salt else 1)])
+    v32, u32, c32 = out[N.SPM_PREC_FP32_MIXED]
+    v64, u64, c64 = out[N.SPM_PREC_FP64]
+    assert rel(v32, v64) <= 1e-5 and rel(u32, u64) <= 1e-5, (rel(v32, v64), rel(u32, u64))
+    for a, b in zip(c32, c64):
+        assert rel(a, b) <= 1e-5, rel(a, b)
 
 
 AVS_REF = os.path.join(ref_runner.REF_DIR, "kapsel_ref_avs")
