@@ -207,6 +207,11 @@ int spm_get_velocity(spm_ctx *ctx, double *u0, double *u1, double *u2);
 /* phi = min(phi_sum, 1) of the current particle positions (NX*NY*NZ_). */
 int spm_get_phi(spm_ctx *ctx, double *phi);
 int spm_get_time(spm_ctx *ctx, int *ts, double *time);
+/* Sets the completed-step count, the time and (Lees-Edwards) degree_oblique,
+ * as Force_restore_parameters restores jikan and degree_oblique
+ * (resume.cxx:555-570) after the state was uploaded with spm_set_zeta and
+ * spm_set_particles.  The step counter selects Euler (0) or Adams-Bashforth. */
+int spm_set_time(spm_ctx *ctx, int ts, double time, double degree_oblique);
 /* Lees-Edwards bookkeeping: degree_oblique and the last step's shear-stress
  * line of Mean_shear_stress (sp_3d_ns.h:296-339): stress[0..7] =
  * {Shear_rate_eff, strain, lj, hydro_old, hydro_new, reynolds, fluid,

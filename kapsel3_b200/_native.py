@@ -149,6 +149,7 @@ _SIGS = {
     "spm_save_state": (C.c_int, [_P, C.c_char_p]),
     "spm_load_state": (C.c_int, [_P, C.c_char_p]),
     "spm_load_restart": (C.c_int, [_P, C.c_char_p]),
+    "spm_set_time": (C.c_int, [_P, C.c_int, C.c_double, C.c_double]),
     "spm_udf_out_open": (C.c_int, [_P, C.c_char_p]),
     "spm_udf_out_record": (C.c_int, [_P]),
     "spm_udf_out_close": (C.c_int, [_P]),

@@ -1768,6 +1768,17 @@ int spm_get_time(spm_ctx *c, int *ts, double *time) {
     return SPM_OK;
 }
 
+int spm_set_time(spm_ctx *c, int ts, double time, double degree_oblique) {
+    if (!c || ts < 0) return fail(SPM_ERR_ARG, "bad argument");
+    int rc = spm_synchronize(c);
+    if (rc != SPM_OK) return rc;
+    c->ts   = ts;
+    c->time = time;
+    SPM_CUDA_CHECK(cudaMemcpy(c->ts_dev, &c->ts, sizeof(int), cudaMemcpyHostToDevice));
+    if (c->le.enabled) c->le.degree_oblique = degree_oblique;
+    return SPM_OK;
+}
+
 int spm_get_shear_state(spm_ctx *c, double *degree_oblique, double stress[8]) {
     if (!c) return fail(SPM_ERR_ARG, "null context");
     int rc = spm_synchronize(c);

@@ -65,6 +65,36 @@ inline spm_params params_from_globals(int equation) {
     p.rotation    = ROTATION;
     for (int d = 0; d < DIM; d++) p.fix_cell[d] = FIX_CELLxyz[d];
     if (equation == SPM_EQ_LEES_EDWARDS) p.shear_rate = Shear_rate;
+    if (equation == SPM_EQ_SHEAR_NAVIER_STOKES) {
+        p.shear_rate      = Shear_rate;
+        p.shear_ac        = Shear_AC ? 1 : 0;
+        p.shear_frequency = Shear_frequency;
+    }
+    if (Component_Number > 1) {  // species: Particle_spec[0..] in particle order
+        p.n_species = Component_Number;
+        for (int s = 0; s < Component_Number && s < SPM_MAX_SPECIES; s++) {
+            p.species_count[s]          = Particle_Numbers[s];
+            p.species_mass_ratio[s]     = MASS_RATIOS[s];
+            p.species_surface_charge[s] = Surface_charge ? Surface_charge[s] : 0.0;
+        }
+    }
+    if (SW_JANUS) {  // Particle_spec[0]'s propulsion (input.cxx:1403-1470; the slip mode is kept halved, :583)
+        const JP  jp = janus_propulsion[0];
+        const JAX ja = janus_axis[0];
+        p.janus_propulsion = jp == motor ? SPM_JANUS_TUMBLER : jp == slip ? SPM_JANUS_SQUIRMER
+                           : jp == obstacle ? SPM_JANUS_OBSTACLE : SPM_JANUS_OFF;
+        p.janus_axis = ja == x_axis ? SPM_AXIS_X : ja == y_axis ? SPM_AXIS_Y : ja == z_axis ? SPM_AXIS_Z : SPM_AXIS_NONE;
+        for (int d = 0; d < DIM; d++) {
+            p.janus_force[d]  = janus_force[0][d];
+            p.janus_torque[d] = janus_torque[0][d];
+        }
+        p.slip_vel  = janus_slip_vel[0];
+        p.slip_mode = 2.0 * janus_slip_mode[0];
+        p.rotlet_c1 = janus_rotlet_C1[0];
+        p.rotlet_c2 = janus_rotlet_dipole_C2[0];
+        p.slip_tol  = MAX_SLIP_TOL;
+        p.slip_iter = MAX_SLIP_ITER;
+    }
     p.dt        = DT;
     p.precision = SPM_PREC_FP64;
     return p;

@@ -11,12 +11,17 @@
 // sp_3d_ns.cxx:863-874) and before the restart file written after the last
 // step (sp_3d_ns.cxx:974-982).
 //
-// Served: Navier_Stokes and Shear_Navier_Stokes_Lees_Edwards runs of one
-// particle species with spherical particles, not resumed.  For any other run
-// the pointer is left alone and the reference steps on the CPU.  In a
-// Lees-Edwards run the main loop's per-step stress print (Mean_shear_stress,
-// sp_3d_ns.h:247-339) reads CPU-side globals this path does not update;
-// spm_get_shear_state returns that line from the device.
+// Served: Navier_Stokes, Shear_Navier_Stokes and Shear_Navier_Stokes_Lees_
+// Edwards runs of spherical particles (several species, or Janus particles of
+// one species), new or resumed.  A resumed run's first pass of the main loop
+// steps its input state and then restores the saved one on the host
+// (sp_3d_ns.cxx:856-1005); the next call uploads the restored state and its
+// time, the generator keeping the draws of that first step as the
+// reference's does.  For any other run the pointer is left alone and the
+// reference steps on the CPU.  In a sheared run the main loop's per-step
+// stress print (Update_strain, Mean_shear_stress, sp_3d_ns.h:205-339) reads
+// CPU-side arrays this path updates only at frames; spm_get_shear_state
+// returns that line from the device.
 #include <vector>
 
 #include "kapsel_b200_common.h"
@@ -31,6 +36,7 @@ using kapsel_b200::check;
 spm_ctx            *g_run = nullptr;
 int                 g_eq  = SPM_EQ_NAVIER_STOKES;
 std::vector<double> g_rec;
+bool                g_restored = false;
 double              g_body_force[3] = {0.0, 0.0, 0.0};
 
 // Host copies of the state the main loop reads: zeta, uk_dc, the particles,
@@ -49,6 +55,12 @@ void download(double **zeta, double uk_dc[DIM], Particle *p) {
 
 void resident_time_evolution(double **zeta, double uk_dc[DIM], double **f, Particle *p, CTime &jikan) {
     (void)f;
+    if (g_run && RESUMED && !g_restored && jikan.ts == last_ts + 1) {  // the state Force_restore_parameters set
+        check(spm_set_zeta(g_run, zeta[0], zeta[1], uk_dc), "spm_set_zeta");
+        check(spm_set_particles(g_run, kapsel_b200::records(p, g_rec)), "spm_set_particles");
+        check(spm_set_time(g_run, jikan.ts, jikan.time, degree_oblique), "spm_set_time");
+        g_restored = true;
+    }
     if (!g_run) {  // the reference's state after its initial projection
         spm_params prm = kapsel_b200::params_from_globals(g_eq);
         for (int d = 0; d < DIM; d++) prm.body_force[d] = g_body_force[d];
@@ -80,9 +92,13 @@ extern "C" void kapsel_b200_set_body_force(double fx, double fy, double fz) {
 // Called by the program once its initialisation is complete and before its
 // main loop (see the build's Show_output_parameter hook).
 extern "C" void kapsel_b200_go_resident() {
-    if (RESUMED || Component_Number != 1 || SW_PT != spherical_particle || SW_JANUS || SW_WALL != NO_WALL) return;
+    if (SW_PT != spherical_particle || SW_WALL != NO_WALL || PINNING || Component_Number > SPM_MAX_SPECIES ||
+        (SW_JANUS && Component_Number != 1))
+        return;
     if (SW_EQ == Navier_Stokes) {
         g_eq = SPM_EQ_NAVIER_STOKES;
+    } else if (SW_EQ == Shear_Navier_Stokes) {
+        g_eq = SPM_EQ_SHEAR_NAVIER_STOKES;
     } else if (SW_EQ == Shear_Navier_Stokes_Lees_Edwards) {
         g_eq = SPM_EQ_LEES_EDWARDS;
     } else {

@@ -47,3 +47,73 @@ def test_resident_reference_program_matches_reference(gpu, name):
         if "traj_degree_oblique" in z.files:
             assert abs(f["degree_oblique"] - z["traj_degree_oblique"][i]) <= TOL * max(1.0, abs(
                 z["traj_degree_oblique"][i]))
+
+
+def _frames(keys, tmp, name, **kw):
+    dump = os.path.join(tmp, name + ".dump")
+    err = ref_runner.run_reference(keys, dump_path=dump, fields_every=0, timeout=600.0, **kw)
+    return err, ref_runner.read_dump(dump)["frames"]
+
+
+def _same(fa, fb, what):
+    assert [f["ts"] for f in fa] == [f["ts"] for f in fb], what
+    for a, b in zip(fa, fb):
+        for k in ("x", "v", "omega", "q", "f_hydro_previous"):
+            e = rel(a[k], b[k])
+            assert e <= TOL, (what, a["ts"], k, e)
+
+
+def _live_cases():
+    from kapsel3_b200.udf import EQ_SNS, SPMConfig
+    from tests.test_gpu_janus import CASES as JANUS
+    return {
+        "shear_ns_dc_thermostat": SPMConfig(npx=5, npy=5, npz=5, n_particles=3, a=4.0, a_xi=2.0, dt=0.05,
+                                            equation=EQ_SNS, shear_rate=0.02, kbt=1e-4, gts=2, num_snap=5),
+        "two_species_thermostat": SPMConfig(npx=5, npy=5, npz=5, n_particles=5, a=3.5, a_xi=2.0, dt=0.05, kbt=1e-4,
+                                            species=((3, 1.0, 0.0), (2, 2.5, 0.0)), gts=2, num_snap=5),
+        "tumblers": JANUS["tumblers"],
+        "squirmers": JANUS["squirmer_example"],
+    }
+
+
+@pytest.mark.parametrize("name", ["shear_ns_dc_thermostat", "two_species_thermostat", "tumblers", "squirmers"])
+def test_resident_loop_serves_more_runs(gpu, name, tmp_path):
+    """Shear_Navier_Stokes, several species and Janus particles through the
+    resident loop: the same frames as the reference program run alone."""
+    if not ref_runner.available(gpu_resident=True):
+        pytest.skip("oracle/_ref/kapsel_gpu_resident is not built")
+    from kapsel3_b200.udf import make_particles
+    cfg = _live_cases()[name]
+    parts = make_particles(cfg, seed=37, v_sd=1e-3, random_orientation=True)
+    keys = os.path.join(str(tmp_path), "run.keys")
+    write_udf_keys(keys, cfg, parts, out_dir=os.path.join(str(tmp_path), "avs"))
+    _, ref = _frames(keys, str(tmp_path), "ref")
+    err, res = _frames(keys, str(tmp_path), "res", gpu_resident=True, threads=4)
+    assert "resident on the GPU" in err
+    _same(res, ref, name)
+
+
+def test_resident_loop_resumes_from_a_restart_file(gpu, tmp_path):
+    """A resumed run (resume.Calculation = CONTINUE): the reference's first
+    pass steps the input state, restores the saved one, and the resident loop
+    takes the restored state over; the frames equal the reference program's
+    own resumed run, thermostat included."""
+    if not ref_runner.available(gpu_resident=True):
+        pytest.skip("oracle/_ref/kapsel_gpu_resident is not built")
+    from kapsel3_b200.udf import SPMConfig, make_particles, read_udf_keys
+    cfg = SPMConfig(npx=5, npy=5, npz=5, n_particles=4, a=3.5, a_xi=2.0, dt=0.05, kbt=1e-4, gts=1, num_snap=5)
+    parts = make_particles(cfg, seed=43, v_sd=1e-3, random_orientation=True)
+    tmp = str(tmp_path)
+    keys = os.path.join(tmp, "run.keys")
+    write_udf_keys(keys, cfg, parts, out_dir=os.path.join(tmp, "avs"))
+    res = os.path.join(tmp, "restart.keys")
+    ref_runner.run_reference(keys, restart_path=res, timeout=600.0)
+    kv = read_udf_keys(res)
+    kv["output.Num_snap"] = "12"
+    cont = os.path.join(tmp, "continue.keys")
+    with open(cont, "w") as f:
+        f.writelines(f"{k} = {v}\n" for k, v in kv.items())
+    _, ref = _frames(cont, tmp, "ref")
+    err, out = _frames(cont, tmp, "res", gpu_resident=True, threads=4)
+    assert "resident on the GPU" in err and ref and ref[0]["ts"] == 6
+    _same(out, ref, "resumed")
