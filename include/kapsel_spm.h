@@ -189,7 +189,9 @@ int spm_initialize(spm_ctx *ctx, const double *particles_host);
 /* Runs n steps of Time_evolution_hydro (sp_3d_ns.cxx:41-194) or
  * Time_evolution_hydro_OBL (sp_3d_ns.cxx:328-433) on device-resident state.
  * Asynchronous on the context stream; errors raised by kernels surface at the
- * next synchronising call. */
+ * next synchronising call.  Navier_Stokes steps, and Electrolyte steps after
+ * the first, replay a CUDA graph of the step captured on first use (the
+ * environment variable SPM_NO_GRAPH=1 at spm_create keeps direct launches). */
 int spm_step(spm_ctx *ctx, int nsteps);
 int spm_synchronize(spm_ctx *ctx);
 /* Copies state to / from host memory (blocking). */

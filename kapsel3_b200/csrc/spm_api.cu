@@ -1111,7 +1111,7 @@ int step_graphed(spm_ctx *c) {
         const double    tm = c->time;
         const long long ln = c->launches;
         SPM_CUDA_CHECK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-        rc              = step_ns<T>(c);
+        rc              = c->el.enabled ? step_el<T>(c) : step_ns<T>(c);
         cudaGraph_t g   = nullptr;
         cudaError_t e   = cudaStreamEndCapture(c->st, &g);
         c->step_kernels = c->launches - ln;
@@ -1638,14 +1638,19 @@ int spm_initialize(spm_ctx *c, const double *particles_host) {
 int spm_step(spm_ctx *c, int nsteps) {
     if (!c || nsteps < 0) return fail(SPM_ERR_ARG, "bad argument");
     // graph replay: lone Navier_Stokes runs (the slip loop of squirmers reads
-    // its convergence on the host), not while a test switch is armed
-    const bool graph = c->use_graph && !c->pool && !c->prof_on && c->P.equation == SPM_EQ_NAVIER_STOKES &&
-                       c->P.janus_propulsion != SPM_JANUS_SQUIRMER && c->pp64->skip_loads == 0 &&
-                       c->pp32->skip_loads == 0;
+    // its convergence on the host) and Electrolyte runs once their ion fields
+    // are inside the 2/3 box (after the first step), not while a test switch
+    // is armed
+    const bool graphable = c->use_graph && !c->pool && !c->prof_on && c->P.janus_propulsion != SPM_JANUS_SQUIRMER &&
+                           c->pp64->skip_loads == 0 && c->pp32->skip_loads == 0;
     for (int i = 0; i < nsteps; i++) {
+        const bool el    = c->P.equation == SPM_EQ_ELECTROLYTE;
+        const bool graph = graphable && (c->P.equation == SPM_EQ_NAVIER_STOKES || (el && c->el.conc_in_box));
+        if (el) SPM_TRY(el_sync_time(c));
         int rc = graph ? (c->fp64() ? step_graphed<double>(c) : step_graphed<float>(c))
                        : (c->fp64() ? step_impl<double>(c) : step_impl<float>(c));
         if (rc != SPM_OK) return rc;
+        if (el) c->el.time_dev = c->time;  // the step advanced the device's time word alike
     }
     return SPM_OK;
 }
@@ -1772,8 +1777,9 @@ int spm_set_time(spm_ctx *c, int ts, double time, double degree_oblique) {
     if (!c || ts < 0) return fail(SPM_ERR_ARG, "bad argument");
     int rc = spm_synchronize(c);
     if (rc != SPM_OK) return rc;
-    c->ts   = ts;
-    c->time = time;
+    c->ts              = ts;
+    c->time            = time;
+    c->el.time_known   = 0;  // the next Electrolyte step writes the time to the device
     SPM_CUDA_CHECK(cudaMemcpy(c->ts_dev, &c->ts, sizeof(int), cudaMemcpyHostToDevice));
     if (c->le.enabled) c->le.degree_oblique = degree_oblique;
     return SPM_OK;

@@ -32,6 +32,8 @@ struct ELState {
     double  surface_ion_number = 0;// -sum over particles of Surface_charge
     int     init_iters = 0;        // iterations of the last initial-profile loop
     int     conc_in_box = 0;       // the ion fields are zero outside the 2/3 box (pruned inverses apply)
+    int     time_known = 0;        // the device's time word holds time_dev
+    double  time_dev   = 0.0;
     double *dev     = nullptr;     // device scalars (kEl*)
     double *partial = nullptr;     // per-CTA partial sums of the field reductions
 };
@@ -41,8 +43,36 @@ constexpr int kElQSum   = 2;  // sum of |surface charge field|
 constexpr int kElCSum   = 3;  // [3, 4]: (1 - phi) c sums of each species
 constexpr int kElVolume = 5;  // sum of (1 - phi)
 constexpr int kElScratch = 6;  // [6, 8]: sums read by the host in the initial-profile loops
-constexpr int kElScalars = 10;
+constexpr int kElTime    = 9;  // the run's time (advanced on the device every step)
+constexpr int kElField   = 10; // [10, 15]: this step's external field: the k = 0 mode of grad psi (3), the Coulomb force's (3)
+constexpr int kElScalars = 16;
 constexpr double kElTol = 1.e-4;  // TOL of the initial-profile loops (operate_electrolyte.h:21)
+
+// The step's external field from the time on the device, so that a captured
+// step replays with the field of its own time: E_ext NX NY NZ sin(omega t)
+// for the k = 0 mode of the potential's gradient (Add_constant_field_k,
+// fluid_solver.cxx:221-231) and E_ext sin(omega t) for the Coulomb force
+// (Make_Coulomb_force_x_on_fluid, operate_electrolyte.cxx:83-171); sin -> 1
+// under a DC field.
+__global__ void k_el_field(double *dev, double e0, double e1, double e2, int ac, double omega, double nxyz) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const double s   = ac ? sin(omega * dev[kElTime]) : 1.0;
+    double       amp = nxyz;
+    if (ac) amp *= s;
+    const double e[3] = {e0, e1, e2};
+    for (int d = 0; d < 3; d++) {
+        dev[kElField + d]     = e[d] * amp;
+        dev[kElField + 3 + d] = e[d] * s;
+    }
+}
+// time += dt at the end of a step (the host's time advances the same way);
+// k_el_set_time: the host's time after it was set outside a step
+__global__ void k_el_time_advance(double *dev, double dt) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) dev[kElTime] += dt;
+}
+__global__ void k_el_set_time(double *dev, double t) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) dev[kElTime] = t;
+}
 
 // Total_solute[n] = (1 - phi) c sum * DX3 (Count_single_solute)
 __global__ void k_el_total(double *dev, int n, double dx3) {
@@ -321,11 +351,11 @@ __global__ void k_el_poisson(Grid g, cplx<T> *__restrict__ a, double iepsilon, i
 
 // Gradient in k space of s a (A_k2da_k, fft_wrapper.cxx:200-225): g_d =
 // (-k_d s a.im, k_d s a.re); at k = 0 the real parts get -e_d
-// (Add_constant_field_k, fluid_solver.cxx:221-231, e_d = E_ext NX NY NZ or
-// the AC amplitude; 0 without a field).
+// (Add_constant_field_k, fluid_solver.cxx:221-231, e = the step's field
+// words of k_el_field; nullptr: no field).
 template <typename T>
 __global__ void k_el_grad(Grid g, const cplx<T> *__restrict__ a, cplx<T> *__restrict__ g0, cplx<T> *__restrict__ g1,
-                          cplx<T> *__restrict__ g2, double s, int scaled, double e0, double e1, double e2) {
+                          cplx<T> *__restrict__ g2, double s, int scaled, const double *__restrict__ e) {
     const size_t n = g.field_elems_c();
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
         KPoint p;
@@ -339,10 +369,10 @@ __global__ void k_el_grad(Grid g, const cplx<T> *__restrict__ a, cplx<T> *__rest
         cplx<T> d0 = {(T)(-p.kx * im), (T)(p.kx * re)};
         cplx<T> d1 = {(T)(-p.ky * im), (T)(p.ky * re)};
         cplx<T> d2 = {(T)(-p.kz * im), (T)(p.kz * re)};
-        if (idx == 0) {
-            d0.re = (T)((double)d0.re - e0);
-            d1.re = (T)((double)d1.re - e1);
-            d2.re = (T)((double)d2.re - e2);
+        if (idx == 0 && e) {
+            d0.re = (T)((double)d0.re - e[0]);
+            d1.re = (T)((double)d1.re - e[1]);
+            d2.re = (T)((double)d2.re - e[2]);
         }
         g0[idx] = d0, g1[idx] = d1, g2[idx] = d2;
     }
@@ -454,13 +484,15 @@ __global__ void k_el_update(Grid g, cplx<T> *__restrict__ z0p, cplx<T> *__restri
 
 // Coulomb body force on the fluid and its velocity kick
 // (Make_Coulomb_force_x_on_fluid, operate_electrolyte.cxx:83-171, then
-// u += f dt / RHO, sp_3d_ns.cxx:85-96): f_d = charge (-grad_d psi + E_d).
+// u += f dt / RHO, sp_3d_ns.cxx:85-96): f_d = charge (-grad_d psi + E_d),
+// E the step's field words of k_el_field.
 template <typename T>
 __global__ void r_el_coulomb(Grid g, const T *__restrict__ charge, const T *__restrict__ gp0, const T *__restrict__ gp1,
                              const T *__restrict__ gp2, T *__restrict__ u0, T *__restrict__ u1, T *__restrict__ u2,
-                             int e_on, double e0, double e1, double e2, double dmy) {
+                             int e_on, const double *__restrict__ e, double dmy) {
     const size_t rowlen = 2 * (size_t)g.hnzp;
     const size_t n      = (size_t)g.nx * g.ny * rowlen;
+    const double e0 = e_on ? e[0] : 0.0, e1 = e_on ? e[1] : 0.0, e2 = e_on ? e[2] : 0.0;
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
         if ((int)(idx % rowlen) >= g.nz) continue;
         const double q  = (double)charge[idx];

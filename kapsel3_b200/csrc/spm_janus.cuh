@@ -52,14 +52,9 @@ __device__ __forceinline__ double dphi_sin_norm(double x, double radius, double 
 // angle theta from the janus axis e3 of the body frame.
 __device__ __forceinline__ void squirmer_coord(const double *x, const double *q, int axis, double *nr, double *nth,
                                                double *ntau, double &theta) {
-    double e1[3] = {0, 0, 0}, e2[3] = {0, 0, 0}, e3[3] = {0, 0, 0};
-    if (axis == 3) {
-        e1[0] = 1.0, e2[1] = 1.0, e3[2] = 1.0;
-    } else if (axis == 2) {
-        e1[2] = 1.0, e2[0] = 1.0, e3[1] = 1.0;
-    } else {
-        e1[1] = 1.0, e2[2] = 1.0, e3[0] = 1.0;
-    }
+    // e3: the body frame's janus axis (z, y or x)
+    double e3[3] = {0, 0, 0};
+    e3[axis == 3 ? 2 : axis == 2 ? 1 : 0] = 1.0;
     double r[3];
     qtn_rotate_d(q, x, r, true);  // SPACE2BODY
     double norm_r = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);

@@ -301,6 +301,11 @@ class SPMRun:
         N.check(self.L.spm_get_time(self.h, C.byref(ts), C.byref(t)), "spm_get_time")
         return ts.value, t.value
 
+    def set_time(self, ts: int, time: float, degree_oblique: float = 0.0):
+        """Sets the step counter, the time and (Lees-Edwards) degree_oblique
+        of the run, e.g. to continue a run whose state was set by hand."""
+        N.check(self.L.spm_set_time(self.h, int(ts), float(time), float(degree_oblique)), "spm_set_time")
+
     def concentration(self, species: int = 0) -> np.ndarray:
         """k-space concentration of one ion species of an Electrolyte run."""
         a = self._kfield()
