@@ -379,8 +379,9 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
     }
     // rigid bodies (object_type.rigid, input.cxx:1583-1700)
     if (p.rigid) {
-        if (p.equation != SPM_EQ_NAVIER_STOKES && p.equation != SPM_EQ_SHEAR_NAVIER_STOKES)
-            return fail(SPM_ERR_ARG, "rigid bodies are served in Navier_Stokes and Shear_Navier_Stokes runs");
+        if (p.equation != SPM_EQ_NAVIER_STOKES && p.equation != SPM_EQ_SHEAR_NAVIER_STOKES &&
+            p.equation != SPM_EQ_LEES_EDWARDS)
+            return fail(SPM_ERR_ARG, "rigid bodies are served in Navier_Stokes, Shear_Navier_Stokes and Lees-Edwards runs");
         if (p.janus_propulsion != SPM_JANUS_OFF) return fail(SPM_ERR_ARG, "rigid bodies have no janus propulsion");
         if (!p.rotation) return fail(SPM_ERR_ARG, "rigid bodies need ROTATION ON");
         if (p.body_force[0] != 0.0 || p.body_force[1] != 0.0 || p.body_force[2] != 0.0)
@@ -937,7 +938,8 @@ int particle_blocks(spm_ctx *c) { return (c->ph.np + 127) / 128; }
 int lj_forces(spm_ctx *c, const Phys &ph) {
     if (ph.np == 0) return SPM_OK;
     if (!c->lj_list || !lj_cell_list_applies(ph)) {
-        PLAUNCH(c, "p_forces", 0.0, p_forces, (ph.np + 3) / 4, 128, 0, ph, c->ps, 0, 0.0);
+        PLAUNCH(c, "p_forces", 0.0, p_forces, (ph.np + 3) / 4, 128, 0, ph, c->ps, 0, 0.0,
+                c->rigid() ? c->rg.rid : nullptr, c->rigid() ? c->rg.f_lo : nullptr, (const double *)nullptr);
         return SPM_OK;
     }
     const int ncell   = lj_ncell(ph);
@@ -994,7 +996,8 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
             if (c->ph.np == 0) continue;
             auto side_work = [&]() -> int {
                 if (c->rigid())
-                    PLAUNCH(c, "r_position", 0.0, r_position, c->rg.nb, 128, 0, c->ph, c->ps, c->rg, c->ts_dev);
+                    PLAUNCH(c, "r_position", 0.0, r_position, c->rg.nb, 128, 0, c->ph, c->ps, c->rg, c->ts_dev, 0, 0.0,
+                            (const double *)nullptr);
                 else
                     PLAUNCH(c, "p_position", 0.0, p_position, particle_blocks(c), 128, 0, c->ph, c->ps, c->ts_dev, 1);
                 const dim3 sgrid((c->ncells + 127) / 128, c->ph.np);
@@ -1027,8 +1030,9 @@ int step_ns_runs(spm_ctx *L, spm_ctx *const *R, int nr) {
                 c->ph, c->ps.x, c->ps.v, c->ps.omega, c->cells, c->ncells, c->sc_idx, c->sc_w, c->real<T>(PHIS),
                 c->real<T>(U0), c->real<T>(U1), c->real<T>(U2), c->ps.f_hydro, c->ps.torque_hydro);
         if (c->rigid()) {
-            LAUNCH(c, r_collect, c->rg.nb, 128, 0, c->ps, c->rg, c->rfree);
-            LAUNCH(c, r_velocity, c->rg.nb, 128, 0, c->ph, c->ps, c->rg, c->rfree, c->ts_dev);
+            LAUNCH(c, r_collect, c->rg.nb, 128, 0, c->ps, c->rg, c->rfree, 0);
+            LAUNCH(c, r_velocity, c->rg.nb, 128, 0, c->ph, c->ps, c->rg, c->rfree, c->ts_dev, 0, 0.0,
+                   (const double *)nullptr);
         } else if (c->ph.janus_prop == SPM_JANUS_SQUIRMER) {
             SPM_TRY(slip_loop<T>(c));  // lone runs only; leaves the slip field in UP
         } else {
@@ -1529,7 +1533,7 @@ int create_ctx(const spm_params &p, cudaStream_t stream, int pool_cap, spm_ctx *
     }
     if (c->le.enabled) {
         if (dev_alloc((void **)&c->le.dev, sizeof(LEDev)) != cudaSuccess ||
-            dev_alloc((void **)&c->le.ppart, (size_t)np * 6 * sizeof(double)) != cudaSuccess ||
+            dev_alloc((void **)&c->le.ppart, (size_t)np * kLePart * sizeof(double)) != cudaSuccess ||
             dev_alloc((void **)&c->le.partial, (size_t)c->grid_blocks() * sizeof(double)) != cudaSuccess) {
             destroy_ctx(c);
             return fail(SPM_ERR_NOMEM, "Lees-Edwards buffers");

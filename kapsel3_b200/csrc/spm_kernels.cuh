@@ -1035,25 +1035,48 @@ __device__ __forceinline__ double min_image(const Phys &ph, const double *xa, co
     return sqrt(d2);
 }
 
+// PBC_OBL (periodic_boundary.h:26-45): the periodic wrap of x with the
+// Lees-Edwards image (crossing the y boundary shifts x by -+ gam LY) and the
+// x-velocity change -sign Shear_rate_eff LY of that crossing.
+__device__ __forceinline__ double pbc_obl(const Phys &ph, double *x, double gam, double srate) {
+    double sy = x[1];
+    x[1]      = fmod(x[1] + ph.L[1], ph.L[1]);
+    sy -= x[1];
+    int sign = (int)sy;
+    if (sign != 0) sign = sign / abs(sign);
+    x[0] -= (double)sign * gam * ph.L[1];
+    x[0] = fmod(x[0] + ph.L[0], ph.L[0]);
+    x[2] = fmod(x[2] + ph.L[2], ph.L[2]);
+    return -(double)sign * srate * ph.L[1];
+}
+
 // LJ pair forces plus the constant body force (Force, particle_solver.h:88-111;
 // Calc_f_Lennard_Jones_shear_cap_primitive_lnk, md_force.cxx:34-196).  Thread
 // n gathers every pair term acting on particle n with the reference's pair
 // multiplicity, so no atomics are needed.  lj_stress[n] receives particle n's
 // share of sum f_x r_y over the pairs where it is the higher index, as the
 // reference accumulates dev_shear_stress_lj.
+// Rigid bodies (rid != nullptr): pairs of beads of one body are skipped
+// (rigid_chain), f_lo[n] receives the pair forces on n where it is the lower
+// index (for the bodies' torques), and under Lees-Edwards lj_stress[n] takes
+// the bodies' term sum f_x R_y instead, R the image distance of the two
+// bodies' centres xg (rigid_dev_shear_stress_lj, md_force.cxx:252-258).
 // One warp per particle: lanes stride over the partners, then a warp sum.
-__global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift) {
+__global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift, const int *__restrict__ rid,
+                         double *__restrict__ f_lo, const double *__restrict__ xg) {
     const int lane = threadIdx.x & 31;
     const int n    = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (n >= ph.np) return;
     double f[3]   = {0.0, 0.0, 0.0};
+    double fl[3]  = {0.0, 0.0, 0.0};
     double stress = 0.0;
     if (ph.lj_on) {
         for (int m = lane; m < ph.np; m += 32) {
-            if (m == n) continue;
+            if (m == n || (rid && rid[m] == rid[n])) continue;
             const int hi = n > m ? n : m, lo = n > m ? m : n;
             double    r[3], rr;  // r = x_other - x_n (with the periodic image rule)
             int       mult = 1;
+            double    ry_body = 0.0;  // rigid, Lees-Edwards: y image distance of the bodies' centres
             if (all_pairs_le) {
                 // O(N^2) loop with Distance0_OBL(x_lo, x_hi) (md_force.cxx:198-304,
                 // interaction.h:50-72): y image first, then the x shift of the
@@ -1074,6 +1097,10 @@ __global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift) {
                 r[0]            = sg * x12;
                 r[1]            = sg * y12;
                 r[2]            = sg * z12;
+                if (rid && xg) {
+                    ry_body = xg[3 * rid[hi] + 1] - xg[3 * rid[lo] + 1];
+                    ry_body -= (double)nint_d(ry_body / ph.L[1]) * ph.L[1];
+                }
             } else {
                 // cell-list pairs (i > j) with Distance0(x_i, x_j)
                 mult = lj_multiplicity(ph, s.x + 3 * hi, s.x + 3 * lo);
@@ -1088,7 +1115,13 @@ __global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift) {
             if (!(rr < ph.lj_cutoff)) continue;
             const double dmy_r = lj_f(rr, ph);
             for (int d = 0; d < 3; d++) f[d] += (double)mult * (-dmy_r * r[d]);
-            if (n == hi) stress += (double)mult * (-dmy_r * r[0]) * r[1];
+            if (n == hi) {
+                // f_x of the lower-index partner (dmy_fn[0] = dmy_r r[0] here) times r_y, or the bodies' R_y
+                stress += (rid && xg) ? (double)mult * (dmy_r * r[0]) * ry_body
+                                      : (double)mult * (-dmy_r * r[0]) * r[1];
+            } else {
+                for (int d = 0; d < 3; d++) fl[d] += (double)mult * (-dmy_r * r[d]);
+            }
         }
     }
 #pragma unroll
@@ -1097,10 +1130,17 @@ __global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift) {
         f[1] += __shfl_xor_sync(0xffffffffu, f[1], o);
         f[2] += __shfl_xor_sync(0xffffffffu, f[2], o);
         stress += __shfl_xor_sync(0xffffffffu, stress, o);
+        if (f_lo) {
+            fl[0] += __shfl_xor_sync(0xffffffffu, fl[0], o);
+            fl[1] += __shfl_xor_sync(0xffffffffu, fl[1], o);
+            fl[2] += __shfl_xor_sync(0xffffffffu, fl[2], o);
+        }
     }
     if (lane == 0) {
         for (int d = 0; d < 3; d++) s.fr[3 * n + d] += f[d] + ph.body_force[d];
         s.lj_stress[n] = stress;
+        if (f_lo)
+            for (int d = 0; d < 3; d++) f_lo[3 * n + d] = fl[d];
     }
 }
 

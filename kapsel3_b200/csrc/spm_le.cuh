@@ -34,7 +34,7 @@ struct LEState {
     double  degree_oblique = 0.0;
     double  xy_aspect      = 1.0;
     LEDev  *dev            = nullptr;  // device scalars
-    double *ppart          = nullptr;  // per-particle stress partials [Np][6]
+    double *ppart          = nullptr;  // per-particle stress partials [Np][kLePart]
     double *partial        = nullptr;  // per-CTA partial sums of the field reductions
     double  stress_host[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
@@ -561,20 +561,29 @@ __device__ __forceinline__ void block_sumK(double v[K]) {
 // Calc_f_hydro_correct_precision_OBL (md_force.cxx:508-745): force and torque
 // of each particle, and per-particle partial sums of the Hydro_force and
 // Hydro_force_new fields' totals (all that Mean_shear_stress reads of them).
-// ppart[p] = {A, Y, force0, volume, new_p, mdf0/volume * Y}
+// ppart[p] = {A, Y, force0, volume, new_p, mdf0/volume * Y, Yy, Yz} with
+// Y = sum w dry, Yy = sum w dry r_y, Yz = sum w dry r_z over the particle's
+// stencil (dry the cell's y with its image).  Rigid beads (rigid != 0) leave
+// the spheres' extra term out of new_p: r_le_stress_new adds the bodies' one
+// from Yy and Yz once their forces are summed.
+constexpr int kLePart = 8;
+struct LeRhoP {
+    double v[4];  // RHO_particle of each species
+};
 template <typename T>
 __global__ void s_le_hydro_force(Grid g, Phys ph, const double *__restrict__ x, const double *__restrict__ v,
                                  const double *__restrict__ w, const double *__restrict__ mdf,
                                  const int *__restrict__ cells, int ncells, double gam, const LEDev *__restrict__ le,
-                                 double rho_p, const T *__restrict__ phi_sum, const T *__restrict__ c0,
+                                 LeRhoP rho_s, const T *__restrict__ phi_sum, const T *__restrict__ c0,
                                  const T *__restrict__ c1, const T *__restrict__ c2, double *__restrict__ f_hydro,
-                                 double *__restrict__ torque_hydro, double *__restrict__ ppart) {
+                                 double *__restrict__ torque_hydro, double *__restrict__ ppart, int rigid) {
     const int p = blockIdx.x;
     if (p >= ph.np) return;
     const double xp[3] = {x[3 * p], x[3 * p + 1], x[3 * p + 2]};
     const double vp[3] = {v[3 * p], v[3 * p + 1], v[3 * p + 2]};
     const double op[3] = {w[3 * p], w[3 * p + 1], w[3 * p + 2]};
     const double srate = le->srate_eff;
+    const double rho_p = rho_s.v[spec_of(ph, p)];
     double       acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // force 3, torque 3, volume, itrace, A
     for (int m = threadIdx.x; m < ncells; m += blockDim.x) {
         StencilPointLE s;
@@ -608,7 +617,7 @@ __global__ void s_le_hydro_force(Grid g, Phys ph, const double *__restrict__ x, 
     __syncthreads();
     const double volume = tot[6], itrace = tot[7] * (2.0 / 3.0);
     const double sv = -ph.rho * tot[0] / volume;
-    double       acc2[2] = {0.0, 0.0};  // Y, new-stress extra term
+    double       acc2[4] = {0.0, 0.0, 0.0, 0.0};  // Y, new-stress extra term, Yy, Yz
     for (int m = threadIdx.x; m < ncells; m += blockDim.x) {
         StencilPointLE s;
         stencil_point_le(g, ph, xp, cells[m], gam, s);
@@ -619,20 +628,24 @@ __global__ void s_le_hydro_force(Grid g, Phys ph, const double *__restrict__ x, 
         const double sw  = -ph.rho * (tot[4] * s.r[2] - tot[5] * s.r[1]) / itrace;
         acc2[0] += dry * wgt;
         acc2[1] += (sv + sw) * dry * wgt;
+        acc2[2] += dry * wgt * s.r[1];
+        acc2[3] += dry * wgt * s.r[2];
     }
-    block_sumK<2>(acc2);
+    block_sumK<4>(acc2);
     if (threadIdx.x == 0) {
         const double dmy = -ph.dx3 * ph.rho / ph.dt;
         for (int d = 0; d < 3; d++) f_hydro[3 * p + d] = dmy * tot[d];
         if (ph.rotation)
             for (int d = 0; d < 3; d++) torque_hydro[3 * p + d] = dmy * tot[3 + d];
-        double *pp = ppart + 6 * p;
+        double *pp = ppart + kLePart * p;
         pp[0]      = tot[8];
         pp[1]      = acc2[0];
         pp[2]      = tot[0];
         pp[3]      = volume;
-        pp[4]      = tot[8] + acc2[1];
+        pp[4]      = rigid ? tot[8] : tot[8] + acc2[1];
         pp[5]      = mdf[3 * p] / volume * acc2[0];
+        pp[6]      = acc2[2];
+        pp[7]      = acc2[3];
     }
 }
 
@@ -643,7 +656,7 @@ __global__ void k_le_stress_finish(LEDev *le, const double *ppart, const double 
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double A = 0, Y = 0, F = 0, V = 0, Nw = 0, M = 0, L = 0;
     for (int p = 0; p < np; p++) {
-        const double *pp = ppart + 6 * p;
+        const double *pp = ppart + kLePart * p;
         A += pp[0];
         Y += pp[1];
         F += pp[2];
@@ -665,16 +678,7 @@ __global__ void k_le_stress_finish(LEDev *le, const double *ppart, const double 
 __global__ void p_le_wrap(Phys ph, PState s, double gam, const LEDev *__restrict__ le) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= ph.np) return;
-    double *x  = s.x + 3 * n;
-    double  sy = x[1];
-    x[1]       = fmod(x[1] + ph.L[1], ph.L[1]);
-    sy -= x[1];
-    int sign = (int)sy;
-    if (sign != 0) sign = sign / abs(sign);
-    x[0] -= (double)sign * gam * ph.L[1];
-    x[0]             = fmod(x[0] + ph.L[0], ph.L[0]);
-    x[2]             = fmod(x[2] + ph.L[2], ph.L[2]);
-    const double dvx = -(double)sign * le->srate_eff * ph.L[1];
+    const double dvx = pbc_obl(ph, s.x + 3 * n, gam, le->srate_eff);
     s.v[3 * n] += dvx;
     s.v_old[3 * n] += dvx;
 }

@@ -83,7 +83,13 @@ __device__ __host__ __forceinline__ void inverse3(const double *A, double *B) {
 // solver_Rigid_Position (Euler / AB2, rigid.h:333-404) followed by
 // update_Orientation (rigid.h:252-276) and update_Particle_Configuration
 // (rigid.h:171-188).  Euler when the run's step counter is 0.
-__global__ void r_position(Phys ph, PState s, RigidDev R, const int *__restrict__ ts_dev) {
+// Lees-Edwards (le != 0; solver_Rigid_Position_OBL, rigid.h:400-463, and
+// update_Particle_Configuration_OBL, rigid.h:190-210): the centre and every
+// bead take the oblique wrap PBC_OBL of degree_oblique gam, and a crossing of
+// the y boundary shifts vG, vG_old (the centre's) or the bead's v, v_old by
+// -+ Shear_rate_eff LY (*srate).
+__global__ void r_position(Phys ph, PState s, RigidDev R, const int *__restrict__ ts_dev, int le, double gam,
+                           const double *__restrict__ srate) {
     const int b = blockIdx.x;
     if (b >= R.nb) return;
     const int f0 = R.first[b], f1 = R.first[b + 1];
@@ -96,10 +102,17 @@ __global__ void r_position(Phys ph, PState s, RigidDev R, const int *__restrict_
             const double dl = euler ? ph.dt * R.vg[i] : ph.hdt * (3.0 * R.vg[i] - R.vg_old[i]);
             R.xg[i] += dl;
             R.xg_nopbc[i] += dl;
-            R.xg[i] = fmod(R.xg[i] + ph.L[d], ph.L[d]);
-            xg[d]   = R.xg[i];
-            vg[d]   = R.vg[i];
-            wg[d]   = R.wg[i];
+            if (!le) R.xg[i] = fmod(R.xg[i] + ph.L[d], ph.L[d]);
+        }
+        if (le) {
+            const double dvx = pbc_obl(ph, R.xg + 3 * b, gam, *srate);
+            R.vg[3 * b] += dvx;
+            R.vg_old[3 * b] += dvx;
+        }
+        for (int d = 0; d < 3; d++) {
+            xg[d] = R.xg[3 * b + d];
+            vg[d] = R.vg[3 * b + d];
+            wg[d] = R.wg[3 * b + d];
         }
         // MD_solver_orientation_Euler / _AB2 on the first bead
         double *qb = s.q + 4 * f0, *qob = s.q_old + 4 * f0;
@@ -140,11 +153,16 @@ __global__ void r_position(Phys ph, PState s, RigidDev R, const int *__restrict_
             const int i       = 3 * n + d;
             R.gr[i]           = gr[d];
             s.x_previous[i]   = s.x[i];
-            s.x[i]            = fmod(xg[d] + gr[d] + ph.L[d], ph.L[d]);
+            s.x[i]            = le ? xg[d] + gr[d] : fmod(xg[d] + gr[d] + ph.L[d], ph.L[d]);
             s.omega_old[i]    = s.omega[i];
             s.v_old[i]        = s.v[i];
             s.omega[i]        = wg[d];
             s.v[i]            = vg[d] + vr[d];
+        }
+        if (le) {
+            const double dvx = pbc_obl(ph, s.x + 3 * n, gam, *srate);
+            s.v_old[3 * n] += dvx;
+            s.v[3 * n] += dvx;
         }
     }
 }
@@ -156,7 +174,11 @@ __global__ void r_position(Phys ph, PState s, RigidDev R, const int *__restrict_
 // torqueGrs = sum GR x (f_hi - f_lo), where a bead's pair forces as the higher
 // index of a pair enter with their sign and those as the lower index with the
 // opposite sign, as the reference adds GRvecs[j] x dmy_fi for both partners.
-__global__ void r_collect(PState s, RigidDev R, RigidFree fr) {
+// Lees-Edwards (obl != 0; Calc_f_Lennard_Jones_shear_cap_primitive,
+// md_force.cxx:244-258): the reference adds GRvecs x dmy_fn, the force on
+// the lower index, for both partners, so there torqueGrs = sum GR x (f_lo -
+// f_hi).
+__global__ void r_collect(PState s, RigidDev R, RigidFree fr, int obl) {
     const int b = blockIdx.x;
     if (b >= R.nb) return;
     double acc[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -169,7 +191,7 @@ __global__ void r_collect(PState s, RigidDev R, RigidFree fr) {
             acc[d] += fh[d];
             acc[3 + d] += c[d] + th[d];
             acc[6 + d] += fr[d];
-            fs[d] = fr[d] - 2.0 * fl[d];
+            fs[d] = obl ? 2.0 * fl[d] - fr[d] : fr[d] - 2.0 * fl[d];
         }
         cross3(gr, fs, c);
         for (int d = 0; d < 3; d++) acc[9 + d] += c[d];
@@ -211,8 +233,11 @@ __device__ __forceinline__ void omega_update_body(double *wg, const double *torq
 
 // calc_Rigid_VOGs (rigid.h:409-527) and set_Particle_Velocities
 // (rigid.h:213-225), then reset_Forces on the beads (particle_solver.cxx:11-37).
-// Euler when the run's step counter is 0.
-__global__ void r_velocity(Phys ph, PState s, RigidDev R, RigidFree fr, const int *__restrict__ ts_dev) {
+// Euler when the run's step counter is 0.  Lees-Edwards (le != 0;
+// set_Particle_Velocities_OBL, rigid.h:232-250): a bead whose position
+// xG + GR lies across the y boundary gets the v_x shift of that image.
+__global__ void r_velocity(Phys ph, PState s, RigidDev R, RigidFree fr, const int *__restrict__ ts_dev, int le,
+                           double gam, const double *__restrict__ srate) {
     const int b = blockIdx.x;
     if (b >= R.nb) return;
     const int f0 = R.first[b], f1 = R.first[b + 1];
@@ -257,10 +282,16 @@ __global__ void r_velocity(Phys ph, PState s, RigidDev R, RigidFree fr, const in
     for (int n = f0 + threadIdx.x; n < f1; n += blockDim.x) {
         double vr[3];
         cross3(wg, R.gr + 3 * n, vr);
+        double dvx = 0.0;
+        if (le) {
+            double r[3] = {R.xg[3 * b] + R.gr[3 * n], R.xg[3 * b + 1] + R.gr[3 * n + 1],
+                           R.xg[3 * b + 2] + R.gr[3 * n + 2]};
+            dvx = pbc_obl(ph, r, gam, *srate);
+        }
         for (int d = 0; d < 3; d++) {
             const int i               = 3 * n + d;
             s.omega[i]                = wg[d];
-            s.v[i]                    = vg[d] + vr[d];
+            s.v[i]                    = vg[d] + vr[d] + (d == 0 ? dvx : 0.0);
             s.fr_previous[i]          = s.fr[i];
             s.fr[i]                   = 0.0;
             s.f_hydro_previous[i]     = s.f_hydro[i];
@@ -270,6 +301,41 @@ __global__ void r_velocity(Phys ph, PState s, RigidDev R, RigidFree fr, const in
             s.torque_hydro_previous[i] = s.torque_hydro[i];
             s.torque_hydro[i]         = 0.0;
         }
+    }
+}
+
+// Lees-Edwards: the bodies' term of the new hydrodynamic stress
+// (Calc_f_hydro_correct_precision_OBL, md_force.cxx:690-716).  With the
+// body's hydrodynamic force and torque of this step (r_collect), dVg = dt
+// IMass forceGs and dWg the Euler change of wG under torqueGs in the body
+// frame (MD_solver_omega_Euler_update, particle_rotation_solver.h:129-145);
+// each bead's new_p (ppart[4]) gains
+//   RHO_p sum_mesh (dVg_x + dWg_y (GR_z + r_z) - dWg_z (GR_y + r_y)) dry w
+// = RHO_p (Y (dVg_x + dWg_y GR_z - dWg_z GR_y) + dWg_y Yz - dWg_z Yy)
+// from the bead's stencil moments Y, Yy, Yz (ppart[1], [6], [7]).
+__global__ void r_le_stress_new(Phys ph, PState s, RigidDev R, RigidFree fr, double *__restrict__ ppart, int stride) {
+    const int b = blockIdx.x;
+    if (b >= R.nb) return;
+    const int f0 = R.first[b], f1 = R.first[b + 1];
+    __shared__ double dv, dw[3];
+    if (threadIdx.x == 0) {
+        dv = ph.dt * R.imass[b] * R.fg[3 * b];
+        const double *q = s.q + 4 * f0;
+        double        wb[3], tb[3], d[3];
+        qtn_rotate_d(q, R.wg + 3 * b, wb, true);
+        qtn_rotate_d(q, R.tg + 3 * b, tb, true);
+        const double Ib[3] = {R.Ibody[9 * b + 0], R.Ibody[9 * b + 4], R.Ibody[9 * b + 8]};
+        d[0] = (ph.dt / Ib[0]) * (tb[0] + (Ib[1] - Ib[2]) * wb[1] * wb[2]);
+        d[1] = (ph.dt / Ib[1]) * (tb[1] + (Ib[2] - Ib[0]) * wb[2] * wb[0]);
+        d[2] = (ph.dt / Ib[2]) * (tb[2] + (Ib[0] - Ib[1]) * wb[0] * wb[1]);
+        qtn_rotate_d(q, d, dw, false);
+    }
+    __syncthreads();
+    const double rho_p = fr.mr[R.spec[b]] * ph.rho;
+    for (int n = f0 + threadIdx.x; n < f1; n += blockDim.x) {
+        double       *pp = ppart + (size_t)stride * n;
+        const double *gr = R.gr + 3 * n;
+        pp[4] += rho_p * (pp[1] * (dv + dw[1] * gr[2] - dw[2] * gr[1]) + dw[1] * pp[7] - dw[2] * pp[6]);
     }
 }
 

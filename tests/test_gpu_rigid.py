@@ -164,3 +164,71 @@ def test_rigid_bodies_under_sustained_shear_match_the_reference(gpu, ac, tmp_pat
                 assert rel(p[k], fr[k]) < 1e-10, (fr["ts"], k, rel(p[k], fr[k]))
             z, _ = run.zeta()
             assert rel(z, fr["zeta"]) < 1e-10, (fr["ts"], "zeta")
+
+
+def _rigid_le_case(kbt):
+    """Two bent three-bead bodies in a 32^3 Lees-Edwards box: body 0 reaches
+    over the y boundary and its centre crosses it in the first steps (vG_y
+    0.5), one bead of body 1 sits 1.08 SIGMA from a bead of body 0 (inside
+    the WCA cutoff), so the bodies' Lennard-Jones force, torque and stress
+    act from the first step."""
+    import dataclasses
+
+    from kapsel3_b200.udf import EQ_LE
+
+    cfg, _, _ = load("rigid_32_free_gravity")
+    cfg = dataclasses.replace(cfg, equation=EQ_LE, shear_rate=0.05, rigid_gravity=(0.0, 0.0, 0.0), kbt=kbt,
+                              rigid=((3, 2, 1.5, "free", (0.0, 0.5, 0.0), (0.0, 0.0, 0.02)),), gts=1, num_snap=8)
+    s, h = 3.6, 3.6 * np.sin(np.deg2rad(60.0))
+    a0 = np.array([10.0, 30.94, 16.0])
+    body0 = [a0, a0 + [s, 0.0, 0.0], a0 + [s + s / 2, h, 0.0]]
+    b0 = a0 + [0.0, 0.0, 1.08 * 6.0]
+    body1 = [b0, b0 + [-s, 0.0, 0.0], b0 + [-s - s / 2, -h, 0.0]]
+    x = np.array(body0 + body1)
+    n = len(x)
+    parts = dict(x=x, v=np.zeros((n, 3)), q=np.tile(np.array([1.0, 0.0, 0.0, 0.0]), (n, 1)), omega=np.zeros((n, 3)))
+    return cfg, parts
+
+
+@pytest.mark.skipif(not __import__("oracle.ref_runner", fromlist=["x"]).available(),
+                    reason="reference program not built (oracle/_ref)")
+@pytest.mark.parametrize("kbt", [0.0, 1e-4])
+def test_rigid_bodies_under_lees_edwards_match_the_reference(gpu, kbt, tmp_path):
+    """Rigid bodies in a Lees-Edwards box (as the reference's
+    Examples/08/helixes_shear0005.udf; solver_Rigid_Position_OBL,
+    set_Particle_Velocities_OBL, the bodies' LJ and hydrodynamic stress): the
+    reference program's particles, degree_oblique and retained zeta after
+    every step within 1e-10, and every column of its stress line."""
+    from kapsel3_b200.udf import write_udf_keys
+    from oracle import ref_runner
+    from tests.golden_util import retained
+
+    cfg, parts = _rigid_le_case(kbt)
+    keys, dump = str(tmp_path / "in.keys"), str(tmp_path / "d.bin")
+    write_udf_keys(keys, cfg, parts, out_dir=str(tmp_path / "avs"))
+    err = ref_runner.run_reference(keys, dump, fields_every=1, timeout=600)
+    frames = ref_runner.read_dump(dump)["frames"]
+    lines = [[float(v) for v in l.split()] for l in err.splitlines()
+             if l and not l.startswith("#") and len(l.split()) == 12]
+    # stress-line columns <- shear_state() entries (Mean_shear_stress, sp_3d_ns.h:296-339)
+    cols = {"shear_rate": (1, 0), "strain": (3, 1), "lj": (4, 2), "hydro_old": (5, 3), "hydro_new": (6, 4),
+            "reynolds": (7, 5), "fluid": (8, 6), "apparent": (10, 7)}
+    assert any(abs(l[4]) > 0 for l in lines), "the bodies' LJ stress never acted"
+    crossed = False
+    with SPMRun(cfg) as run:
+        run.initialize(parts)
+        for fr in frames:
+            if fr["ts"] > 0:
+                run.step(1)
+                deg, st = run.shear_state()
+                assert abs(deg - fr["degree_oblique"]) < 1e-13
+                ref = lines[fr["ts"] - 1]
+                for k, (ci, si) in cols.items():
+                    assert abs(st[si] - ref[ci]) <= 6e-8 * abs(ref[ci]) + 1e-14, (fr["ts"], k, st[si], ref[ci])
+            p = run.particles()
+            for k in ("x", "v", "omega", "q", "f_hydro_previous"):
+                assert rel(p[k], fr[k]) < 1e-10, (fr["ts"], k, rel(p[k], fr[k]))
+            crossed |= bool(run.rigid_bodies()["xg"][0][1] < 16.0)
+            z, _ = run.zeta()
+            assert rel(retained(cfg, z), retained(cfg, fr["zeta"])) < 1e-10, (fr["ts"], "zeta")
+    assert crossed, "body 0's centre did not cross the y boundary"
