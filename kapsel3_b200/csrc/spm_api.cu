@@ -345,6 +345,9 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
     if (p.equation != SPM_EQ_NAVIER_STOKES && p.equation != SPM_EQ_LEES_EDWARDS && p.equation != SPM_EQ_ELECTROLYTE &&
         p.equation != SPM_EQ_SHEAR_NAVIER_STOKES)
         return fail(SPM_ERR_ARG, "bad equation");
+    if (p.rigid && p.equation != SPM_EQ_NAVIER_STOKES && p.equation != SPM_EQ_SHEAR_NAVIER_STOKES &&
+        p.equation != SPM_EQ_LEES_EDWARDS)
+        return fail(SPM_ERR_ARG, "rigid bodies are served in Navier_Stokes, Shear_Navier_Stokes and Lees-Edwards runs");
     if (p.equation == SPM_EQ_SHEAR_NAVIER_STOKES && (p.shear_ac < 0 || p.shear_ac > 1))
         return fail(SPM_ERR_ARG, "shear_ac must be 0 (DC) or 1 (AC)");
     if (p.equation == SPM_EQ_ELECTROLYTE) {
@@ -379,9 +382,6 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
     }
     // rigid bodies (object_type.rigid, input.cxx:1583-1700)
     if (p.rigid) {
-        if (p.equation != SPM_EQ_NAVIER_STOKES && p.equation != SPM_EQ_SHEAR_NAVIER_STOKES &&
-            p.equation != SPM_EQ_LEES_EDWARDS)
-            return fail(SPM_ERR_ARG, "rigid bodies are served in Navier_Stokes, Shear_Navier_Stokes and Lees-Edwards runs");
         if (p.janus_propulsion != SPM_JANUS_OFF) return fail(SPM_ERR_ARG, "rigid bodies have no janus propulsion");
         if (!p.rotation) return fail(SPM_ERR_ARG, "rigid bodies need ROTATION ON");
         if (p.body_force[0] != 0.0 || p.body_force[1] != 0.0 || p.body_force[2] != 0.0)

@@ -76,7 +76,7 @@ def test_rigid_udf_round_trip(tmp_path, writer):
 
 
 @pytest.mark.parametrize("change, message", [
-    (dict(equation="Shear_Navier_Stokes_Lees_Edwards", shear_rate=0.01), b"Navier_Stokes runs"),
+    (dict(equation="Electrolyte", surface_charge=-1.0, valency=(1.0, 0.0), kbt=1.0), b"Lees-Edwards runs"),
     (dict(rotation=False), b"ROTATION ON"),
     (dict(body_force=(1e-3, 0.0, 0.0)), b"no constant body force"),
     (dict(rigid_gravity=(1e-3, 1e-3, 0.0)), b"one axis"),
@@ -134,10 +134,10 @@ def _rigid_examples():
 def test_reference_rigid_examples_pass_the_checks():
     """Every rigid example input of the reference parses unless it switches
     on a force outside the step (Examples/12: a flat wall and Quincke
-    rotation); the Navier_Stokes and Shear_Navier_Stokes ones pass the
-    library's checks (gravity included), the Lees-Edwards one is refused
-    with a message."""
-    ns = 0
+    rotation); the others, Navier_Stokes, Shear_Navier_Stokes and the
+    Lees-Edwards one (Examples/08/helixes_shear0005.udf), pass the library's
+    checks (gravity included)."""
+    ns = le = 0
     for f in _rigid_examples():
         p = N.SpmParams()
         kv = read_udf(f)
@@ -147,9 +147,7 @@ def test_reference_rigid_examples_pass_the_checks():
             continue
         assert N.lib().spm_params_from_udf(f.encode(), C.byref(p), None, 0) == 0, f
         rc, nbytes = _bytes(p)
-        if p.equation in (N.SPM_EQ_NAVIER_STOKES, N.SPM_EQ_SHEAR_NAVIER_STOKES):
-            assert rc == 0 and nbytes > 0, (f, N.lib().spm_last_error())
-            ns += 1
-        else:
-            assert rc == N.SPM_ERR_ARG and b"Navier_Stokes runs" in N.lib().spm_last_error(), f
-    assert ns >= 6
+        assert rc == 0 and nbytes > 0, (f, N.lib().spm_last_error())
+        ns += p.equation in (N.SPM_EQ_NAVIER_STOKES, N.SPM_EQ_SHEAR_NAVIER_STOKES)
+        le += p.equation == N.SPM_EQ_LEES_EDWARDS
+    assert ns >= 6 and le >= 1
