@@ -229,6 +229,12 @@ int spm_get_shear_state(spm_ctx *ctx, double *degree_oblique, double stress[8]);
  * (0: the counterion of a saltfree run or the positive ion; 1: the negative
  * ion of a salt run), in the reference's r2c layout (Concentration[n]). */
 int spm_get_concentration(spm_ctx *ctx, int species, double *conc_k);
+/* Electrolyte runs: sets the k-space concentration of ion species `species`
+ * (the reference's Concentration[n], r2c layout) and its Total_solute, the
+ * amount Rescale_solute keeps outside the particles (solute_rhs.cxx:91-116;
+ * Count_solute_each of the initial profile, solute_rhs.h:124-137): the state
+ * a host that initialised the ions itself hands over. */
+int spm_set_solute(spm_ctx *ctx, int species, const double *conc_k, double total_solute);
 /* Checkpoint / restart (the reference's restart files, resume.cxx:10-74,
  * 381-588): writes, or reads back into a context created with the same
  * parameters, every piece of device state the next steps read (zeta with its

@@ -146,6 +146,7 @@ _SIGS = {
     "spm_get_time": (C.c_int, [_P, C.POINTER(C.c_int), _D]),
     "spm_get_shear_state": (C.c_int, [_P, _D, _D]),
     "spm_get_concentration": (C.c_int, [_P, C.c_int, _D]),
+    "spm_set_solute": (C.c_int, [_P, C.c_int, _D, C.c_double]),
     "spm_save_state": (C.c_int, [_P, C.c_char_p]),
     "spm_load_state": (C.c_int, [_P, C.c_char_p]),
     "spm_load_restart": (C.c_int, [_P, C.c_char_p]),

@@ -35,7 +35,7 @@ inline int log2_exact(int n, const char *axis) {
 }
 
 // spm_params of the run the reference's globals describe, for `equation`
-// (SPM_EQ_NAVIER_STOKES or SPM_EQ_LEES_EDWARDS), FP64, one particle species.
+// (the SPM_EQ_* the program's SW_EQ maps to), FP64.
 inline spm_params params_from_globals(int equation) {
     if (spm_params_size() != sizeof(spm_params)) {
         fprintf(stderr, "kapsel_b200: libkapsel_spm was built from another kapsel_spm.h (spm_params %zu bytes, "
@@ -69,6 +69,25 @@ inline spm_params params_from_globals(int equation) {
         p.shear_rate      = Shear_rate;
         p.shear_ac        = Shear_AC ? 1 : 0;
         p.shear_frequency = Shear_frequency;
+    }
+    if (equation == SPM_EQ_ELECTROLYTE) {  // constitutive_eq.Electrolyte (input.cxx:834-930)
+        p.dielectric     = Dielectric_cst;
+        p.init_pb        = Poisson_Boltzmann ? 1 : 0;
+        p.salt           = N_spec == 2 ? 1 : 0;
+        p.surface_charge = Surface_charge ? Surface_charge[0] : 0.0;
+        if (p.salt) {
+            p.valency[0]   = Valency_positive_ion;
+            p.valency[1]   = Valency_negative_ion;
+            p.onsager[0]   = Onsager_coeff_positive_ion;
+            p.onsager[1]   = Onsager_coeff_negative_ion;
+            p.debye_length = Debye_length;
+        } else {
+            p.valency[0] = Valency_counterion;
+            p.onsager[0] = Onsager_coeff_counterion;
+        }
+        p.e_field = External_field ? (AC ? 2 : 1) : 0;
+        for (int d = 0; d < DIM; d++) p.e_ext[d] = E_ext[d];
+        p.e_frequency = AC ? Frequency : 0.0;
     }
     if (Component_Number > 1) {  // species: Particle_spec[0..] in particle order
         p.n_species = Component_Number;

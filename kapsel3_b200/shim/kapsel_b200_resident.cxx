@@ -11,9 +11,12 @@
 // sp_3d_ns.cxx:863-874) and before the restart file written after the last
 // step (sp_3d_ns.cxx:974-982).
 //
-// Served: Navier_Stokes, Shear_Navier_Stokes and Shear_Navier_Stokes_Lees_
-// Edwards runs of spherical particles (several species, or Janus particles of
-// one species), new or resumed.  A resumed run's first pass of the main loop
+// Served: Navier_Stokes, Shear_Navier_Stokes, Shear_Navier_Stokes_Lees_
+// Edwards and Electrolyte runs of spherical particles (several species, or
+// Janus particles of one species), new or resumed; an Electrolyte run hands
+// over its ion concentrations and Total_solute with the rest, and gets the
+// concentrations back at frames (Output_charge_field_data,
+// Electrolyte_free_energy) and for its restart file.  A resumed run's first pass of the main loop
 // steps its input state and then restores the saved one on the host
 // (sp_3d_ns.cxx:856-1005); the next call uploads the restored state and its
 // time, the generator keeping the draws of that first step as the
@@ -27,7 +30,9 @@
 #include "kapsel_b200_common.h"
 
 extern void (*Time_evolution)(double **zeta, double uk_dc[DIM], double **f, Particle *p, CTime &jikan);
-extern double *phi;
+extern double  *phi;
+extern double **Concentration;  // solute_rhs.cxx:16
+extern double  *Total_solute;   // solute_rhs.h:17
 
 namespace {
 
@@ -47,10 +52,19 @@ void download(double **zeta, double uk_dc[DIM], Particle *p) {
     check(spm_get_particles(g_run, g_rec.data()), "spm_get_particles");
     kapsel_b200::unpack_records(g_rec.data(), p);
     if (phi) check(spm_get_phi(g_run, phi), "spm_get_phi");
+    if (g_eq == SPM_EQ_ELECTROLYTE)
+        for (int n = 0; n < N_spec; n++) check(spm_get_concentration(g_run, n, Concentration[n]), "spm_get_concentration");
     if (g_eq == SPM_EQ_LEES_EDWARDS) {
         double stress[8];
         check(spm_get_shear_state(g_run, &degree_oblique, stress), "spm_get_shear_state");
     }
+}
+
+// Electrolyte: the ions as the reference initialised (or restored) them
+void upload_solute() {
+    if (g_eq != SPM_EQ_ELECTROLYTE) return;
+    for (int n = 0; n < N_spec; n++)
+        check(spm_set_solute(g_run, n, Concentration[n], Total_solute[n]), "spm_set_solute");
 }
 
 void resident_time_evolution(double **zeta, double uk_dc[DIM], double **f, Particle *p, CTime &jikan) {
@@ -58,6 +72,7 @@ void resident_time_evolution(double **zeta, double uk_dc[DIM], double **f, Parti
     if (g_run && RESUMED && !g_restored && jikan.ts == last_ts + 1) {  // the state Force_restore_parameters set
         check(spm_set_zeta(g_run, zeta[0], zeta[1], uk_dc), "spm_set_zeta");
         check(spm_set_particles(g_run, kapsel_b200::records(p, g_rec)), "spm_set_particles");
+        upload_solute();
         check(spm_set_time(g_run, jikan.ts, jikan.time, degree_oblique), "spm_set_time");
         g_restored = true;
     }
@@ -67,6 +82,7 @@ void resident_time_evolution(double **zeta, double uk_dc[DIM], double **f, Parti
         check(spm_create(&prm, nullptr, &g_run), "spm_create");
         check(spm_set_zeta(g_run, zeta[0], zeta[1], uk_dc), "spm_set_zeta");
         check(spm_set_particles(g_run, kapsel_b200::records(p, g_rec)), "spm_set_particles");
+        upload_solute();
     }
     if (jikan.dt_fluid != DT) {
         fprintf(stderr, "kapsel_b200: dt changed during the run (%g != %g)\n", jikan.dt_fluid, DT);
@@ -101,7 +117,16 @@ extern "C" void kapsel_b200_go_resident() {
         g_eq = SPM_EQ_SHEAR_NAVIER_STOKES;
     } else if (SW_EQ == Shear_Navier_Stokes_Lees_Edwards) {
         g_eq = SPM_EQ_LEES_EDWARDS;
+    } else if (SW_EQ == Electrolyte) {
+        g_eq = SPM_EQ_ELECTROLYTE;
     } else {
+        return;
+    }
+    // a run the library refuses stays on the CPU
+    spm_params prm = kapsel_b200::params_from_globals(g_eq);
+    size_t     bytes = 0;
+    if (spm_device_bytes(&prm, &bytes) != SPM_OK) {
+        fprintf(stderr, "# kapsel_b200: time evolution stays on the CPU: %s\n", spm_last_error());
         return;
     }
     Time_evolution = resident_time_evolution;

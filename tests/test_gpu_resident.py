@@ -49,9 +49,9 @@ def test_resident_reference_program_matches_reference(gpu, name):
                 z["traj_degree_oblique"][i]))
 
 
-def _frames(keys, tmp, name, **kw):
+def _frames(keys, tmp, name, fields_every=0, **kw):
     dump = os.path.join(tmp, name + ".dump")
-    err = ref_runner.run_reference(keys, dump_path=dump, fields_every=0, timeout=600.0, **kw)
+    err = ref_runner.run_reference(keys, dump_path=dump, fields_every=fields_every, timeout=600.0, **kw)
     return err, ref_runner.read_dump(dump)["frames"]
 
 
@@ -117,3 +117,34 @@ def test_resident_loop_resumes_from_a_restart_file(gpu, tmp_path):
     err, out = _frames(cont, tmp, "res", gpu_resident=True, threads=4)
     assert "resident on the GPU" in err and ref and ref[0]["ts"] == 6
     _same(out, ref, "resumed")
+
+
+@pytest.mark.parametrize("name", ["salt_ac", "saltfree_dc"])
+def test_resident_loop_serves_electrolyte_runs(gpu, name, tmp_path):
+    """Electrolyte runs through the resident loop: the reference initialises
+    the ions (salt with an AC field; counterions under a DC field), hands
+    them over with Total_solute
+    (spm_set_solute) and gets them back at every frame; the frames' particles,
+    retained zeta and k-space concentrations equal the reference program's own
+    run within 1e-10."""
+    if not ref_runner.available(gpu_resident=True):
+        pytest.skip("oracle/_ref/kapsel_gpu_resident is not built")
+    import dataclasses
+
+    from kapsel3_b200.udf import make_particles
+    from tests.golden_util import retained
+    from tests.test_gpu_electrolyte import CASES as EL
+
+    cfg = dataclasses.replace(EL[name], gts=2, num_snap=4)
+    parts = make_particles(cfg, seed=47, v_sd=1e-3, random_orientation=True)
+    keys = os.path.join(str(tmp_path), "run.keys")
+    write_udf_keys(keys, cfg, parts, out_dir=os.path.join(str(tmp_path), "avs"))
+    _, ref = _frames(keys, str(tmp_path), "ref", fields_every=1)
+    err, res = _frames(keys, str(tmp_path), "res", fields_every=1, gpu_resident=True, threads=4)
+    assert "resident on the GPU" in err
+    _same(res, ref, name)
+    for a, b in zip(res, ref):
+        assert rel(retained(cfg, a["zeta"]), retained(cfg, b["zeta"])) <= TOL, (name, a["ts"], "zeta")
+        assert a["conc"].shape == b["conc"].shape
+        for n in range(b["conc"].shape[0]):
+            assert rel(a["conc"][n], b["conc"][n]) <= TOL, (name, a["ts"], "conc", n)
