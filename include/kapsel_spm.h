@@ -47,6 +47,12 @@ extern "C" {
 /* Per rigid body: xGs[3], xGs without the periodic wrap[3], velocityGs[3],
  * omegaGs[3] (space frame), Rigid_Masses, the diagonal of Rigid_Moments_body[3] */
 #define SPM_RIGID_WORDS 16
+/* The whole state of a rigid body (spm_get_rigid_state): xGs, xGs_nopbc,
+ * xGs_previous, velocityGs, velocityGs_old, omegaGs, omegaGs_old, forceGs,
+ * forceGrs, torqueGs, torqueGrs, forceGs_previous, forceGrs_previous,
+ * torqueGs_previous, torqueGrs_previous (3 each, space frame), then
+ * Rigid_Moments and Rigid_IMoments (9 each, row-major). */
+#define SPM_RIGID_STATE_WORDS 63
 
 #define SPM_EQ_NAVIER_STOKES 0  /* constitutive_eq.type = Navier_Stokes */
 #define SPM_EQ_LEES_EDWARDS 1   /* Shear_Navier_Stokes_Lees_Edwards */
@@ -200,6 +206,14 @@ int spm_get_particles(spm_ctx *ctx, double *particles_host);
  * (SPM_RIGID_WORDS doubles per body; synchronising). */
 int spm_rigid_count(spm_ctx *ctx, int *n);
 int spm_get_rigid(spm_ctx *ctx, double *bodies);
+/* The whole rigid state (SPM_RIGID_STATE_WORDS doubles per body) and every
+ * bead's offset from its body's centre (6 doubles per bead: GRvecs, then
+ * GRvecs_body), to and from host memory (synchronising).  A host that keeps
+ * the reference's rigid globals (rigid.h; the resident time evolution)
+ * reads them back for its output frames and restart file, and hands over a
+ * state it set itself after spm_initialize. */
+int spm_get_rigid_state(spm_ctx *ctx, double *bodies, double *offsets);
+int spm_set_rigid_state(spm_ctx *ctx, const double *bodies, const double *offsets);
 int spm_set_particles(spm_ctx *ctx, const double *particles_host);
 int spm_get_zeta(spm_ctx *ctx, double *zeta0, double *zeta1, double uk_dc[3]);
 int spm_set_zeta(spm_ctx *ctx, const double *zeta0, const double *zeta1, const double uk_dc[3]);

@@ -20,6 +20,7 @@ SPM_ERR_DEVICE = 4
 SPM_ERR_NO_DEVICE = 5
 SPM_PARTICLE_WORDS = 44
 SPM_RIGID_WORDS = 16
+SPM_RIGID_STATE_WORDS = 63
 SPM_EQ_NAVIER_STOKES = 0
 SPM_EQ_LEES_EDWARDS = 1
 SPM_EQ_ELECTROLYTE = 2
@@ -180,6 +181,8 @@ _SIGS = {
     "spm_profile_kernels": (C.c_int, [_P, C.c_int, C.c_char_p, C.c_size_t]),
     "spm_rigid_count": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "spm_get_rigid": (C.c_int, [_P, _D]),
+    "spm_get_rigid_state": (C.c_int, [_P, _D, _D]),
+    "spm_set_rigid_state": (C.c_int, [_P, _D, _D]),
     "spm_make_f_particle_dt_sole_noalloc": (C.c_int, [_P] * 10 + [C.c_int, C.c_int, C.c_int, _P]),
     "spm_pool_device_bytes": (C.c_int, [C.POINTER(SpmParams), C.c_int, C.POINTER(C.c_size_t),
                                         C.POINTER(C.c_size_t)]),

@@ -1710,6 +1710,20 @@ int spm_get_rigid(spm_ctx *c, double *bodies) {
     return rigid_download(c, bodies);
 }
 
+int spm_get_rigid_state(spm_ctx *c, double *bodies, double *offsets) {
+    if (!c || !c->rigid() || !bodies || !offsets) return fail(SPM_ERR_ARG, "bad argument (no rigid bodies)");
+    int rc = spm_synchronize(c);
+    if (rc != SPM_OK) return rc;
+    return rigid_state_io(c, bodies, offsets, true);
+}
+
+int spm_set_rigid_state(spm_ctx *c, const double *bodies, const double *offsets) {
+    if (!c || !c->rigid() || !bodies || !offsets) return fail(SPM_ERR_ARG, "bad argument (no rigid bodies)");
+    int rc = spm_synchronize(c);
+    if (rc != SPM_OK) return rc;
+    return rigid_state_io(c, const_cast<double *>(bodies), const_cast<double *>(offsets), false);
+}
+
 int spm_set_particles(spm_ctx *c, const double *rec) {
     if (!c || (!rec && c->ph.np > 0)) return fail(SPM_ERR_ARG, "bad argument");
     return upload_particles(c, rec, false);

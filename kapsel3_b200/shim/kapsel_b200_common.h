@@ -89,7 +89,28 @@ inline spm_params params_from_globals(int equation) {
         for (int d = 0; d < DIM; d++) p.e_ext[d] = E_ext[d];
         p.e_frequency = AC ? Frequency : 0.0;
     }
-    if (Component_Number > 1) {  // species: Particle_spec[0..] in particle order
+    if (SW_PT == rigid) {  // Rigid_spec[0..] (input.cxx:1583-1700) and switch.free_rigid (:1961-2008)
+        p.rigid = 1;
+        for (int s = 0; s < Component_Number && s < SPM_MAX_SPECIES; s++) {
+            p.rigid_beads[s] = Beads_Numbers[s];
+            p.rigid_count[s] = Chain_Numbers[s];
+            for (int d = 0; d < DIM; d++) {
+                p.rigid_free[s][d]     = Rigid_Motions_vel[s][d];
+                p.rigid_free[s][3 + d] = Rigid_Motions_omega[s][d];
+                p.rigid_velocity[s][d] = Rigid_Velocities[s][d];
+                p.rigid_omega[s][d]    = Rigid_Omegas[s][d];
+            }
+        }
+    }
+    if (G != 0.0) {  // Add_f_gravity (md_force.cxx:306-324): on the bodies, or a constant force on the spheres
+        if (SW_PT == rigid) {
+            p.rigid_gravity[G_direction] = G;
+        } else {
+            const double R = A * DX;
+            p.body_force[G_direction] = -(G * RHO * 4.0 / 3.0 * M_PI * R * R * R) * (MASS_RATIOS[0] - 1.0);
+        }
+    }
+    if (Component_Number > 1) {  // species: Particle_spec[0..] (Rigid_spec[0..]) in particle order
         p.n_species = Component_Number;
         for (int s = 0; s < Component_Number && s < SPM_MAX_SPECIES; s++) {
             p.species_count[s]          = Particle_Numbers[s];

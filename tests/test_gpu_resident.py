@@ -25,7 +25,8 @@ TOL = 1e-10
 
 
 @pytest.mark.parametrize("name", ["c1_32_two_spheres_body_force", "thermostat_32_four_spheres",
-                                  "le_32_boundary_crossing"])
+                                  "le_32_boundary_crossing", "rigid_32_free_gravity", "rigid_32_fixed_motion",
+                                  "rigid_species_dof_thermostat"])
 def test_resident_reference_program_matches_reference(gpu, name):
     if not ref_runner.available(gpu_resident=True):
         pytest.skip("oracle/_ref/kapsel_gpu_resident is not built (make -C oracle/ref_build gpu)")
@@ -148,3 +149,26 @@ def test_resident_loop_serves_electrolyte_runs(gpu, name, tmp_path):
         assert a["conc"].shape == b["conc"].shape
         for n in range(b["conc"].shape[0]):
             assert rel(a["conc"][n], b["conc"][n]) <= TOL, (name, a["ts"], "conc", n)
+
+
+def test_resident_loop_applies_gravity_to_heavy_spheres(gpu, tmp_path):
+    """Spheres heavier than the fluid under gravity (gravity.G, G_direction,
+    MASS_RATIO 2): the resident loop maps Add_f_gravity's force on each
+    sphere (md_force.cxx:306-315) and its frames equal the reference
+    program's own."""
+    if not ref_runner.available(gpu_resident=True):
+        pytest.skip("oracle/_ref/kapsel_gpu_resident is not built")
+    from kapsel3_b200.udf import SPMConfig, make_particles, read_udf_keys
+    cfg = SPMConfig(npx=5, npy=5, npz=5, n_particles=3, a=3.5, a_xi=2.0, dt=0.05, mass_ratio=2.0, gts=2, num_snap=4)
+    parts = make_particles(cfg, seed=53, v_sd=1e-3, random_orientation=True)
+    keys = os.path.join(str(tmp_path), "run.keys")
+    write_udf_keys(keys, cfg, parts, out_dir=os.path.join(str(tmp_path), "avs"))
+    kv = read_udf_keys(keys)
+    kv["gravity.G"], kv["gravity.G_direction"] = "0.002", "-Y"
+    with open(keys, "w") as f:
+        f.writelines(f"{k} = {v}\n" for k, v in kv.items())
+    _, ref = _frames(keys, str(tmp_path), "ref")
+    err, res = _frames(keys, str(tmp_path), "res", gpu_resident=True, threads=4)
+    assert "resident on the GPU" in err
+    _same(res, ref, "gravity")
+    assert abs(ref[-1]["v"][:, 1]).max() > 1e-4  # the spheres sink along -y
