@@ -848,29 +848,53 @@ __global__ void s_hydro_force_cached(Grid g, Phys ph, const double *__restrict__
     double       res[3];
     particle_residue(g, xp, res);
     double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int m = threadIdx.x; m < ncells; m += blockDim.x) {
-        const size_t o  = (size_t)p * ncells + m;
-        const int    id = sc_idx[o];
-        if (id < 0) continue;
-        double r[3];
-        cell_offset(g, cells[m], res, r);
-        const double ps  = (double)phi_sum[id];
-        const double wgt = sc_w[o] / (ps > 1.0 ? ps : 1.0);
-        double       vs[3] = {vp[0], vp[1], vp[2]};
-        if (ph.rotation) {
-            vs[0] += op[1] * r[2] - op[2] * r[1];
-            vs[1] += op[2] * r[0] - op[0] * r[2];
-            vs[2] += op[0] * r[1] - op[1] * r[0];
+    // U cells per thread per round: their cache entries first, then every
+    // gather, then the sums, in the order m = t, t + B, t + 2B, ... of a
+    // one-cell loop (the gathers of a round are in flight together)
+    constexpr int U = 4;
+    for (int m0 = threadIdx.x; m0 < ncells; m0 += U * blockDim.x) {
+        int    id[U], cm[U];
+        double sw[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const int    m = m0 + k * blockDim.x;
+            const size_t o = (size_t)p * ncells + m;
+            id[k]          = m < ncells ? sc_idx[o] : -1;
+            sw[k]          = m < ncells ? sc_w[o] : 0.0;
+            cm[k]          = m < ncells ? cells[m] : 0;
         }
-        const double fp0 = (vs[0] - (double)u0[id]) * wgt;
-        const double fp1 = (vs[1] - (double)u1[id]) * wgt;
-        const double fp2 = (vs[2] - (double)u2[id]) * wgt;
-        acc[0] += fp0;
-        acc[1] += fp1;
-        acc[2] += fp2;
-        acc[3] += r[1] * fp2 - r[2] * fp1;
-        acc[4] += r[2] * fp0 - r[0] * fp2;
-        acc[5] += r[0] * fp1 - r[1] * fp0;
+        T ps[U], a0[U], a1[U], a2[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const int j = id[k] < 0 ? 0 : id[k];
+            ps[k]       = phi_sum[j];
+            a0[k]       = u0[j];
+            a1[k]       = u1[j];
+            a2[k]       = u2[j];
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            if (id[k] < 0) continue;
+            double r[3];
+            cell_offset(g, cm[k], res, r);
+            const double psd = (double)ps[k];
+            const double wgt = sw[k] / (psd > 1.0 ? psd : 1.0);
+            double       vs[3] = {vp[0], vp[1], vp[2]};
+            if (ph.rotation) {
+                vs[0] += op[1] * r[2] - op[2] * r[1];
+                vs[1] += op[2] * r[0] - op[0] * r[2];
+                vs[2] += op[0] * r[1] - op[1] * r[0];
+            }
+            const double fp0 = (vs[0] - (double)a0[k]) * wgt;
+            const double fp1 = (vs[1] - (double)a1[k]) * wgt;
+            const double fp2 = (vs[2] - (double)a2[k]) * wgt;
+            acc[0] += fp0;
+            acc[1] += fp1;
+            acc[2] += fp2;
+            acc[3] += r[1] * fp2 - r[2] * fp1;
+            acc[4] += r[2] * fp0 - r[0] * fp2;
+            acc[5] += r[0] * fp1 - r[1] * fp0;
+        }
     }
     block_sum6(acc);
     if (threadIdx.x == 0) {
