@@ -274,7 +274,10 @@ int spm_load_state(spm_ctx *ctx, const char *path);
  * spm_save_restart = Save_Restart_udf (resume.cxx:10-74, 381-506): writes a key
  * file with the keys of input_path (the run's input, UDF or key file; NULL for
  * the resume section alone), resume.Calculation = CONTINUE and the section
- * above for the context's state.  Rigid bodies and squirmers are refused. */
+ * above for the context's state.  In a rigid run Particles[] holds the bodies,
+ * followed by GR_body, GR_masses and GR_moments_body (resume.cxx:253-379,
+ * 925-1100); loading it needs the bodies' layout of spm_initialize.
+ * Squirmers are refused. */
 int spm_load_restart(spm_ctx *ctx, const char *path);
 /* Per-frame particle records of the reference's UDF output (output.UDF = ON;
  * Output_udf, output.cxx:268-375): spm_udf_out_record appends one record of

@@ -11,6 +11,7 @@
 #include <unordered_map>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <map>
 #include <memory>
 #include <sstream>

@@ -158,3 +158,42 @@ def test_restart_refuses_another_grid(gpu, tmp_path):
         run.initialize(parts)
         with pytest.raises(N.SpmError, match="not the context's grid"):
             run.load_restart(res)
+
+
+@pytest.mark.parametrize("fixture", ["rigid_32_free_gravity", "rigid_species_dof_thermostat"])
+def test_rigid_restart_both_ways(gpu, fixture, tmp_path):
+    """Rigid bodies in the restart file (Particles[] hold the bodies, then
+    GR_body, GR_masses and GR_moments_body; resume.cxx:253-379, 925-1100):
+    the reference's file resumes on the GPU, and this library's file resumes
+    in the reference program; both resumed runs follow the reference's own
+    resumed run within 1e-10 (bodies under gravity; two species with
+    switched-off degrees of freedom and the thermostat)."""
+    from tests.golden_util import load
+
+    cfg, parts, _ = load(fixture)
+    cfg = dataclasses.replace(cfg, num_snap=N1, gts=1)
+    tmp = str(tmp_path)
+    keys = _keys(tmp, "run.keys", cfg, parts)
+    # reference -> GPU
+    res = os.path.join(tmp, "ref_restart.keys")
+    ref_runner.run_reference(keys, restart_path=res)
+    cont = _extend(res, os.path.join(tmp, "ref_continue.keys"), N1 + N2)
+    dump = os.path.join(tmp, "resumed.dump")
+    ref_runner.run_reference(cont, dump_path=dump, fields_every=1)
+    frames = ref_runner.read_dump(dump)["frames"]
+    assert [f["ts"] for f in frames] == list(range(N1 + 1, N1 + N2 + 1))
+    with resume_run(cont, config=cfg) as run:
+        _follow(run, frames, "rigid restart file of the reference")
+    # GPU -> reference
+    mine = os.path.join(tmp, "gpu_restart.keys")
+    with SPMRun(cfg) as run:
+        run.initialize(parts)
+        run.step(N1 + 1)
+        run.save_restart(mine, keys)
+    cont2 = _extend(mine, os.path.join(tmp, "gpu_continue.keys"), N1 + N2)
+    dump2 = os.path.join(tmp, "resumed2.dump")
+    ref_runner.run_reference(cont2, dump_path=dump2, fields_every=1)
+    frames2 = ref_runner.read_dump(dump2)["frames"]
+    assert [f["ts"] for f in frames2] == list(range(N1 + 1, N1 + N2 + 1))
+    with resume_run(cont2, config=cfg) as run:
+        _follow(run, frames2, "rigid restart file of this library")
