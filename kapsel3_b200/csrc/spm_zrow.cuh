@@ -376,8 +376,9 @@ __device__ __forceinline__ cplx<T> advection_product(const AdvCoef &k, const cpl
 // (io fields 0..2), the five products, forward z of the products into io
 // fields 0..4.  Inputs kz >= kz_keep read as zero; outputs kz >= kz_span not
 // written.  UREG: the velocity rows stay in registers (3 V complex values per
-// thread); otherwise each thread parks them in its own slots of dynamic
-// shared memory (laid out thread-fastest, conflict-free).
+// thread); otherwise each thread parks u_x and u_y in its own slots of
+// dynamic shared memory (laid out thread-fastest, conflict-free) and keeps
+// u_z in registers, so that more rows fit an SM.
 template <typename T, int M, int R, bool UREG, int MINB = 1>
 __global__ void __launch_bounds__(R *ZR<M>::P, MINB)
     zr_products_kernel(cplx<T> *io, size_t field_stride_c, size_t run_stride_c, int nrows, int hnzp,
@@ -407,11 +408,14 @@ __global__ void __launch_bounds__(R *ZR<M>::P, MINB)
             zr_c2r<T, M>(t, a, wb, kv, xn, S, twM, scale, u[d]);
         }
     } else {
+        // u_x and u_y wait in shared memory, u_z stays in the registers it
+        // was transformed into
 #pragma unroll 1
         for (int d = 0; d < 3; d++) {
             cplx<T> kv[2][J], xn;
             zr_load_k<T, M>(io + d * field_stride_c + roff, ok, a, kz_keep, kv, xn);
             zr_c2r<T, M>(t, a, wb, kv, xn, S, twM, scale, u[0]);
+            if (d == 2) break;
 #pragma unroll
             for (int s = 0; s < BPT; s++)
 #pragma unroll
@@ -433,7 +437,7 @@ __global__ void __launch_bounds__(R *ZR<M>::P, MINB)
                     const cplx<T> zero{0, 0};
                     const cplx<T> ux = (p != 0 && p != 3) ? Upark[((0 * BPT + s) * Q + c) * NT] : zero;
                     const cplx<T> uy = (p != 1 && p != 4) ? Upark[((1 * BPT + s) * Q + c) * NT] : zero;
-                    const cplx<T> uz = (p != 2) ? Upark[((2 * BPT + s) * Q + c) * NT] : zero;
+                    const cplx<T> uz = (p != 2) ? u[0][s][c] : zero;
                     in[s][c]         = advection_product<T>(k, ux, uy, uz);
                 }
             }
@@ -446,7 +450,7 @@ __global__ void __launch_bounds__(R *ZR<M>::P, MINB)
 // Dynamic shared memory of zr_products_kernel.
 template <typename T, int M, int R, bool UREG>
 constexpr size_t zr_products_smem() {
-    return (size_t)R * ZRSmem<T, M>::blk + (UREG ? 0 : (size_t)3 * ZR<M>::V * R * ZR<M>::P * sizeof(cplx<T>));
+    return (size_t)R * ZRSmem<T, M>::blk + (UREG ? 0 : (size_t)2 * ZR<M>::V * R * ZR<M>::P * sizeof(cplx<T>));
 }
 
 }  // namespace spm
