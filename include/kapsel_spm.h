@@ -108,7 +108,8 @@ typedef struct spm_params {
     int    e_field;              /* Electric_field: 0 OFF, 1 DC, 2 AC */
     double e_ext[3];             /* Ex, Ey, Ez */
     double e_frequency;          /* AC: Frequency */
-    /* Janus particles (Particle_spec[0].janus_*, input.cxx:1403-1470; Navier_Stokes runs) */
+    /* Janus particles (Particle_spec[0].janus_*, input.cxx:1403-1470): tumblers and squirmers in
+     * Navier_Stokes and Shear_Navier_Stokes runs, obstacles with every equation (input.cxx:1509-1512) */
     int    janus_axis;           /* SPM_AXIS_*: the body axis e3 of the slip profile */
     int    janus_propulsion;     /* SPM_JANUS_* */
     double janus_force[3];       /* TUMBLER: janus_force, body frame */

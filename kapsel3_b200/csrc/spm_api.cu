@@ -373,9 +373,12 @@ int derive(const spm_params &p, Grid &g, Phys &ph) {
     if (p.janus_propulsion < SPM_JANUS_OFF || p.janus_propulsion > SPM_JANUS_OBSTACLE)
         return fail(SPM_ERR_ARG, "bad janus_propulsion");
     if (p.janus_axis < SPM_AXIS_NONE || p.janus_axis > SPM_AXIS_Z) return fail(SPM_ERR_ARG, "bad janus_axis");
-    if (p.janus_propulsion != SPM_JANUS_OFF && p.equation != SPM_EQ_NAVIER_STOKES &&
-        p.equation != SPM_EQ_SHEAR_NAVIER_STOKES)
-        return fail(SPM_ERR_ARG, "janus particles are served in Navier_Stokes and Shear_Navier_Stokes runs only");
+    // tumblers and squirmers only with the Navier-Stokes solvers; obstacles
+    // with every equation (input.cxx:1509-1512)
+    if ((p.janus_propulsion == SPM_JANUS_TUMBLER || p.janus_propulsion == SPM_JANUS_SQUIRMER) &&
+        p.equation != SPM_EQ_NAVIER_STOKES && p.equation != SPM_EQ_SHEAR_NAVIER_STOKES)
+        return fail(SPM_ERR_ARG, "janus tumblers and squirmers are served in Navier_Stokes and Shear_Navier_Stokes "
+                                 "runs only");
     if (p.janus_propulsion == SPM_JANUS_SQUIRMER) {
         if (p.janus_axis == SPM_AXIS_NONE) return fail(SPM_ERR_ARG, "a SQUIRMER needs a janus_axis (X, Y or Z)");
         if (!(p.slip_vel > 0.0)) return fail(SPM_ERR_ARG, "a SQUIRMER needs janus_slip_vel (B1) > 0");

@@ -1085,6 +1085,8 @@ __device__ __forceinline__ double pbc_obl(const Phys &ph, double *x, double gam,
 // index (for the bodies' torques), and under Lees-Edwards lj_stress[n] takes
 // the bodies' term sum f_x R_y instead, R the image distance of the two
 // bodies' centres xg (rigid_dev_shear_stress_lj, md_force.cxx:252-258).
+// Pairs of two obstacles are skipped (obstacle_chain, interaction.h:29-35);
+// the janus propulsion is the run's, so obstacle runs have no LJ pairs.
 // One warp per particle: lanes stride over the partners, then a warp sum.
 __global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift, const int *__restrict__ rid,
                          double *__restrict__ f_lo, const double *__restrict__ xg) {
@@ -1094,7 +1096,7 @@ __global__ void p_forces(Phys ph, PState s, int all_pairs_le, double le_shift, c
     double f[3]   = {0.0, 0.0, 0.0};
     double fl[3]  = {0.0, 0.0, 0.0};
     double stress = 0.0;
-    if (ph.lj_on) {
+    if (ph.lj_on && ph.janus_prop != 3) {
         for (int m = lane; m < ph.np; m += 32) {
             if (m == n || (rid && rid[m] == rid[n])) continue;
             const int hi = n > m ? n : m, lo = n > m ? m : n;
@@ -1366,29 +1368,10 @@ __global__ void p_velocity_mdf(Phys ph, PState s, const int *__restrict__ ts_dev
         const int i = 3 * n + d;
         s.mdf[i]    = euler ? ph.dt * s.fr[i] : ph.hdt * (s.fr[i] + s.fr_previous[i]);
     }
-    const int    sp  = spec_of(ph, n);
-    const double dmy = (euler ? ph.dt : ph.hdt) * ph.imass_s[sp];
-    const double dmr = (euler ? ph.dt : ph.hdt) * ph.imoi_s[sp];
-    for (int d = 0; d < 3; d++) {
-        const int i    = 3 * n + d;
-        s.v_old[i]     = s.v[i];
-        s.omega_old[i] = s.omega[i];
-        if (euler) {
-            s.v[i] += dmy * (s.f_hydro[i] + s.fr[i]);
-            s.omega[i] += dmr * (s.torque_hydro[i] + s.torque_r[i]);
-        } else {
-            s.v[i] += dmy * (2.0 * s.f_hydro[i] + s.fr[i] + s.fr_previous[i]);
-            s.omega[i] += dmr * (2.0 * s.torque_hydro[i] + s.torque_r[i] + s.torque_r_previous[i]);
-        }
-        s.fr_previous[i]           = s.fr[i];
-        s.fr[i]                    = 0.0;
-        s.f_hydro_previous[i]      = s.f_hydro[i];
-        s.f_hydro[i]               = 0.0;
-        s.torque_r_previous[i]     = s.torque_r[i];
-        s.torque_r[i]              = 0.0;
-        s.torque_hydro_previous[i] = s.torque_hydro[i];
-        s.torque_hydro[i]          = 0.0;
-    }
+    // then the same update as Navier_Stokes runs, obstacles held at rest (the
+    // obstacle branch of the _OBL solvers); tumblers and squirmers are
+    // refused under Lees-Edwards, so the self-propulsion term is zero here
+    velocity_update_one(ph, s, n, euler);
 }
 
 // Advances the device step counters of `nr` consecutive runs (end of every

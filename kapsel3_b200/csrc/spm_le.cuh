@@ -674,10 +674,11 @@ __global__ void k_le_stress_finish(LEDev *le, const double *ppart, const double 
 
 // PBC_OBL wrap after the position update (particle_solver.cxx:283-334,
 // periodic_boundary.h:26-45): crossing the y boundary shifts x by the
-// oblique image and v_x by -+ Shear_rate_eff * LY.
+// oblique image and v_x by -+ Shear_rate_eff * LY.  Obstacles stay where
+// they are (the wrap sits inside the non-obstacle branch there).
 __global__ void p_le_wrap(Phys ph, PState s, double gam, const LEDev *__restrict__ le) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= ph.np) return;
+    if (n >= ph.np || ph.janus_prop == 3) return;
     const double dvx = pbc_obl(ph, s.x + 3 * n, gam, le->srate_eff);
     s.v[3 * n] += dvx;
     s.v_old[3 * n] += dvx;

@@ -51,6 +51,13 @@ CASES["salt_lj_contact"] = SPMConfig(npx=5, npy=5, npz=5, n_particles=2, a=4.0, 
                                      kbt=1.0, salt=True, valency=(1.0, -1.0), onsager=(1.0, 1.0),
                                      debye_length=5.0, surface_charge=10.0, gts=1, num_snap=8)
 
+# obstacles (fixed particles, out of the LJ pairs: obstacle_chain,
+# interaction.h:29-35) in contact, in a DC field
+CASES["salt_dc_obstacles"] = SPMConfig(npx=5, npy=5, npz=5, n_particles=2, a=4.0, a_xi=2.0, dt=0.01,
+                                       equation=EQ_EL, kbt=1.0, salt=True, valency=(1.0, -1.0), onsager=(1.0, 1.0),
+                                       debye_length=5.0, surface_charge=10.0, janus_propulsion="OBSTACLE",
+                                       e_field="DC", e_ext=(0.1, 0.0, 0.0), gts=1, num_snap=8)
+
 
 PB = dict(npx=5, npy=5, npz=5, a=4.0, a_xi=2.0, dt=0.01, equation=EQ_EL, kbt=1.0, init_pb=True, gts=1, num_snap=4)
 CASES["pb_counterions"] = SPMConfig(n_particles=1, dielectric=1.0, valency=(1.0, 0.0), onsager=(1.0, 1.0),
@@ -66,7 +73,7 @@ CASES["pb_salt_two_dc"] = SPMConfig(n_particles=2, dielectric=1.0, salt=True, va
 
 def _particles(name, cfg):
     parts = make_particles(cfg, seed=7, v_sd=1e-3, random_orientation=True)
-    if name == "salt_lj_contact":
+    if name in ("salt_lj_contact", "salt_dc_obstacles"):
         # centres 8.6 apart: inside the cut-off 2^(1/6) SIGMA = 8.98 (SIGMA = 2 A DX)
         parts["x"][0] = (12.0, 16.0, 15.5)
         parts["x"][1] = (20.6, 16.0, 15.5)
@@ -99,6 +106,8 @@ def test_electrolyte_matches_the_reference_program(gpu, name, tmp_path):
             for n in range(fr["conc"].shape[0]):
                 c = run.concentration(n)
                 assert rel(c, fr["conc"][n]) <= TOL, (name, fr["ts"], "conc", n, rel(c, fr["conc"][n]))
+    if cfg.janus_propulsion == "OBSTACLE":
+        assert not p["v"].any() and np.array_equal(p["x"], parts["x"])
 
 
 def test_electrolyte_parameter_checks(gpu):
