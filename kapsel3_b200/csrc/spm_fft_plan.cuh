@@ -39,6 +39,14 @@ struct FFTPlan {
     static constexpr int pminb() {
         return ureg<MM>() && MM == 128 ? 3 : 1;
     }
+    // The FP64 inverse pass at M = 128 wants 132 registers, three CTAs of 128
+    // threads per SM; capped at 128 a fourth fits, for a pass bound by load
+    // latency (FP64 step at 256^3: 1.649 -> 1.623 ms).  Every other
+    // instance keeps the compiler's own allocation (0: no cap).
+    template <int MM>
+    static constexpr int c2r_minb() {
+        return sizeof(T) == 8 && MM == 128 ? 4 : 0;
+    }
 
     // Fused inverse-z / advection products / forward-z pass over five slots.
     cudaError_t z_products(cplx<T> *io, size_t fs_c, int nruns, size_t run_stride_c, cudaStream_t st, int kz_keep,
@@ -117,8 +125,13 @@ struct FFTPlan {
 #define SPM_ZC2R(MM)                                                                                          \
     case MM: {                                                                                                \
         constexpr int RR = zr_rows<T, MM>();                                                                  \
-        zr_c2r_kernel<T, MM, RR><<<dim3((nrows + RR - 1) / RR, nfields), RR * ZR<MM>::P, 0, st>>>(            \
-            in, out, fs_c, fs_real, nrows, g.hnzp, tw_zm, tw_zn, scale, kz_keep);                             \
+        const dim3    grid((nrows + RR - 1) / RR, nfields);                                                   \
+        if constexpr (c2r_minb<MM>() > 1)                                                                     \
+            zr_c2r_kernel_capped<T, MM, RR, c2r_minb<MM>()><<<grid, RR * ZR<MM>::P, 0, st>>>(                 \
+                in, out, fs_c, fs_real, nrows, g.hnzp, tw_zm, tw_zn, scale, kz_keep);                         \
+        else                                                                                                  \
+            zr_c2r_kernel<T, MM, RR><<<grid, RR * ZR<MM>::P, 0, st>>>(in, out, fs_c, fs_real, nrows, g.hnzp,  \
+                                                                      tw_zm, tw_zn, scale, kz_keep);          \
     } break;
             SPM_ZC2R(4) SPM_ZC2R(8) SPM_ZC2R(16) SPM_ZC2R(32) SPM_ZC2R(64) SPM_ZC2R(128) SPM_ZC2R(256)
 #undef SPM_ZC2R

@@ -278,11 +278,11 @@ constexpr int zr_rows() {
 // Inverse z pass: complex rows -> real rows scaled by `scale` (in place
 // allowed); inputs kz >= kz_keep read as zero.
 template <typename T, int M, int R>
-__global__ void __launch_bounds__(R *ZR<M>::P)
-    zr_c2r_kernel(const cplx<T> *in, T *out, size_t field_stride_c, size_t field_stride_real, int nrows, int hnzp,
-                  const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale, int kz_keep) {
+__device__ __forceinline__ void zr_c2r_rows(unsigned char *smem, const cplx<T> *in, T *out, size_t field_stride_c,
+                                            size_t field_stride_real, int nrows, int hnzp,
+                                            const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale,
+                                            int kz_keep) {
     constexpr int P = ZR<M>::P, Q = ZR<M>::Q, J = ZR<M>::J, BPT = ZR<M>::BPT;
-    __shared__ __align__(16) unsigned char smem[R * ZRSmem<T, M>::blk];
     const int  r   = threadIdx.x / P;
     const int  t   = threadIdx.x % P;
     const int  row = blockIdx.x * R + r;
@@ -308,6 +308,22 @@ __global__ void __launch_bounds__(R *ZR<M>::P)
         }
     if (t == 0)
         for (int k = 2 * M; k < 2 * hnzp; k++) rout[k] = (T)0;
+}
+template <typename T, int M, int R>
+__global__ void __launch_bounds__(R *ZR<M>::P)
+    zr_c2r_kernel(const cplx<T> *in, T *out, size_t field_stride_c, size_t field_stride_real, int nrows, int hnzp,
+                  const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale, int kz_keep) {
+    __shared__ __align__(16) unsigned char smem[R * ZRSmem<T, M>::blk];
+    zr_c2r_rows<T, M, R>(smem, in, out, field_stride_c, field_stride_real, nrows, hnzp, twM, twN, scale, kz_keep);
+}
+// The same pass with the registers capped for MINB resident CTAs per SM.
+template <typename T, int M, int R, int MINB>
+__global__ void __launch_bounds__(R *ZR<M>::P, MINB)
+    zr_c2r_kernel_capped(const cplx<T> *in, T *out, size_t field_stride_c, size_t field_stride_real, int nrows,
+                         int hnzp, const cplx<T> *__restrict__ twM, const cplx<T> *__restrict__ twN, T scale,
+                         int kz_keep) {
+    __shared__ __align__(16) unsigned char smem[R * ZRSmem<T, M>::blk];
+    zr_c2r_rows<T, M, R>(smem, in, out, field_stride_c, field_stride_real, nrows, hnzp, twM, twN, scale, kz_keep);
 }
 
 // Forward z pass: real rows -> complex rows (in place allowed); outputs kz >=
